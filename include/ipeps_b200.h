@@ -1,0 +1,138 @@
+/*
+ * libipeps_b200 — C ABI of the B200 CTMRG engine (drop-in for the CTMRG hot
+ * path of iPEPS.jl).
+ *
+ * The reference has no FFI: its hot path sits behind the Julia functions
+ * listed beside each entry point (paths relative to the iPEPS.jl source
+ * tree).  A Julia binding calls these through `ccall`; the Python binding in
+ * ipeps.jl_b200/host.py calls them through ctypes.
+ *
+ * Conventions
+ *  - Every function returns an int status (IPEPS_OK, or one of the codes
+ *    below); the message of the last failure is ipeps_last_error(ctx).
+ *  - Host arrays are column-major (Julia layout).  Real data is double;
+ *    complex data is interleaved (re, im) double pairs (ComplexF64).
+ *  - Hamiltonian bond matrices (d^2 x d^2) are always passed as complex.
+ *  - The library owns all device memory behind opaque handles.  Each context
+ *    owns one CUDA stream; calls are synchronous on return; a handle is not
+ *    thread-safe (use one context per host thread).
+ */
+#ifndef IPEPS_B200_H
+#define IPEPS_B200_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define IPEPS_API __attribute__((visibility("default")))
+#else
+#define IPEPS_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define IPEPS_OK 0
+#define IPEPS_ENOTCONV 1   /* an iteration cap was hit (CTMRG or Jacobi) */
+#define IPEPS_ENONFINITE 2 /* NaN/Inf detected in a result */
+#define IPEPS_EOOM 3       /* device allocation failed */
+#define IPEPS_EINVAL 4     /* bad argument / shape */
+#define IPEPS_ECUDA 5      /* other CUDA error */
+
+#define IPEPS_PREC_FP64 0  /* every contraction in FP64 */
+#define IPEPS_PREC_MIXED 1 /* contractions as 3xTF32 on tcgen05, FP64 SVD/normalisation/energy */
+
+#define IPEPS_CONV_ENERGY 0   /* run_ctm with conv_fun = get_gs_energy (ctmrg.jl:21-28) */
+#define IPEPS_CONV_SPECTRUM 1 /* run_ctm without conv_fun: left-move spectrum (ctmrg.jl:29-31) */
+#define IPEPS_CONV_ES 2       /* conv_fun = get_es_energy / get_all_norm (optim_es.jl:175) */
+
+typedef struct ipeps_ctx ipeps_ctx;
+typedef struct ipeps_env ipeps_env;
+
+typedef struct {
+  uint64_t launches[8]; /* per kernel family: permute, gemm_f64, gemm_tf32x3, reduce, elementwise, small_linalg, jacobi */
+  double flops[8];
+  double bytes[8];
+  uint64_t moves;       /* directional moves done by all envs of this context */
+  double move_seconds;  /* host wall time inside moves (synchronous) */
+} ipeps_stats_t;
+
+/* ---- context (no reference counterpart: the reference is one CPU process) */
+IPEPS_API int ipeps_ctx_create(int device, ipeps_ctx** out);
+IPEPS_API int ipeps_ctx_destroy(ipeps_ctx* ctx);
+IPEPS_API const char* ipeps_last_error(ipeps_ctx* ctx);
+IPEPS_API int ipeps_ctx_set_precision(ipeps_ctx* ctx, int precision);
+IPEPS_API int ipeps_ctx_set_seed(ipeps_ctx* ctx, uint64_t seed);
+IPEPS_API int ipeps_stats(ipeps_ctx* ctx, ipeps_stats_t* out);
+IPEPS_API int ipeps_stats_reset(ipeps_ctx* ctx);
+/* the context's CUDA stream (cudaStream_t), for callers that time or order work on it */
+IPEPS_API int ipeps_ctx_stream(ipeps_ctx* ctx, void** stream);
+/* per-kernel-family CUDA-event timing: enable, then query ms / launches /
+ * credited flops / bytes per family since enabling (query clears the window) */
+IPEPS_API int ipeps_prof_enable(ipeps_ctx* ctx, int on);
+IPEPS_API int ipeps_prof_query(ipeps_ctx* ctx, double* ms, uint64_t* launches, double* flops, double* bytes);
+
+/* ---- contraction operator: tcon(ind_xs, ind_y, A, B) (src/utility/wrapper.jl:15-23).
+ * la/lb: labels per leg (positive = summed, negative -1..-n = output order).
+ * out receives the result (capacity out_cap elements), out_dims/out_nd its shape.
+ * is_complex applies to A, B and out. */
+IPEPS_API int ipeps_tcon(ipeps_ctx* ctx, int is_complex, const double* A, int nA, const int64_t* dimsA, const int* la,
+               const double* B, int nB, const int64_t* dimsB, const int* lb, double* out, int64_t out_cap,
+               int64_t* out_dims, int* out_nd);
+/* ---- projector: get_projector(R1, R2, chi) (ctmrg.jl:254-265) for real N x N R1, R2.
+ * P1 (N x n) and P2 (n x N) need capacity N*(chi+1); s capacity chi+1; *n = kept count. */
+IPEPS_API int ipeps_projector(ipeps_ctx* ctx, const double* R1, const double* R2, int64_t N, int chi, double* P1,
+                    double* P2, double* s, int* n);
+
+/* ---- environment state: CTMTensors (src/ctm/ctm_tensor.jl:3-18, ctors :57-69) */
+IPEPS_API int ipeps_env_create(ipeps_ctx* ctx, int D, int d, int chi, int is_complex, ipeps_env** out);
+IPEPS_API int ipeps_env_destroy(ipeps_env* env);
+/* Params Dict keys chi/min_iter/max_iter/ad_max_iter/rg_tol (default_config.toml:9-17) */
+IPEPS_API int ipeps_env_set_params(ipeps_env* env, int chi, int min_iter, int max_iter, int ad_max_iter, double rg_tol);
+/* projector sketch: k = n+1 + max(min_over, (n+1)*num/den); power iterations cold/warm */
+IPEPS_API int ipeps_env_set_svd_params(ipeps_env* env, int over_num, int over_den, int min_over, int power_iters,
+                             int power_iters_warm, int warm_start);
+/* A (D,D,D,D,d); Ad = NULL means conj(A) (CTMTensors(A, cfg), ctm_tensor.jl:63) */
+IPEPS_API int ipeps_env_set_A(ipeps_env* env, const double* A, const double* Ad);
+/* init_ctm1 (ctm_tensor.jl:97-130) */
+IPEPS_API int ipeps_env_init(ipeps_env* env);
+/* C_k (chi_a x chi_b) and E_k (chi_a, chi_b, D, D), k = 1..4 (ts.Cs[k], ts.Es[k]).
+ * Pass NULL data pointers to query the dims only. */
+IPEPS_API int ipeps_env_get_CT(ipeps_env* env, int k, double* C, int64_t* C_dims, double* E, int64_t* E_dims);
+IPEPS_API int ipeps_env_set_CT(ipeps_env* env, int k, const double* C, const int64_t* C_dims, const double* E,
+                     const int64_t* E_dims);
+
+/* ---- moves: left_rg/right_rg/top_rg/bottom_rg (ctmrg.jl:66-120), dir 0..3.
+ * s_out (capacity *s_len on entry) receives the kept singular values of the
+ * projector; *s_len is set to their count. */
+IPEPS_API int ipeps_ctm_move(ipeps_env* env, int dir, double* s_out, int* s_len);
+/* rg_step (ctmrg.jl:57-64): left, right, top, bottom; s of the left move */
+IPEPS_API int ipeps_ctm_step(ipeps_env* env, double* s_out, int* s_len);
+/* run_ctm (ctmrg.jl:1-55).  Hh/Hv complex d2 x d2 (needed for the energy
+ * and es modes).  Returns IPEPS_OK also when not converged (the reference only
+ * prints "Not Converged"); *converged reports it. */
+IPEPS_API int ipeps_ctm_run(ipeps_env* env, int conv_mode, const double* Hh, const double* Hv, int d2, int* iters,
+                  double* last_diff, int* converged);
+/* per-iteration log of the last run: 4 doubles per iteration (diff, obj_re, obj_im, chi) */
+IPEPS_API int ipeps_ctm_log(ipeps_env* env, double* out, int* n_iters);
+
+/* ---- observables (src/graph/evaluation.jl) */
+/* get_gs_energy (evaluation.jl:15-29): E and Na complex (re, im) */
+IPEPS_API int ipeps_energy(ipeps_env* env, const double* Hh, const double* Hv, int d2, double* E, double* Na);
+/* get_gs_norm (evaluation.jl:47-59) */
+IPEPS_API int ipeps_gs_norm(ipeps_env* env, double* nrm);
+
+/* ---- nested-tensor (excited-state) move, optim_es (src/optimize/optim_es.jl:167-210) */
+/* setproperties(ts, B=B, Bd=conj(B)) + Params px, py (in radians); B complex (D,D,D,D,d).
+ * Clears the B/Bd/BB environment slots (EmptyT). */
+IPEPS_API int ipeps_nested_set_B(ipeps_env* env, const double* B, double px, double py);
+/* get_es_energy (evaluation.jl:31-45) */
+IPEPS_API int ipeps_es_energy(ipeps_env* env, const double* Hh, const double* Hv, int d2, double* E);
+/* get_all_norm (evaluation.jl:61-77): Nb (complex) and envB (complex, size of A) */
+IPEPS_API int ipeps_all_norm(ipeps_env* env, double* Nb, double* envB);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* IPEPS_B200_H */

@@ -1,0 +1,85 @@
+// CTMRG environment and moves (src/ctm/ctmrg.jl, src/ctm/ctm_tensor.jl,
+// src/graph/evaluation.jl, src/nested_tensor/*.jl of the reference).
+#pragma once
+#include "projector.cuh"
+
+#include <array>
+#include <complex>
+
+namespace ipeps {
+
+// Nested tensor: component 0 is the plain tensor; 1..3 are the B, Bd, BB
+// slots (empty tensor == EmptyT).  A plain tensor has nested == false.
+struct NT {
+  std::array<Tensor, 4> c;
+  bool nested = false;
+  NT() = default;
+  NT(const Tensor& t) { c[0] = t; }  // NOLINT: implicit plain -> NT
+  bool has(int i) const { return !c[i].empty(); }
+};
+
+NT ntcon(Ctx& c, const NT& A, const std::vector<int>& la, const NT& B, const std::vector<int>& lb);
+NT nreshape(const NT& A, const std::vector<int64_t>& s);
+NT npermute(Ctx& c, const NT& A, const std::vector<int>& perm);
+NT nmatmul(Ctx& c, const NT& A, char opA, const NT& B, char opB);
+NT nshift(Ctx& c, const NT& A, double phi);
+void nrenormalize(Ctx& c, NT& A);
+
+struct CtmParams {
+  int chi = 32;
+  int min_iter = 4;
+  int max_iter = 20;
+  int ad_max_iter = 4;
+  double rg_tol = 1e-6;
+  SvdParams svd;
+};
+
+struct CtmLogEntry {
+  int iter;
+  double diff;
+  double obj_re, obj_im;
+  int chi_left;
+};
+
+struct Env {
+  Ctx* ctx = nullptr;
+  int D = 0, d = 0;
+  DType dt = DType::F64;   // dtype of A
+  CtmParams prm;
+  Tensor A, Ad;
+  std::array<Tensor, 4> Cs, Es;
+  // nested (excited-state) slots
+  bool nested = false;
+  Tensor B, Bd;
+  std::array<Tensor, 4> B_Cs, Bd_Cs, BB_Cs, B_Es, Bd_Es, BB_Es;
+  double px = 0, py = 0;
+  ProjCache cache[4];
+  std::vector<double> last_s;  // spectrum of the last left move
+  std::vector<CtmLogEntry> log;
+  // statistics
+  uint64_t moves = 0;
+  double move_seconds = 0;
+
+  NT all_A() const;
+  NT all_Ad() const;
+  NT all_C(int i) const;
+  NT all_E(int i) const;
+};
+
+void init_ctm1(Env& e);
+// one directional move; dir 0=left 1=right 2=top 3=bottom; returns s (host)
+std::vector<double> ctm_move(Env& e, int dir);
+std::vector<double> rg_step(Env& e);
+// energy (evaluation.jl:15-29): E (complex) and Na (complex)
+void gs_energy(Env& e, const Tensor& Hh, const Tensor& Hv, std::complex<double>* E, std::complex<double>* Na);
+// nested energy (evaluation.jl:31-45): real(E[4])
+double es_energy(Env& e, const Tensor& Hh, const Tensor& Hv);
+// get_all_norm (evaluation.jl:61-77): returns Nb, writes envB (complex, size of A)
+std::complex<double> all_norm(Env& e, Tensor* envB);
+// get_gs_norm (evaluation.jl:47-59)
+std::complex<double> gs_norm(Env& e);
+// run_ctm (ctmrg.jl:1-55). conv_mode 0: energy (gs), 1: spectrum, 2: es energy / all_norm.
+// Returns iterations done; *last_diff = diffs[end]; *converged.
+int run_ctm(Env& e, int conv_mode, const Tensor* Hh, const Tensor* Hv, double* last_diff, bool* converged);
+
+}  // namespace ipeps

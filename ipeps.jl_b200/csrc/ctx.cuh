@@ -1,0 +1,151 @@
+// Engine context: one CUDA stream per context, a stream-ordered memory pool,
+// per-kernel-family launch/flop counters and the small helpers every
+// contraction uses.
+#pragma once
+
+#include "common.cuh"
+
+#include <array>
+#include <map>
+#include <tuple>
+
+namespace ipeps {
+
+enum class KFam : int {
+  Permute = 0,
+  GemmF64,
+  GemmTF32x3,
+  Reduce,
+  Elementwise,
+  SmallLinalg,
+  Jacobi,
+  Count
+};
+
+struct KStat {
+  uint64_t launches = 0;
+  double flops = 0;   // algorithmic flops credited (2*M*N*K per real GEMM, 8*M*N*K complex)
+  double bytes = 0;   // algorithmic bytes moved (permutes, reductions)
+};
+
+enum Precision : int { kPrecFP64 = 0, kPrecMixed = 1 };
+
+struct Ctx {
+  int device = 0;
+  std::shared_ptr<StreamHolder> sh;
+  cudaStream_t stream = nullptr;
+  int sm_count = 148;
+  int precision = kPrecFP64;
+  uint64_t rng_seed = 0x1234abcdULL;
+  uint64_t rng_counter = 0;
+  std::string last_error;
+  std::array<KStat, int(KFam::Count)> stats{};
+  // split-K partial sums live here (grown on demand, stream ordered)
+  std::shared_ptr<DBuf> ws;
+  // small device scalars (max-abs, traces, status words)
+  std::shared_ptr<DBuf> scal;
+  int* d_status = nullptr;
+  // per-kernel-family CUDA-event timing (enabled by ipeps_prof_enable)
+  bool prof = false;
+  std::array<KStat, int(KFam::Count)> prof_stats{};
+  std::vector<std::tuple<int, cudaEvent_t, cudaEvent_t>> prof_rec;
+  std::vector<cudaEvent_t> ev_pool;
+  cudaEvent_t take_event();
+  // returns ms per family and clears the records
+  std::array<double, int(KFam::Count)> prof_collect();
+
+  explicit Ctx(int dev);
+  ~Ctx();
+
+  Tensor alloc(DType dt, const std::vector<int64_t>& dims);
+  Tensor zeros(DType dt, const std::vector<int64_t>& dims);
+  void* workspace(size_t bytes);
+  void sync() { IPEPS_CUDA(cudaStreamSynchronize(stream)); }
+  void count(KFam f, double flops = 0, double bytes = 0) {
+    auto& s = stats[int(f)];
+    s.launches++;
+    s.flops += flops;
+    s.bytes += bytes;
+    if (prof) {
+      auto& p = prof_stats[int(f)];
+      p.launches++;
+      p.flops += flops;
+      p.bytes += bytes;
+    }
+  }
+};
+
+// Brackets the launches of one kernel family with CUDA events on the
+// context stream while profiling is enabled.
+struct ProfScope {
+  Ctx& c;
+  int fam;
+  cudaEvent_t a = nullptr;
+  ProfScope(Ctx& cc, KFam f) : c(cc), fam(int(f)) {
+    if (c.prof) {
+      a = c.take_event();
+      cudaEventRecord(a, c.stream);
+    }
+  }
+  ~ProfScope() {
+    if (a) {
+      cudaEvent_t b = c.take_event();
+      cudaEventRecord(b, c.stream);
+      c.prof_rec.emplace_back(fam, a, b);
+    }
+  }
+};
+
+// ---------------------------------------------------------------- kernels
+// permute: out = permutedims(in, perm) (0-based perm, Julia semantics:
+// size(out,i) = size(in, perm[i])).
+Tensor permute(Ctx& c, const Tensor& in, const std::vector<int>& perm);
+// out = in (copy) into a fresh contiguous tensor
+Tensor clone(Ctx& c, const Tensor& in);
+
+// C = alpha*op(A)*op(B) + beta*C, column-major, op in {'N','T','C'}.
+// Dispatches on c.precision for real operands (FP64 SIMT or 3xTF32 tcgen05).
+void gemm(Ctx& c, DType dt, char opA, char opB, int64_t m, int64_t n, int64_t k,
+          cuDoubleComplex alpha, const void* A, int64_t lda, const void* B, int64_t ldb,
+          cuDoubleComplex beta, void* C, int64_t ldc, bool force_fp64 = false);
+// FP64 SIMT GEMM (always available)
+void gemm_f64(Ctx& c, DType dt, char opA, char opB, int64_t m, int64_t n, int64_t k,
+              cuDoubleComplex alpha, const void* A, int64_t lda, const void* B, int64_t ldb,
+              cuDoubleComplex beta, void* C, int64_t ldc);
+// 3xTF32 tcgen05 GEMM for real operands (FP32-accumulated split products)
+void gemm_tf32x3(Ctx& c, char opA, char opB, int64_t m, int64_t n, int64_t k, double alpha,
+                 const double* A, int64_t lda, const double* B, int64_t ldb, double beta, double* C,
+                 int64_t ldc);
+
+inline cuDoubleComplex cplx(double r, double i = 0) { return make_cuDoubleComplex(r, i); }
+
+// Matrix product helpers on 2-D tensors: returns op(A)*op(B)
+Tensor matmul(Ctx& c, const Tensor& A, char opA, const Tensor& B, char opB);
+
+// tcon: contraction with the reference's label convention (positive labels
+// are summed, negative labels -1,-2,... give the output order).
+Tensor tcon(Ctx& c, const Tensor& A, const std::vector<int>& la, const Tensor& B,
+            const std::vector<int>& lb);
+// out += tcon(...) (out must have the output shape)
+void tcon_acc(Ctx& c, Tensor& out, const Tensor& A, const std::vector<int>& la, const Tensor& B,
+              const std::vector<int>& lb);
+
+// ------------------------------------------------------------ reductions
+// d_out[0] = max |x| (device scalar)
+void maxabs(Ctx& c, const Tensor& x, double* d_out);
+// x *= 1/d_s[0] (x real or complex), in place
+void scale_inv(Ctx& c, Tensor& x, const double* d_s);
+// x *= s (complex scalar), in place
+void scale(Ctx& c, Tensor& x, cuDoubleComplex s);
+// y += a*x
+void axpy(Ctx& c, cuDoubleComplex a, const Tensor& x, Tensor& y);
+// conj copy (returns new tensor; real input -> plain copy)
+Tensor conj(Ctx& c, const Tensor& x);
+// convert real tensor to complex128
+Tensor to_complex(Ctx& c, const Tensor& x);
+// nonfinite scan: sets bit in c.d_status
+void check_finite(Ctx& c, const Tensor& x);
+// fill with N(0,1) (counter-based hash RNG, reproducible)
+void randn(Ctx& c, Tensor& x);
+
+}  // namespace ipeps

@@ -1,0 +1,29 @@
+// Small dense FP64 linear algebra (single-CTA kernels) used by the projector.
+#pragma once
+#include "ctx.cuh"
+
+namespace ipeps {
+
+// In-place guarded Cholesky of a k x k SPD matrix: G = R^T R (upper R,
+// strict lower triangle zeroed).  If d_trace_shift is given, shift_factor *
+// (*d_trace_shift) is first added to the diagonal (shifted CholeskyQR).
+void chol_upper(Ctx& c, double* G, int k, int64_t ldg, const double* d_trace_shift, double shift_factor);
+// X = R^-1 (R upper triangular)
+void triinv_upper(Ctx& c, const double* R, int k, int64_t ldr, double* X, int64_t ldx);
+// d_out = trace(G)
+void trace(Ctx& c, const double* G, int k, int64_t ldg, double* d_out);
+// One-sided Jacobi on the m x k matrix X: X <- X J with orthogonal columns,
+// J accumulated (k x k), S = column norms (unsorted).
+void jacobi_svd(Ctx& c, double* X, int m, int k, int64_t ldx, double* J, int64_t ldj, double* S,
+                int max_sweeps, double tol, int* d_sweeps);
+// Descending sort with permutation (ties: later index first)
+void sort_desc(Ctx& c, const double* S, int k, double* S_out, int* perm);
+// out[:, j] = in[:, perm[j]] * f(scale[j]); scale_mode 0: 1, 1: scale, 2: 1/scale
+void gather_cols(Ctx& c, const double* in, int64_t ldi, int64_t m, const int* perm, int ncols,
+                 const double* scale_v, int scale_mode, double* out, int64_t ldo);
+// X[:, j] *= f(s[j]); mode 1: 1/sqrt(s), 0: s
+void scale_cols(Ctx& c, double* X, int64_t ldx, int64_t m, int ncols, const double* s, int mode);
+// X[i, :] *= f(s[i]); mode 1: 1/sqrt(s), 0: s
+void scale_rows(Ctx& c, double* X, int64_t ldx, int64_t m, int64_t ncols, const double* s, int mode);
+
+}  // namespace ipeps

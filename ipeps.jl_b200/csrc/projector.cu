@@ -1,0 +1,171 @@
+// Projector of the directional CTMRG move.
+//
+// The reference forms M = R1*R2 (N x N, N = chi*D^2) and takes its full LAPACK
+// SVD (ctmrg.jl:254-265, wrapper.jl:25-55).  Here M is never formed: a
+// randomized range finder with power iterations works on R1 (R2 X) and
+// R2^T (R1^T X) (all GEMMs), the sketches are orthonormalised by shifted
+// CholeskyQR in FP64, and the projected k x k matrix is diagonalised by a
+// one-sided Jacobi SVD in FP64 (k = n+1 plus oversampling).  The previous
+// right singular vectors of the same direction seed the sketch (warm start),
+// which near the CTMRG fixed point leaves the Jacobi almost nothing to do.
+// Sorting, the relative cutoff 1e-12 and the degenerate-pair rule are applied
+// exactly as in cutoff_matrix.
+#include "linalg.cuh"
+#include "projector.cuh"
+
+#include <algorithm>
+#include <cmath>
+
+namespace ipeps {
+
+Tensor apply(Ctx& c, const MatRef& R, char op, const Tensor& X) {
+  // op(R) * X
+  bool t = (op == 'T') != R.trans;
+  int64_t m = (op == 'N') ? R.rows() : R.cols();
+  int64_t kk = (op == 'N') ? R.cols() : R.rows();
+  IPEPS_CHECK(X.dims[0] == kk, "apply: shape mismatch");
+  int64_t n = X.nd > 1 ? X.dims[1] : 1;
+  Tensor Y = c.alloc(DType::F64, {m, n});
+  gemm(c, DType::F64, t ? 'T' : 'N', 'N', m, n, kk, cplx(1), R.t.data(), R.t.dims[0], X.data(), X.dims[0],
+       cplx(0), Y.data(), m);
+  return Y;
+}
+
+Tensor apply_left_T(Ctx& c, const Tensor& X, const MatRef& R, char op) {
+  // X^T * op(R): X is (kk x m) -> result (m x ncols)
+  bool t = (op == 'T') != R.trans;
+  int64_t kk = (op == 'N') ? R.rows() : R.cols();
+  int64_t n = (op == 'N') ? R.cols() : R.rows();
+  IPEPS_CHECK(X.dims[0] == kk, "apply_left_T: shape mismatch");
+  int64_t m = X.dims[1];
+  Tensor Y = c.alloc(DType::F64, {m, n});
+  gemm(c, DType::F64, 'T', t ? 'T' : 'N', m, n, kk, cplx(1), X.data(), X.dims[0], R.t.data(), R.t.dims[0],
+       cplx(0), Y.data(), m);
+  return Y;
+}
+
+Tensor orth(Ctx& c, const Tensor& Y0, int passes, Tensor* Rout) {
+  const int64_t N = Y0.dims[0];
+  const int k = int(Y0.dims[1]);
+  Tensor Y = Y0;
+  Tensor G = c.alloc(DType::F64, {k, k});
+  Tensor Ri = c.alloc(DType::F64, {k, k});
+  Tensor Racc;
+  double* d_tr = reinterpret_cast<double*>(c.scal->p) + 8;
+  const double u = 1.1102230246251565e-16;
+  for (int pass = 0; pass < passes; ++pass) {
+    // G = Y^T Y  (FP64 always: the Gram matrix is where precision is lost)
+    gemm(c, DType::F64, 'T', 'N', k, k, N, cplx(1), Y.data(), N, Y.data(), N, cplx(0), G.data(), k, true);
+    if (pass == 0) {
+      trace(c, G.f64(), k, k, d_tr);
+      chol_upper(c, G.f64(), k, k, d_tr, 11.0 * (double(N) * k + double(k) * (k + 1)) * u);
+    } else {
+      chol_upper(c, G.f64(), k, k, nullptr, 0.0);
+    }
+    triinv_upper(c, G.f64(), k, k, Ri.f64(), k);
+    Tensor Yn = c.alloc(DType::F64, {N, k});
+    gemm(c, DType::F64, 'N', 'N', N, k, k, cplx(1), Y.data(), N, Ri.data(), k, cplx(0), Yn.data(), N, true);
+    Y = Yn;
+    if (Rout) {
+      if (pass == 0) {
+        Racc = clone(c, G);
+      } else {
+        Tensor Rn = c.alloc(DType::F64, {k, k});
+        gemm(c, DType::F64, 'N', 'N', k, k, k, cplx(1), G.data(), k, Racc.data(), k, cplx(0), Rn.data(), k, true);
+        Racc = Rn;
+      }
+    }
+  }
+  if (Rout) *Rout = Racc;
+  return Y;
+}
+
+ProjResult get_projector(Ctx& c, const MatRef& R1, const MatRef& R2, int chi, const SvdParams& sp,
+                         ProjCache* cache) {
+  const int64_t N = R1.rows();
+  IPEPS_CHECK(R1.cols() == R2.rows() && R2.cols() == N, "get_projector: R1*R2 must be square");
+  IPEPS_CHECK(R1.t.dt == DType::F64 && R2.t.dt == DType::F64, "get_projector: real operands expected");
+  const int new_chi = int(std::min<int64_t>(chi, R1.cols()));
+  const int want = int(std::min<int64_t>(N, new_chi + 1));
+  int over = std::max(sp.min_oversample, want * sp.oversample_num / std::max(sp.oversample_den, 1));
+  const int k = int(std::min<int64_t>(N, int64_t(want) + over));
+
+  // sketch Omega (N x k): previous V of this direction first, then Gaussian columns
+  Tensor Om = c.alloc(DType::F64, {N, k});
+  randn(c, Om);
+  bool warm = false;
+  if (sp.warm_start && cache && !cache->V.empty() && cache->V.dims[0] == N) {
+    int nv = int(std::min<int64_t>(cache->V.dims[1], k));
+    IPEPS_CUDA(cudaMemcpyAsync(Om.data(), cache->V.data(), size_t(N) * nv * 8, cudaMemcpyDeviceToDevice, c.stream));
+    warm = true;
+  }
+  const int q = (k == N) ? 0 : (warm ? sp.power_iters_warm : sp.power_iters);
+
+  Tensor Y = apply(c, R1, 'N', apply(c, R2, 'N', Om));
+  for (int it = 0; it < q; ++it) {
+    Tensor Q = orth(c, Y, 2, nullptr);
+    Tensor Z = orth(c, apply(c, R2, 'T', apply(c, R1, 'T', Q)), 2, nullptr);
+    Y = apply(c, R1, 'N', apply(c, R2, 'N', Z));
+  }
+  Tensor Q = orth(c, Y, 3, nullptr);
+  // B^T = M^T Q (N x k);  B^T = Q2 R  =>  B = R^T Q2^T
+  Tensor Bt = apply(c, R2, 'T', apply(c, R1, 'T', Q));
+  Tensor Rm;
+  Tensor Q2 = orth(c, Bt, 3, &Rm);
+  // X = R^T ; one-sided Jacobi: X J = W = Ux S  =>  U = Q Ux, V = Q2 J
+  Tensor X = permute(c, Rm, {1, 0});
+  Tensor J = c.alloc(DType::F64, {k, k});
+  Tensor S = c.alloc(DType::F64, {k});
+  int* d_sweeps = reinterpret_cast<int*>(static_cast<char*>(c.scal->p) + 3900);
+  jacobi_svd(c, X.f64(), k, k, k, J.f64(), k, S.f64(), sp.jacobi_max_sweeps, sp.jacobi_tol, d_sweeps);
+  Tensor Ss = c.alloc(DType::F64, {k});
+  Tensor perm = c.alloc(DType::F64, {(k + 1) / 2});  // int storage
+  int* d_perm = static_cast<int*>(perm.data());
+  sort_desc(c, S.f64(), k, Ss.f64(), d_perm);
+
+  ProjResult r;
+  r.k = k;
+  r.s_host.resize(k);
+  int sweeps = 0;
+  IPEPS_CUDA(cudaMemcpyAsync(r.s_host.data(), Ss.data(), size_t(k) * 8, cudaMemcpyDeviceToHost, c.stream));
+  IPEPS_CUDA(cudaMemcpyAsync(&sweeps, d_sweeps, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+  c.sync();
+  r.sweeps = sweeps;
+
+  // cutoff_matrix (wrapper.jl:37-55)
+  const double smax = r.s_host[0];
+  int n_above = 0;
+  for (int i = 0; i < k; ++i)
+    if (smax > 0 && r.s_host[i] / smax > 1e-12) n_above++;
+  int n = std::min(new_chi, n_above);
+  IPEPS_CHECK(n >= 1, "get_projector: no singular value above the cutoff (zero enlarged corner?)");
+  // the reference's s has length N (full SVD); ours is the top-k part, k > n whenever N > n
+  if (int64_t(N) > n && k > n) {
+    if (std::fabs(r.s_host[n] - r.s_host[n - 1]) < 1e-10) n = n + 1;
+  }
+  IPEPS_CHECK(n <= k, "get_projector: truncation beyond the sketch");
+  r.n = n;
+  r.s_host.resize(n);
+
+  // Ux[:, j] = W[:, perm[j]] / S_sorted[j] ; Js[:, j] = J[:, perm[j]]
+  Tensor Ux = c.alloc(DType::F64, {k, n});
+  gather_cols(c, X.f64(), k, k, d_perm, n, Ss.f64(), 2, Ux.f64(), k);
+  Tensor Js = c.alloc(DType::F64, {k, n});
+  gather_cols(c, J.f64(), k, k, d_perm, n, nullptr, 0, Js.f64(), k);
+  Tensor U = c.alloc(DType::F64, {N, n});
+  gemm(c, DType::F64, 'N', 'N', N, n, k, cplx(1), Q.data(), N, Ux.data(), k, cplx(0), U.data(), N, true);
+  Tensor V = c.alloc(DType::F64, {N, n});
+  gemm(c, DType::F64, 'N', 'N', N, n, k, cplx(1), Q2.data(), N, Js.data(), k, cplx(0), V.data(), N, true);
+  if (cache) cache->V = clone(c, V);
+
+  r.S = c.alloc(DType::F64, {n});
+  IPEPS_CUDA(cudaMemcpyAsync(r.S.data(), Ss.data(), size_t(n) * 8, cudaMemcpyDeviceToDevice, c.stream));
+  // P1 = R2 V S^-1/2 ; P2 = S^-1/2 U^T R1
+  scale_cols(c, V.f64(), N, N, n, r.S.f64(), 1);
+  scale_cols(c, U.f64(), N, N, n, r.S.f64(), 1);
+  r.P1 = apply(c, R2, 'N', V);
+  r.P2 = apply_left_T(c, U, R1, 'N');
+  return r;
+}
+
+}  // namespace ipeps

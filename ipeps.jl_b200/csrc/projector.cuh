@@ -1,0 +1,57 @@
+// Truncated-SVD projector of the enlarged corners (ctmrg.jl:254-265 and
+// wrapper.jl:25-55), computed without forming R1*R2.
+#pragma once
+#include "ctx.cuh"
+
+namespace ipeps {
+
+// A logical matrix: t (2-D) or its transpose.
+struct MatRef {
+  Tensor t;
+  bool trans = false;
+  int64_t rows() const { return trans ? t.dims[1] : t.dims[0]; }
+  int64_t cols() const { return trans ? t.dims[0] : t.dims[1]; }
+};
+
+struct SvdParams {
+  int oversample_num = 1;   // k = want + max(min_oversample, want*num/den)
+  int oversample_den = 1;
+  int min_oversample = 16;
+  int power_iters = 4;      // cold start
+  int power_iters_warm = 2; // when the previous V of this direction seeds the sketch
+  bool warm_start = true;
+  int jacobi_max_sweeps = 40;
+  double jacobi_tol = 1e-15;
+};
+
+// Cache of the last right singular vectors of one direction (warm start).
+struct ProjCache {
+  Tensor V;  // N x n
+};
+
+struct ProjResult {
+  Tensor P1;  // N x n   (P  in the reference)
+  Tensor P2;  // n x N   (Pd in the reference)
+  Tensor S;   // n (device)
+  std::vector<double> s_host;  // n singular values, descending
+  int n = 0;
+  int k = 0;
+  int sweeps = 0;
+};
+
+// Returns P1 = R2 V S^-1/2, P2 = S^-1/2 U^T R1 with (U,S,V) the truncated
+// SVD of R1*R2 following wrap_svd/cutoff_matrix (keep min(chi, #{s/smax >
+// 1e-12}), plus one when |s[n+1]-s[n]| < 1e-10).
+ProjResult get_projector(Ctx& c, const MatRef& R1, const MatRef& R2, int chi, const SvdParams& sp,
+                         ProjCache* cache);
+
+// op(R)*X with R a MatRef; op in {'N','T'}
+Tensor apply(Ctx& c, const MatRef& R, char op, const Tensor& X);
+// X^T * op(R)   (returns X^T op(R))
+Tensor apply_left_T(Ctx& c, const Tensor& X, const MatRef& R, char op);
+
+// Orthonormalise the columns of Y (N x k) by shifted CholeskyQR; if Rout is
+// non-null it receives R with Y = Q R.
+Tensor orth(Ctx& c, const Tensor& Y, int passes, Tensor* Rout);
+
+}  // namespace ipeps

@@ -1,0 +1,467 @@
+"""Host side of the B200 CTMRG engine: the reference's Julia API, in Python.
+
+The names, argument meaning and defaults mirror iPEPS.jl (paths relative to
+its source tree):
+
+    CTMTensors(A, cfg)          src/ctm/ctm_tensor.jl:57-69 (init_ctm1 :97-130)
+    run_ctm(ts, conv_fun=...)   src/ctm/ctmrg.jl:1-55
+    rg_step(ts, chi)            src/ctm/ctmrg.jl:57-64
+    left_rg/right_rg/top_rg/bottom_rg   src/ctm/ctmrg.jl:66-120
+    get_gs_energy(ts, H)        src/graph/evaluation.jl:15-29
+    get_gs_norm(ts)             src/graph/evaluation.jl:47-59
+    compute_gs_energy(A, H, cfg) src/graph/evaluation.jl:1-13
+    get_es_energy(ts, H)        src/graph/evaluation.jl:31-45
+    get_all_norm(ts)            src/graph/evaluation.jl:61-77
+
+Every call goes through the C ABI of libipeps_b200.so (include/ipeps_b200.h);
+there is no CPU fallback: if the shared library is missing the import fails.
+Arrays are numpy arrays with Julia (column-major) semantics: shapes are the
+Julia shapes and data is passed in Fortran order.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import os
+from typing import Any, Dict, Optional
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libipeps_b200.so")
+
+OK, ENOTCONV, ENONFINITE, EOOM, EINVAL, ECUDA = range(6)
+PREC_FP64, PREC_MIXED = 0, 1
+CONV_ENERGY, CONV_SPECTRUM, CONV_ES = 0, 1, 2
+
+EXPORTED = [
+    "ipeps_ctx_create", "ipeps_ctx_destroy", "ipeps_last_error", "ipeps_ctx_set_precision",
+    "ipeps_ctx_set_seed", "ipeps_stats", "ipeps_stats_reset", "ipeps_env_create", "ipeps_env_destroy",
+    "ipeps_env_set_params", "ipeps_env_set_svd_params", "ipeps_env_set_A", "ipeps_env_init",
+    "ipeps_env_get_CT", "ipeps_env_set_CT", "ipeps_ctm_move", "ipeps_ctm_step", "ipeps_ctm_run",
+    "ipeps_ctm_log", "ipeps_energy", "ipeps_gs_norm", "ipeps_nested_set_B", "ipeps_es_energy",
+    "ipeps_all_norm", "ipeps_tcon", "ipeps_projector", "ipeps_ctx_stream", "ipeps_prof_enable",
+    "ipeps_prof_query",
+]
+
+
+class IPEPSError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[ipeps status {code}] {msg}")
+        self.code = code
+
+
+class Stats(ct.Structure):
+    _fields_ = [("launches", ct.c_uint64 * 8), ("flops", ct.c_double * 8), ("bytes", ct.c_double * 8),
+                ("moves", ct.c_uint64), ("move_seconds", ct.c_double)]
+
+    FAMILIES = ["permute", "gemm_f64", "gemm_tf32x3", "reduce", "elementwise", "small_linalg", "jacobi"]
+
+    def as_dict(self):
+        fam = {n: {"launches": int(self.launches[i]), "flops": float(self.flops[i]), "bytes": float(self.bytes[i])}
+               for i, n in enumerate(self.FAMILIES)}
+        return {"families": fam, "moves": int(self.moves), "move_seconds": float(self.move_seconds)}
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH) -> ct.CDLL:
+    """Load libipeps_b200.so and declare the C signatures (fails loudly when absent)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(f"libipeps_b200.so not found at {path}: build it with "
+                          "`python ipeps.jl_b200/build.py` (the engine has no CPU fallback)")
+    lib = ct.CDLL(path)
+    P, I, D, U64 = ct.c_void_p, ct.c_int, ct.c_double, ct.c_uint64
+    dp = ct.POINTER(ct.c_double)
+    ip = ct.POINTER(ct.c_int)
+    lp = ct.POINTER(ct.c_int64)
+    sig = {
+        "ipeps_ctx_create": [I, ct.POINTER(P)],
+        "ipeps_ctx_destroy": [P],
+        "ipeps_ctx_set_precision": [P, I],
+        "ipeps_ctx_set_seed": [P, U64],
+        "ipeps_stats": [P, ct.POINTER(Stats)],
+        "ipeps_stats_reset": [P],
+        "ipeps_env_create": [P, I, I, I, I, ct.POINTER(P)],
+        "ipeps_env_destroy": [P],
+        "ipeps_env_set_params": [P, I, I, I, I, D],
+        "ipeps_env_set_svd_params": [P, I, I, I, I, I, I],
+        "ipeps_env_set_A": [P, dp, dp],
+        "ipeps_env_init": [P],
+        "ipeps_env_get_CT": [P, I, dp, lp, dp, lp],
+        "ipeps_env_set_CT": [P, I, dp, lp, dp, lp],
+        "ipeps_ctm_move": [P, I, dp, ip],
+        "ipeps_ctm_step": [P, dp, ip],
+        "ipeps_ctm_run": [P, I, dp, dp, I, ip, dp, ip],
+        "ipeps_ctm_log": [P, dp, ip],
+        "ipeps_energy": [P, dp, dp, I, dp, dp],
+        "ipeps_gs_norm": [P, dp],
+        "ipeps_nested_set_B": [P, dp, D, D],
+        "ipeps_es_energy": [P, dp, dp, I, dp],
+        "ipeps_all_norm": [P, dp, dp],
+        "ipeps_tcon": [P, I, dp, I, lp, ip, dp, I, lp, ip, dp, ct.c_int64, lp, ip],
+        "ipeps_projector": [P, dp, dp, ct.c_int64, I, dp, dp, dp, ip],
+        "ipeps_ctx_stream": [P, ct.POINTER(P)],
+        "ipeps_prof_enable": [P, I],
+        "ipeps_prof_query": [P, dp, ct.POINTER(ct.c_uint64), dp, dp],
+    }
+    for name, args in sig.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = I
+    lib.ipeps_last_error.argtypes = [P]
+    lib.ipeps_last_error.restype = ct.c_char_p
+    _lib = lib
+    return lib
+
+
+def _dp(a: Optional[np.ndarray]):
+    if a is None:
+        return None
+    return a.ctypes.data_as(ct.POINTER(ct.c_double))
+
+
+def _fortran(a, dtype) -> np.ndarray:
+    return np.asfortranarray(np.asarray(a, dtype=dtype))
+
+
+class Engine:
+    """One device context (one CUDA stream).  Not thread-safe."""
+
+    def __init__(self, device: int = 0, precision: str = "fp64", seed: int = 0x1234ABCD):
+        self.lib = load_library()
+        h = ct.c_void_p()
+        st = self.lib.ipeps_ctx_create(int(device), ct.byref(h))
+        if st != OK:
+            raise IPEPSError(st, f"ipeps_ctx_create(device={device}) failed")
+        self.h = h
+        self.set_precision(precision)
+        self.check(self.lib.ipeps_ctx_set_seed(self.h, ct.c_uint64(seed)))
+
+    def check(self, st: int):
+        if st != OK:
+            msg = self.lib.ipeps_last_error(self.h)
+            raise IPEPSError(st, msg.decode() if msg else "")
+
+    def set_precision(self, precision: str):
+        p = {"fp64": PREC_FP64, "mixed": PREC_MIXED}[precision]
+        self.precision = precision
+        self.check(self.lib.ipeps_ctx_set_precision(self.h, p))
+
+    def stats(self) -> Dict[str, Any]:
+        s = Stats()
+        self.check(self.lib.ipeps_stats(self.h, ct.byref(s)))
+        return s.as_dict()
+
+    def stream_ptr(self) -> int:
+        """The engine's cudaStream_t as an int (for torch.cuda.ExternalStream)."""
+        p = ct.c_void_p()
+        self.check(self.lib.ipeps_ctx_stream(self.h, ct.byref(p)))
+        return int(p.value or 0)
+
+    def prof_enable(self, on: bool = True):
+        self.check(self.lib.ipeps_prof_enable(self.h, int(on)))
+
+    def prof_query(self) -> Dict[str, Dict[str, float]]:
+        ms = np.zeros(8)
+        fl = np.zeros(8)
+        by = np.zeros(8)
+        la = (ct.c_uint64 * 8)()
+        self.check(self.lib.ipeps_prof_query(self.h, _dp(ms), la, _dp(fl), _dp(by)))
+        return {n: {"ms": float(ms[i]), "launches": int(la[i]), "flops": float(fl[i]), "bytes": float(by[i])}
+                for i, n in enumerate(Stats.FAMILIES)}
+
+    def reset_stats(self):
+        self.check(self.lib.ipeps_stats_reset(self.h))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.ipeps_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_default_engine: Optional[Engine] = None
+
+
+def default_engine() -> Engine:
+    global _default_engine
+    if _default_engine is None:
+        _default_engine = Engine(int(os.environ.get("IPEPS_DEVICE", "0")))
+    return _default_engine
+
+
+def default_config() -> Dict[str, Any]:
+    """src/optimize/default_config.toml:1-49 (keys the hot path reads)."""
+    return {"gc": True, "dir": 0, "out_prefix": "test", "model": "test", "D": 2, "chi": 32,
+            "min_iter": 4, "max_iter": 20, "ad_max_iter": 4, "rg_tol": 1e-6, "resume": False,
+            "basis": False, "basis_t": "default", "basis_cut": 1e-3, "basis_name": 0,
+            "es_resume": 1, "es_num": 0, "ad": True, "save": True, "part_save": False,
+            "nrmB_cut": 1e-3, "wp": 1}
+
+
+def _H_pair(H):
+    hs = [_fortran(h, np.complex128) for h in H]
+    d2 = hs[0].shape[0]
+    return hs[0], hs[1], d2
+
+
+class CTMTensors:
+    """Environment state on the device (ctm_tensor.jl:3-18).
+
+    ``CTMTensors(A, cfg)`` sets Ad = conj(A) and runs init_ctm1, like the
+    reference constructor.  The Params dict is ``self.Params``; keys chi,
+    min_iter, max_iter, ad_max_iter, rg_tol are pushed to the device before
+    every run/step.  Extra keys (not read by the reference): ``svd_oversample``
+    (num, den, min), ``svd_power_iters`` (cold, warm), ``svd_warm_start``.
+    """
+
+    def __init__(self, A, cfg: Optional[Dict[str, Any]] = None, Ad=None, engine: Optional[Engine] = None,
+                 init: bool = True):
+        self.engine = engine or default_engine()
+        self.lib = self.engine.lib
+        A = np.asarray(A)
+        self.is_complex = np.iscomplexobj(A) or (Ad is not None and np.iscomplexobj(Ad))
+        self.dtype = np.complex128 if self.is_complex else np.float64
+        self.D, self.d = int(A.shape[0]), int(A.shape[4])
+        self.Params = dict(default_config() if cfg is None else cfg)
+        h = ct.c_void_p()
+        self.engine.check(self.lib.ipeps_env_create(self.engine.h, self.D, self.d, int(self.Params.get("chi", 30)),
+                                                    int(self.is_complex), ct.byref(h)))
+        self.h = h
+        self._push_params()
+        self.set_A(A, Ad)
+        if init:
+            self.engine.check(self.lib.ipeps_env_init(self.h))
+        self.B = None
+
+    # -------------------------------------------------------------- state
+    def set_A(self, A, Ad=None):
+        self._A = _fortran(A, self.dtype)
+        self._Ad = None if Ad is None else _fortran(Ad, self.dtype)
+        self.engine.check(self.lib.ipeps_env_set_A(self.h, _dp(self._A), _dp(self._Ad)))
+
+    @property
+    def A(self):
+        return self._A
+
+    @property
+    def Ad(self):
+        return np.conj(self._A) if self._Ad is None else self._Ad
+
+    def _push_params(self):
+        p = self.Params
+        self.engine.check(self.lib.ipeps_env_set_params(
+            self.h, int(p.get("chi", 30)), int(p.get("min_iter", 4)), int(p.get("max_iter", 20)),
+            int(p.get("ad_max_iter", 4)), float(p.get("rg_tol", 1e-6))))
+        over = p.get("svd_oversample", (1, 1, 16))
+        pit = p.get("svd_power_iters", (4, 2))
+        self.engine.check(self.lib.ipeps_env_set_svd_params(
+            self.h, int(over[0]), int(over[1]), int(over[2]), int(pit[0]), int(pit[1]),
+            int(bool(p.get("svd_warm_start", True)))))
+
+    def get_CT(self, k: int):
+        """(C_k, E_k) as column-major numpy arrays, k = 1..4."""
+        cd = (ct.c_int64 * 2)()
+        ed = (ct.c_int64 * 4)()
+        self.engine.check(self.lib.ipeps_env_get_CT(self.h, k, None, cd, None, ed))
+        C = np.empty(tuple(cd), dtype=self.dtype, order="F")
+        E = np.empty(tuple(ed), dtype=self.dtype, order="F")
+        self.engine.check(self.lib.ipeps_env_get_CT(self.h, k, _dp(C), cd, _dp(E), ed))
+        return C, E
+
+    def set_CT(self, k: int, C, E):
+        C = _fortran(C, self.dtype)
+        E = _fortran(E, self.dtype)
+        cd = (ct.c_int64 * 2)(*C.shape)
+        ed = (ct.c_int64 * 4)(*E.shape)
+        self.engine.check(self.lib.ipeps_env_set_CT(self.h, k, _dp(C), cd, _dp(E), ed))
+
+    @property
+    def Cs(self):
+        return [self.get_CT(k)[0] for k in range(1, 5)]
+
+    @property
+    def Es(self):
+        return [self.get_CT(k)[1] for k in range(1, 5)]
+
+    def set_B(self, B, px: float, py: float):
+        """setproperties(ts, B=B, Bd=conj(B)) with Params px, py (optim_es.jl:124-125,171)."""
+        self.B = _fortran(B, np.complex128)
+        self.Params["px"], self.Params["py"] = float(px), float(py)
+        self.engine.check(self.lib.ipeps_nested_set_B(self.h, _dp(self.B), float(px), float(py)))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.ipeps_env_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def tcon(xs, ind_xs, engine: Optional[Engine] = None):
+    """``tcon(xs, ind_xs)`` (wrapper.jl:15-23) on the device: positive labels
+    are summed, negative labels -1, -2, ... give the output order."""
+    eng = engine or default_engine()
+    A, B = xs
+    la, lb = ind_xs
+    cplx = np.iscomplexobj(A) or np.iscomplexobj(B)
+    dt = np.complex128 if cplx else np.float64
+    A = _fortran(A, dt)
+    B = _fortran(B, dt)
+    ext = {}
+    for l, n in zip(la, A.shape):
+        ext[l] = n
+    for l, n in zip(lb, B.shape):
+        ext[l] = n
+    nout = sum(1 for l in list(la) + list(lb) if l < 0)
+    oshape = tuple(ext[-(i + 1)] for i in range(nout))
+    out = np.empty(oshape, dtype=dt, order="F")
+    od = (ct.c_int64 * 16)()
+    ond = ct.c_int(0)
+    dA = (ct.c_int64 * max(1, A.ndim))(*A.shape)
+    dB = (ct.c_int64 * max(1, B.ndim))(*B.shape)
+    lA = (ct.c_int * max(1, len(la)))(*la)
+    lB = (ct.c_int * max(1, len(lb)))(*lb)
+    eng.check(eng.lib.ipeps_tcon(eng.h, int(cplx), _dp(A), A.ndim, dA, lA, _dp(B), B.ndim, dB, lB, _dp(out),
+                                 int(max(out.size, 1)), od, ct.byref(ond)))
+    return out
+
+
+def get_projector(R1, R2, chi: int, engine: Optional[Engine] = None):
+    """get_projector(R1, R2, chi) (ctmrg.jl:254-265) on the device: (P1, P2, S)."""
+    eng = engine or default_engine()
+    R1 = _fortran(R1, np.float64)
+    R2 = _fortran(R2, np.float64)
+    N = R1.shape[0]
+    P1 = np.empty(N * (chi + 1))
+    P2 = np.empty(N * (chi + 1))
+    s = np.empty(chi + 1)
+    n = ct.c_int(0)
+    eng.check(eng.lib.ipeps_projector(eng.h, _dp(R1), _dp(R2), N, int(chi), _dp(P1), _dp(P2), _dp(s), ct.byref(n)))
+    k = n.value
+    return (P1[: N * k].reshape((N, k), order="F"), P2[: N * k].reshape((k, N), order="F"), s[:k].copy())
+
+
+# ------------------------------------------------------------------ moves
+def _spectrum_call(ts, fn, *args):
+    n = ct.c_int(4096)
+    buf = np.empty(4096, dtype=np.float64)
+    ts.engine.check(fn(ts.h, *args, _dp(buf), ct.byref(n)))
+    return buf[: n.value].copy()
+
+
+def rg_step(ts: CTMTensors, chi: Optional[int] = None):
+    """ctmrg.jl:57-64: returns (ts, s) with s the left-move spectrum."""
+    if chi is not None:
+        ts.Params["chi"] = int(chi)
+    ts._push_params()
+    return ts, _spectrum_call(ts, ts.lib.ipeps_ctm_step)
+
+
+def _move(ts, chi, d):
+    if chi is not None:
+        ts.Params["chi"] = int(chi)
+    ts._push_params()
+    return ts, _spectrum_call(ts, ts.lib.ipeps_ctm_move, d)
+
+
+def left_rg(ts, chi=None):
+    """ctmrg.jl:66-78"""
+    return _move(ts, chi, 0)
+
+
+def right_rg(ts, chi=None):
+    """ctmrg.jl:80-92"""
+    return _move(ts, chi, 1)
+
+
+def top_rg(ts, chi=None):
+    """ctmrg.jl:94-106"""
+    return _move(ts, chi, 2)
+
+
+def bottom_rg(ts, chi=None):
+    """ctmrg.jl:108-120"""
+    return _move(ts, chi, 3)
+
+
+def run_ctm(ts: CTMTensors, conv_fun: Optional[str] = None, H=None):
+    """ctmrg.jl:1-55.
+
+    ``conv_fun`` selects the reference's convergence criterion: None (left
+    spectrum), "energy" (get_gs_energy, as in optim_gs / compute_gs_energy) or
+    "es" (get_es_energy / get_all_norm, as in optim_es).  Returns (ts, info)
+    with info = {"iters", "diff", "converged", "log"}.
+    """
+    ts._push_params()
+    mode = {None: CONV_SPECTRUM, "spectrum": CONV_SPECTRUM, "energy": CONV_ENERGY, "es": CONV_ES}[conv_fun]
+    if mode != CONV_SPECTRUM:
+        Hh, Hv, d2 = _H_pair(H)
+    else:
+        Hh = Hv = None
+        d2 = 0
+    iters, conv = ct.c_int(0), ct.c_int(0)
+    diff = ct.c_double(0)
+    ts.engine.check(ts.lib.ipeps_ctm_run(ts.h, mode, _dp(Hh), _dp(Hv), d2, ct.byref(iters), ct.byref(diff),
+                                         ct.byref(conv)))
+    n = ct.c_int(100000)
+    log = np.empty((100000, 4))
+    ts.engine.check(ts.lib.ipeps_ctm_log(ts.h, _dp(log), ct.byref(n)))
+    info = {"iters": iters.value, "diff": diff.value, "converged": bool(conv.value),
+            "log": [{"iter": i + 1, "diff": float(r[0]), "obj": complex(r[1], r[2]), "chi": int(r[3])}
+                    for i, r in enumerate(log[: n.value])]}
+    return ts, info
+
+
+# ------------------------------------------------------------ observables
+def get_gs_energy(ts: CTMTensors, H):
+    """evaluation.jl:15-29: returns (E, Na) as complex numbers."""
+    Hh, Hv, d2 = _H_pair(H)
+    E = np.zeros(2)
+    Na = np.zeros(2)
+    ts.engine.check(ts.lib.ipeps_energy(ts.h, _dp(Hh), _dp(Hv), d2, _dp(E), _dp(Na)))
+    return complex(E[0], E[1]), complex(Na[0], Na[1])
+
+
+def get_gs_norm(ts: CTMTensors):
+    """evaluation.jl:47-59"""
+    out = np.zeros(2)
+    ts.engine.check(ts.lib.ipeps_gs_norm(ts.h, _dp(out)))
+    return complex(out[0], out[1])
+
+
+def get_es_energy(ts: CTMTensors, H) -> float:
+    """evaluation.jl:31-45"""
+    Hh, Hv, d2 = _H_pair(H)
+    out = np.zeros(1)
+    ts.engine.check(ts.lib.ipeps_es_energy(ts.h, _dp(Hh), _dp(Hv), d2, _dp(out)))
+    return float(out[0])
+
+
+def get_all_norm(ts: CTMTensors):
+    """evaluation.jl:61-77: returns (Nb, envB)."""
+    nb = np.zeros(2)
+    envB = np.empty(ts.A.shape, dtype=np.complex128, order="F")
+    ts.engine.check(ts.lib.ipeps_all_norm(ts.h, _dp(nb), _dp(envB)))
+    return complex(nb[0], nb[1]), envB
+
+
+def compute_gs_energy(A, H, cfg, engine: Optional[Engine] = None):
+    """evaluation.jl:1-13: converge from init_ctm1 with the energy criterion."""
+    ts = CTMTensors(A, cfg, engine=engine)
+    ts, info = run_ctm(ts, conv_fun="energy", H=H)
+    E, Na = get_gs_energy(ts, H)
+    return (E, Na), ts, info

@@ -1,0 +1,46 @@
+"""Generate tests/golden/ctm_energies.json from the CPU oracle.
+
+The reference (Julia) cannot run in this environment, so the golden energies
+of seeded synthetic cases come from the oracle, which is itself pinned to the
+reference's honeycomb known-answer test.  Inputs are regenerated from seeds
+(numpy default_rng, N(0,1), max|A| = 1, column-major).
+
+Usage: python tests/golden/make_golden.py
+"""
+import json
+import os
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(HERE, "..", "..", "oracle"))
+import ipeps_oracle as O  # noqa: E402
+
+CASES = [
+    dict(model="ising", h=2.0, Jz=None, D=2, d=2, chi=16, seed=0, min_iter=4, max_iter=30, rg_tol=1e-10),
+    dict(model="heisenberg", h=None, Jz=1.0, D=2, d=2, chi=12, seed=3, min_iter=4, max_iter=30, rg_tol=1e-10),
+    dict(model="ising", h=2.0, Jz=None, D=2, d=2, chi=30, seed=0, min_iter=4, max_iter=30, rg_tol=1e-6),
+    dict(model="heisenberg", h=None, Jz=1.0, D=3, d=2, chi=27, seed=1, min_iter=4, max_iter=30, rg_tol=1e-11),
+]
+
+
+def main():
+    out = []
+    for c in CASES:
+        A = O.random_A(c["D"], c["d"], seed=c["seed"])
+        H = O.ising(c["h"]) if c["model"] == "ising" else O.heisenberg(c["Jz"])
+        cfg = O.default_config()
+        cfg.update(chi=c["chi"], min_iter=c["min_iter"], max_iter=c["max_iter"], rg_tol=c["rg_tol"])
+        log = []
+        e0, _ = O.compute_gs_energy(A, H, cfg, log=log)
+        c = dict(c)
+        c["E"] = complex(e0).real
+        c["iters"] = len(log)
+        c["chi_final"] = log[-1]["chi"]
+        out.append(c)
+        print(c)
+    with open(os.path.join(HERE, "ctm_energies.json"), "w") as f:
+        json.dump({"generator": "tests/golden/make_golden.py (CPU oracle, torch float64)", "cases": out}, f, indent=1)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,155 @@
+"""GPU parity of the CTMRG engine (through the C ABI) against the CPU oracle.
+
+Bars (FP64 form):
+  * contraction operator and init_ctm1: 1e-12 relative (same FP64 sums, different order)
+  * projector singular values: 1e-10 relative for the leading ones;
+    gauge-invariant P1*P2 to 1e-8 relative
+  * converged energy per site: |dE| <= 1e-10 absolute
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+import torch
+
+import ipeps_oracle as O
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def npa(t):
+    return t.detach().numpy() if isinstance(t, torch.Tensor) else np.asarray(t)
+
+
+@pytest.mark.parametrize("cplx", [False, True])
+def test_tcon_random_labels(engine, pkg, cplx):
+    rng = np.random.default_rng(7)
+    cases = [
+        ([[1, 2, -1, -2], [1, 2, -3]], [(5, 4, 3, 6), (5, 4, 7)]),
+        ([[-2, 1], [1, -1, -3, -4]], [(6, 5), (5, 7, 3, 2)]),
+        ([[-1, -4, 1, 2, -2, -5, 3], [1, 2, -3, -6, 3]], [(4, 3, 2, 2, 3, 3, 2), (2, 2, 3, 3, 2)]),
+        ([[1, 2, 3, 4, -1, -3], [1, 2, 3, 4, -2, -4]], [(3, 4, 2, 2, 2, 2), (3, 4, 2, 2, 2, 2)]),
+        ([[1, 2, 3, 4, 5], [1, 2, 3, 4, 5]], [(2, 3, 2, 3, 2), (2, 3, 2, 3, 2)]),
+        ([[-1, 1, -2, -3], [1, -4, -5, -6]], [(7, 5, 2, 2), (5, 6, 2, 2)]),
+    ]
+    for labels, shapes in cases:
+        def mk(s):
+            x = rng.standard_normal(s)
+            if cplx:
+                x = x + 1j * rng.standard_normal(s)
+            return x
+        A, B = mk(shapes[0]), mk(shapes[1])
+        ref = npa(O.tcon([torch.tensor(A), torch.tensor(B)], labels))
+        got = pkg.tcon([A, B], labels, engine=engine)
+        assert got.shape == ref.shape
+        assert np.allclose(got, ref, rtol=1e-12, atol=1e-12 * np.abs(ref).max())
+
+
+def test_gemm_large_tcon(engine, pkg):
+    """Large matrix-shaped contractions exercise both GEMM tilings and split-K."""
+    rng = np.random.default_rng(3)
+    for (m, k, n) in [(300, 700, 260), (40, 5000, 30), (1000, 64, 900)]:
+        A = rng.standard_normal((m, k))
+        B = rng.standard_normal((k, n))
+        got = pkg.tcon([A, B], [[-1, 1], [1, -2]], engine=engine)
+        assert np.allclose(got, A @ B, rtol=1e-12, atol=1e-11 * np.sqrt(k))
+        got = pkg.tcon([A, B.T.copy()], [[-1, 1], [-2, 1]], engine=engine)
+        assert np.allclose(got, A @ B, rtol=1e-12, atol=1e-11 * np.sqrt(k))
+
+
+def test_projector_matches_oracle(engine, pkg):
+    rng = np.random.default_rng(11)
+    N, chi = 120, 30
+    # decaying spectrum like an enlarged corner
+    U, _ = np.linalg.qr(rng.standard_normal((N, N)))
+    V, _ = np.linalg.qr(rng.standard_normal((N, N)))
+    s = np.exp(-0.35 * np.arange(N))
+    R1 = U @ np.diag(np.sqrt(s)) @ rng.standard_normal((N, N)) * 0.1
+    R2 = np.linalg.solve(rng.standard_normal((N, N)) * 0.1, np.diag(np.sqrt(s)) @ V.T)
+    P1o, P2o, So = O.get_projector(torch.tensor(R1), torch.tensor(R2), chi)
+    P1, P2, S = pkg.get_projector(R1, R2, chi, engine=engine)
+    So = npa(So)
+    assert len(S) == len(So)
+    lead = min(10, len(S))
+    assert np.allclose(S[:lead], So[:lead], rtol=1e-10)
+    Po = npa(P1o) @ npa(P2o)
+    Pg = P1 @ P2
+    assert np.linalg.norm(Pg - Po) <= 1e-8 * np.linalg.norm(Po)
+
+
+def _oracle_ts_after_init(A, cfg):
+    return O.make_ctm_tensors(torch.tensor(A), cfg)
+
+
+def test_init_ctm1_matches(engine, pkg):
+    A = npa(O.random_A(3, 2, seed=5))
+    cfg = O.default_config()
+    ts_o = _oracle_ts_after_init(A, cfg)
+    ts = pkg.CTMTensors(A, cfg, engine=engine)
+    for k in range(4):
+        C, E = ts.get_CT(k + 1)
+        assert np.allclose(C, npa(ts_o.Cs[k]), rtol=1e-13, atol=1e-14)
+        assert np.allclose(E, npa(ts_o.Es[k]), rtol=1e-13, atol=1e-14)
+
+
+def test_single_move_spectra(engine, pkg):
+    A = npa(O.random_A(2, 2, seed=2))
+    cfg = O.default_config()
+    cfg.update(chi=12)
+    ts_o = _oracle_ts_after_init(A, cfg)
+    ts = pkg.CTMTensors(A, cfg, engine=engine)
+    for it in range(3):
+        for d, (fo, fg) in enumerate([(O.left_rg, pkg.left_rg), (O.right_rg, pkg.right_rg),
+                                       (O.top_rg, pkg.top_rg), (O.bottom_rg, pkg.bottom_rg)]):
+            ts_o, so = fo(ts_o, 12)
+            ts, sg = fg(ts, 12)
+            so = npa(so)
+            assert len(sg) == len(so), (it, d)
+            lead = min(8, len(so))
+            assert np.allclose(sg[:lead], so[:lead], rtol=1e-10), (it, d, sg[:lead], so[:lead])
+
+
+@pytest.mark.parametrize("idx", [0, 1, 3])
+def test_converged_energy_matches_golden(engine, pkg, idx):
+    with open(os.path.join(GOLD, "ctm_energies.json")) as f:
+        case = json.load(f)["cases"][idx]
+    A = npa(O.random_A(case["D"], case["d"], seed=case["seed"]))
+    H = O.ising(case["h"]) if case["model"] == "ising" else O.heisenberg(case["Jz"])
+    H = [npa(h) for h in H]
+    cfg = O.default_config()
+    cfg.update(chi=case["chi"], min_iter=case["min_iter"], max_iter=case["max_iter"], rg_tol=case["rg_tol"])
+    (E, Na), ts, info = pkg.compute_gs_energy(A, H, cfg, engine=engine)
+    assert abs(E.real - case["E"]) <= 1e-10, (E, case["E"])
+    assert info["log"][-1]["chi"] == case["chi_final"]
+
+
+def test_nested_energy_and_norm(engine, pkg):
+    """A few nested (excited-state) iterations: get_es_energy and get_all_norm."""
+    D, chi = 2, 8
+    A = O.random_A(D, 2, seed=4)
+    H = O.heisenberg(1.0)
+    cfg = O.default_config()
+    cfg.update(chi=chi, min_iter=1, max_iter=3, rg_tol=0.0)
+    ts_o = O.make_ctm_tensors(A, cfg)
+    ts_o, _ = O.run_ctm(ts_o)
+    g = np.random.default_rng(9)
+    B = g.standard_normal(A.shape) + 1j * g.standard_normal(A.shape)
+    px, py = 0.5 * np.pi, 0.25 * np.pi
+    ts_o.Params.update(px=px, py=py, max_iter=2)
+    ts_o = ts_o.replace(B=torch.tensor(B), Bd=torch.tensor(B).conj())
+    ts_o, _ = O.run_ctm(ts_o)
+    Eo = O.get_es_energy(ts_o, H).item()
+    Nbo, envBo = O.get_all_norm(ts_o)
+
+    ts = pkg.CTMTensors(npa(A), cfg, engine=engine)
+    pkg.run_ctm(ts)
+    ts.Params["max_iter"] = 2
+    ts.set_B(B, px, py)
+    pkg.run_ctm(ts)
+    E = pkg.get_es_energy(ts, [npa(h) for h in H])
+    Nb, envB = pkg.get_all_norm(ts)
+    assert abs(E - Eo) <= 1e-9 * max(1.0, abs(Eo))
+    assert abs(Nb - complex(Nbo.item())) <= 1e-9 * max(1.0, abs(complex(Nbo.item())))
+    assert np.allclose(envB, npa(envBo), rtol=1e-8, atol=1e-10 * np.abs(npa(envBo)).max())
