@@ -1,0 +1,393 @@
+"""Benchmark of the CTMRG hot path on B200.
+
+Workload (default): spin-1/2 Heisenberg (sublattice-rotated), single-site
+iPEPS A of shape (4,4,4,4,2), i.i.d. N(0,1) seeded, max|A| = 1, chi = 64;
+one step = init_ctm1 + 30 CTMRG iterations (4 directional moves each) with the
+energy evaluated every iteration (the reference's conv_fun), i.e. 120 moves.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|mixed]
+    python bench.py --impl reference ...   # CPU arm (see below)
+
+Timing: K steps timed with CUDA events recorded on the engine's own stream,
+L2 flushed (512 MB write) between steps, max over ranks; value = moves/s of the
+whole job.  e2e = the same metric through the public API with host buffers
+(A and H copied in, energy copied out, inside the timed region).
+
+Reference arm: the reference is Julia, which is not installed, so
+``--impl reference`` times the CPU FP64 oracle (a restatement of the
+reference's algorithm) on the host cores, on a bounded sample of the same
+workload.  It is the CPU baseline, not a target.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG_DIR = os.path.join(ROOT, "ipeps.jl_b200")
+
+
+def load_pkg():
+    if "ipeps_b200" in sys.modules:
+        return sys.modules["ipeps_b200"]
+    spec = importlib.util.spec_from_file_location("ipeps_b200", os.path.join(PKG_DIR, "__init__.py"),
+                                                  submodule_search_locations=[PKG_DIR])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["ipeps_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+# ---------------------------------------------------------------- inputs
+def random_A(D, d, seed):
+    """N(0,1) from numpy default_rng, column-major (Julia) order, max|A| = 1."""
+    rng = np.random.default_rng(seed)
+    A = rng.standard_normal(D ** 4 * d).reshape((D, D, D, D, d), order="F")
+    return np.asfortranarray(A / np.abs(A).max())
+
+
+def tout(a, b):
+    """basis.jl:16-21: reshape(tcon([a,b], [[-1,-3],[-2,-4]]), d1*d2, d3*d4) (column-major)."""
+    c = np.einsum("ac,bd->abcd", a, b)
+    s = c.shape
+    return c.reshape((s[0] * s[1], s[2] * s[3]), order="F")
+
+
+def heisenberg(Jz=1.0):
+    """basis.jl:31-35"""
+    Sx = np.array([[0, 1], [1, 0]]) / 2
+    Sy = np.array([[0, -1j], [1j, 0]]) / 2
+    Sz = np.array([[1, 0], [0, -1]]) / 2
+    H = Jz * tout(Sz, Sz) - tout(Sx, Sx) - tout(Sy, Sy)
+    H = np.asfortranarray(H.astype(np.complex128))
+    return [H, H]
+
+
+WORKLOAD = dict(model="heisenberg", D=4, d=2, chi=64, iters=30)
+
+
+def workload_cfg(pkg, chi, iters):
+    cfg = pkg.default_config()
+    cfg.update(chi=chi, min_iter=iters, max_iter=iters, rg_tol=0.0)
+    return cfg
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ["index", "clocks.sm", "clocks.max.sm", "power.draw", "clocks_event_reasons.active",
+              "clocks_event_reasons.hw_slowdown", "clocks_event_reasons.hw_thermal_slowdown",
+              "clocks_event_reasons.sw_thermal_slowdown", "clocks_event_reasons.sw_power_cap"]
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.samples = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + ",".join(self.FIELDS),
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) == len(self.FIELDS):
+                self.samples.append(parts)
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        if not self.samples:
+            return None
+        mhz = []
+        maxmhz = 0.0
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for s in self.samples:
+            try:
+                mhz.append(float(s[1]))
+                maxmhz = max(maxmhz, float(s[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, s[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(mhz) if mhz else None, "sm_max_mhz": maxmhz or None,
+                "reasons": sorted(reasons), "samples": len(self.samples)}
+
+
+# ---------------------------------------------------------------- helpers
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+def measure_fp64_peak(torch):
+    """cuBLAS DGEMM (torch.matmul float64, 8192^3) on this GPU: the FP64 roofline denominator."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 1e30
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        torch.cuda.synchronize()
+        best = min(best, s.elapsed_time(e) / 1e3)
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / best / 1e12
+
+
+def cpu_oracle_sample(D, d, chi, seed, budget_s=15.0, threads=None):
+    """Time the CPU oracle on a bounded sample of the workload: init_ctm1 + as
+    many CTMRG iterations (with the energy) as fit in ~budget_s.  Returns moves/s."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import torch
+    import ipeps_oracle as O
+    if threads:
+        torch.set_num_threads(threads)
+    A = torch.tensor(random_A(D, d, seed))
+    H = O.heisenberg(1.0)
+    cfg = O.default_config()
+    cfg.update(chi=chi, min_iter=1, max_iter=1, rg_tol=0.0)
+    ts = O.make_ctm_tensors(A, cfg)
+    moves = 0
+    # first iterations have small chi: run two untimed to reach the full bond dimension
+    for _ in range(2):
+        ts, _ = O.rg_step(ts, chi)
+    t0 = time.perf_counter()
+    while True:
+        ts, _ = O.rg_step(ts, chi)
+        O.get_gs_energy(ts, H)
+        moves += 4
+        if time.perf_counter() - t0 > budget_s:
+            break
+    dt = time.perf_counter() - t0
+    return moves / dt, moves, dt, torch.get_num_threads()
+
+
+# ---------------------------------------------------------------- arms
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    D, d, chi = WORKLOAD["D"], WORKLOAD["d"], WORKLOAD["chi"]
+    threads = os.cpu_count() or 1
+    per_step = []
+    total_moves = 0
+    total_t = 0.0
+    for i in range(args.warmup + args.steps):
+        v, moves, dt, nth = cpu_oracle_sample(D, d, chi, seed=1000 + i, budget_s=args.ref_budget, threads=threads)
+        if i >= args.warmup:
+            per_step.append(dt)
+            total_moves += moves
+            total_t += dt
+    value = total_moves / total_t
+    sample = (f"CPU oracle (torch float64, {nth} threads): init_ctm1 + 2 untimed iterations, then CTMRG "
+              f"iterations with the energy for ~{args.ref_budget:.0f} s per step")
+    line = {"impl": "reference", "metric": "CTMRG moves/s (Heisenberg D=4 chi=64, FP64)", "value": value,
+            "unit": "moves/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * total_t / max(args.steps, 1), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "heisenberg D=4 d=2 chi=64: CTMRG iterations from init_ctm1", "D": D,
+                       "chi": chi, "sample": "bounded CPU sample, see cpu_baseline"},
+            "cpu_baseline": {"value": value, "unit": "moves/s", "cores": nth, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": "moves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "reference_note": "iPEPS.jl is Julia; no Julia toolchain on this machine, so the CPU arm is the "
+                              "oracle restatement of its algorithm"}
+    print(json.dumps(line))
+    return 0
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+
+    pkg = load_pkg()
+    eng = pkg.Engine(local, precision=args.precision)
+    D, d, chi, iters = WORKLOAD["D"], WORKLOAD["d"], WORKLOAD["chi"], WORKLOAD["iters"]
+    cfg = workload_cfg(pkg, chi, iters)
+    H = heisenberg(1.0)
+    A = random_A(D, d, seed=1000 + rank)
+    moves_per_step = 4 * iters
+
+    ext = torch.cuda.ExternalStream(eng.stream_ptr())
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    ts = pkg.CTMTensors(A, cfg, engine=eng)
+
+    def device_step():
+        # inputs resident: A already on the device; re-initialise and iterate
+        eng.check(eng.lib.ipeps_env_init(ts.h))
+        pkg.run_ctm(ts, conv_fun="energy", H=H)
+
+    for _ in range(args.warmup):
+        device_step()
+    barrier()
+
+    # ---- timed region (device): K steps, events on the engine stream, L2 flushed between steps
+    eng.reset_stats()
+    sampler = ClockSampler(local)
+    sampler.start()
+    times = []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(ext)
+        device_step()
+        e.record(ext)
+        e.synchronize()
+        times.append(s.elapsed_time(e) / 1e3)
+    barrier()
+    clocks = sampler.stop()
+    st = eng.stats()
+    launches = sum(f["launches"] for f in st["families"].values())
+    t_local = sum(times)
+    t_max = t_local
+    if world > 1:
+        tt = torch.tensor([t_local], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_max = float(tt.item())
+    total_moves = moves_per_step * args.steps * world
+    value = total_moves / t_max
+
+    # ---- e2e: public API with host buffers (A, H in; energy out) each step
+    e2e_times = []
+    for _ in range(max(1, args.steps)):
+        flush.zero_()
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(ext)
+        (E, Na), ts2, info = pkg.compute_gs_energy(A, H, cfg, engine=eng)
+        e.record(ext)
+        e.synchronize()
+        e2e_times.append(s.elapsed_time(e) / 1e3)
+        ts2.close()
+    barrier()
+    te = sum(e2e_times)
+    if world > 1:
+        tt = torch.tensor([te], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        te = float(tt.item())
+    e2e_value = moves_per_step * len(e2e_times) * world / te
+    h2d = A.nbytes + 2 * H[0].nbytes * (iters + 2)   # A once, H per energy call
+    d2h = 16 * 2 * (iters + 1) + 8 * 4 * chi * iters  # energies + left spectra
+
+    # ---- live per-kernel roofline: one profiled step (events around each launch)
+    eng.prof_enable(True)
+    device_step()
+    prof = eng.prof_query()
+    eng.prof_enable(False)
+
+    out = None
+    if rank == 0:
+        peaks, peak_kind = measured_peaks()
+        fp64_peak = measure_fp64_peak(torch)
+        g = prof["gemm_f64"] if args.precision == "fp64" else prof["gemm_tf32x3"]
+        achieved = g["flops"] / (g["ms"] / 1e3) / 1e12 if g["ms"] > 0 else 0.0
+        if args.precision == "fp64":
+            peak, peak_note = fp64_peak, "cuBLAS DGEMM 8192^3 measured in this run (FP64 has no entry in MEASURED_PEAKS.json)"
+        else:
+            peak, peak_note = peaks["bf16_tflops"] / 2 / 3, f"{peak_kind} bf16 / 2 (TF32) / 3 (three products)"
+        total_ms = sum(f["ms"] for f in prof.values())
+        cpu = None
+        if not args.no_cpu_baseline:
+            v, moves, dt, nth = cpu_oracle_sample(D, d, chi, seed=1000, budget_s=args.cpu_budget, threads=os.cpu_count())
+            cpu = {"value": v, "unit": "moves/s", "cores": nth, "kind": "port",
+                   "sample": f"CPU oracle (torch float64): {moves} moves of the same workload in {dt:.1f} s "
+                             f"after 2 untimed iterations"}
+        out = {
+            "metric": "CTMRG moves/s (Heisenberg D=4 chi=64; E+grad evals/s reported separately when built)",
+            "value": value, "unit": "moves/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f64 (3xTF32 contractions)",
+            "data": "synthetic",
+            "config": {"workload": "heisenberg D=4 d=2 chi=64: init_ctm1 + 30 CTMRG iterations with the energy "
+                                   "per iteration (120 moves per step)",
+                       "precision": args.precision, "l2": "flushed between steps (512 MB write)",
+                       "replicas": world},
+            "e2e": {"value": e2e_value, "unit": "moves/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "tensor" if args.precision == "mixed" else "fp64",
+                         "kernel": "gemm_f64 (register-tiled DFMA)" if args.precision == "fp64" else "gemm_tf32x3",
+                         "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak if peak else None, "traffic": None,
+                         "peak_source": peak_note, "kernel_share_of_device_time": g["ms"] / total_ms if total_ms else None,
+                         "launches_in_profiled_step": g["launches"]},
+            "kernel_families_ms_profiled_step": {k: round(v["ms"], 3) for k, v in prof.items()},
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+            "energy_last": [E.real, E.imag],
+        }
+        print(json.dumps(out))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--ref-budget", type=float, default=10.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())
