@@ -26,12 +26,18 @@ int guarded(ipeps_ctx* ctx, F&& f) {
   if (!ctx) return IPEPS_EINVAL;
   try {
     ctx->err.clear();
+    if (ctx->c) IPEPS_CUDA(cudaMemsetAsync(ctx->c->d_status, 0, sizeof(int), ctx->c->stream));
     int st = f();
     if (ctx->c) {
+      // status bits: 2 non-finite value, 4 Jacobi sweep cap hit, 8 tensor-core pipeline wait timed out
       int dev_status = 0;
-      cudaMemcpyAsync(&dev_status, ctx->c->d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx->c->stream);
-      cudaStreamSynchronize(ctx->c->stream);
-      if (st == IPEPS_OK && (dev_status & 2)) {
+      IPEPS_CUDA(cudaMemcpyAsync(&dev_status, ctx->c->d_status, sizeof(int), cudaMemcpyDeviceToHost,
+                                 ctx->c->stream));
+      IPEPS_CUDA(cudaStreamSynchronize(ctx->c->stream));
+      if (st == IPEPS_OK && (dev_status & 8)) {
+        ctx->err = "tensor-core GEMM pipeline wait timed out (results invalid)";
+        st = IPEPS_ECUDA;
+      } else if (st == IPEPS_OK && (dev_status & 2)) {
         ctx->err = "non-finite value detected";
         st = IPEPS_ENONFINITE;
       }
