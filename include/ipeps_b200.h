@@ -131,6 +131,21 @@ IPEPS_API int ipeps_es_energy(ipeps_env* env, const double* Hh, const double* Hv
 /* get_all_norm (evaluation.jl:61-77): Nb (complex) and envB (complex, size of A) */
 IPEPS_API int ipeps_all_norm(ipeps_env* env, double* Nb, double* envB);
 
+/* ---- allocation-free FP64 GEMM (no counterpart in the reference).
+ * C = alpha*op(A)*op(B) + beta*C, column-major, op in {'N','T'}; A, B, C are
+ * DEVICE pointers and the work is enqueued on `stream` (a cudaStream_t; NULL =
+ * the legacy default stream); the call returns without synchronising.
+ * For callers that cannot call cudaMalloc (device memory owned by a host
+ * framework's pool, or sections where cudaMalloc/cudaFree are not allowed):
+ * its split-K partial sums live in a fixed 4 MiB device array instead of an
+ * allocation, so it rejects m*n > 262144 with IPEPS_EINVAL (and a message on
+ * stderr).  The first call on a device sets up the array's address (make it
+ * before any stream capture).  All calls share the array: calls that overlap
+ * on the GPU race. */
+IPEPS_API int ipeps_gemm_f64_noalloc(char opA, char opB, int64_t m, int64_t n, int64_t k, double alpha,
+                                     const double* A, int64_t lda, const double* B, int64_t ldb, double beta,
+                                     double* C, int64_t ldc, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

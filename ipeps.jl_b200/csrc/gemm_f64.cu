@@ -255,3 +255,107 @@ void gemm_f64(Ctx& c, DType dt, char opA, char opB, int64_t m, int64_t n, int64_
 }
 
 }  // namespace ipeps
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of the split-K FP64 GEMM.
+//
+// Some callers cannot call cudaMalloc: a host framework that owns every byte
+// of device memory through its own pool (a Julia CUDA.jl session, a plugin
+// host with a fixed budget), or a latency-critical section where
+// cudaMalloc/cudaFree, which may synchronise the device, are not allowed.
+// For them the split-K partial sums live in this fixed device array
+// (4 MiB; every GPU that loads the library holds it until the process
+// exits).  The caller passes device pointers for A, B and C and a stream.
+//
+// The first call on a device looks up the array's device address with
+// cudaGetSymbolAddress (with that device current); make that first call
+// before any stream capture.  Every call shares the array: calls that overlap
+// on the GPU (different streams, or threads without ordering) race on it.
+// Each call overwrites all the partial sums it reads, so nothing needs
+// clearing between calls.
+// ---------------------------------------------------------------------------
+#include <mutex>
+
+#include "../../include/ipeps_b200.h"
+
+namespace ipeps {
+namespace {
+
+constexpr int64_t kNoAllocScratchDoubles = int64_t(1) << 19;  // 4 MiB of FP64 partial sums
+constexpr int64_t kNoAllocMaxOutput = kNoAllocScratchDoubles / 2;
+constexpr int kNoAllocMaxDevices = 64;
+
+static __device__ __align__(256) double g_noalloc_splitk_scratch[kNoAllocScratchDoubles];
+
+std::mutex g_noalloc_mu;
+double* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// Device address of the scratch array on the current device (set-up once per device).
+cudaError_t noalloc_scratch(double** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kNoAllocMaxDevices) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_splitk_scratch);
+    if (e != cudaSuccess) return e;
+    g_noalloc_ptr[dev] = static_cast<double*>(p);
+  }
+  *out = g_noalloc_ptr[dev];
+  return cudaSuccess;
+}
+
+}  // namespace
+}  // namespace ipeps
+
+extern "C" int ipeps_gemm_f64_noalloc(char opA, char opB, int64_t m, int64_t n, int64_t k, double alpha,
+                                      const double* A, int64_t lda, const double* B, int64_t ldb, double beta,
+                                      double* C, int64_t ldc, void* stream) {
+  using namespace ipeps;
+  if (!A || !B || !C || m <= 0 || n <= 0 || k <= 0) return IPEPS_EINVAL;
+  int oa, ob;
+  try {
+    oa = opcode(opA);
+    ob = opcode(opB);
+  } catch (...) {
+    return IPEPS_EINVAL;
+  }
+  if (oa == 2 || ob == 2) return IPEPS_EINVAL;  // real data: 'C' is not meaningful
+  if (m * n > kNoAllocMaxOutput) {
+    std::fprintf(stderr,
+                 "ipeps_gemm_f64_noalloc: m*n = %lld output elements exceeds the static scratch limit of %lld\n",
+                 static_cast<long long>(m * n), static_cast<long long>(kNoAllocMaxOutput));
+    return IPEPS_EINVAL;
+  }
+  if (lda < ((oa == 0) ? m : k) || ldb < ((ob == 0) ? k : n) || ldc < m) return IPEPS_EINVAL;
+  double* scratch = nullptr;
+  if (noalloc_scratch(&scratch) != cudaSuccess) return IPEPS_ECUDA;
+  constexpr int BM = 64, BN = 64, BK = 16, TM = 4, TN = 4, NT = (BM / TM) * (BN / TN);
+  const int64_t gx = (m + BM - 1) / BM, gy = (n + BN - 1) / BN;
+  if (gy > 65535) return IPEPS_EINVAL;
+  int sms = 148;
+  int dev = 0;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  // same split heuristic as the allocating path, capped by the scratch size
+  const int64_t tiles = gx * gy, target = 2LL * sms;
+  int64_t S = 1;
+  if (tiles < target && k >= 8 * BK * 2) S = std::min<int64_t>(std::min<int64_t>((target + tiles - 1) / tiles, k / (8 * BK)), 64);
+  S = std::max<int64_t>(1, std::min<int64_t>(S, kNoAllocScratchDoubles / (m * n)));
+  int64_t kchunk = (k + S - 1) / S;
+  kchunk = ((kchunk + BK - 1) / BK) * BK;
+  S = (k + kchunk - 1) / kchunk;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const cuDoubleComplex a = make_cuDoubleComplex(alpha, 0), b = make_cuDoubleComplex(beta, 0);
+  dim3 grid{unsigned(gx), unsigned(gy), unsigned(S)};
+  gemm_kernel<double, BM, BN, BK, TM, TN><<<grid, NT, 0, st>>>(oa, ob, m, n, k, kchunk, a, A, lda, B, ldb, b, C, ldc,
+                                                                S > 1 ? scratch : nullptr);
+  if (cudaGetLastError() != cudaSuccess) return IPEPS_ECUDA;
+  if (S > 1) {
+    const int64_t tot = m * n;
+    splitk_reduce<double><<<unsigned((tot + 255) / 256), 256, 0, st>>>(m, n, int(S), scratch, a, b, C, ldc);
+    if (cudaGetLastError() != cudaSuccess) return IPEPS_ECUDA;
+  }
+  return IPEPS_OK;
+}
