@@ -55,6 +55,8 @@ typedef struct {
   double bytes[8];
   uint64_t moves;       /* directional moves done by all envs of this context */
   double move_seconds;  /* host wall time inside moves (synchronous) */
+  uint64_t projector_calls; /* truncated-SVD projectors computed */
+  uint64_t jacobi_sweeps;   /* one-sided Jacobi sweeps summed over those projectors */
 } ipeps_stats_t;
 
 /* ---- context (no reference counterpart: the reference is one CPU process) */

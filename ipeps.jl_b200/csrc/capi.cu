@@ -128,6 +128,8 @@ int ipeps_stats(ipeps_ctx* ctx, ipeps_stats_t* out) {
     }
     out->moves = ctx->moves_done;
     out->move_seconds = ctx->move_seconds;
+    out->projector_calls = ctx->c->projector_calls;
+    out->jacobi_sweeps = ctx->c->jacobi_sweeps;
     return IPEPS_OK;
   });
 }
@@ -137,6 +139,8 @@ int ipeps_stats_reset(ipeps_ctx* ctx) {
     for (auto& s : ctx->c->stats) s = ipeps::KStat{};
     ctx->moves_done = 0;
     ctx->move_seconds = 0;
+    ctx->c->projector_calls = 0;
+    ctx->c->jacobi_sweeps = 0;
     return IPEPS_OK;
   });
 }

@@ -296,3 +296,202 @@ void scale_rows(Ctx& c, double* X, int64_t ldx, int64_t m, int64_t ncols, const 
 }
 
 }  // namespace ipeps
+
+// ---------------------------------------------------------------------------
+// Shared-memory kernels for the projector's k x k problems.
+// ---------------------------------------------------------------------------
+namespace ipeps {
+namespace {
+
+__device__ __forceinline__ int pidx(int i, int j) { return j * (j + 1) / 2 + i; }  // packed upper, i <= j
+
+__device__ __forceinline__ double warp_sum2(double v) {
+  for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Fused guarded Cholesky + in-place triangular inverse on the packed upper
+// triangle held in shared memory.  On exit G holds R (G = R^T R after the
+// optional shift, strict lower triangle zeroed) and Rinv = R^-1.
+// shift_factor > 0 adds shift_factor * trace(G) to the diagonal first.
+__global__ void __launch_bounds__(1024) cholinv_packed_kernel(double* G, int k, int64_t ldg, double shift_factor,
+                                                              double* Rinv, int64_t ldr) {
+  extern __shared__ double P[];
+  double* tmp = P + k * (k + 1) / 2;
+  __shared__ double s_red[32];
+  __shared__ double s_tr;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
+  for (int j = warp; j < k; j += nw)
+    for (int i = lane; i <= j; i += 32) P[pidx(i, j)] = G[i + int64_t(j) * ldg];
+  __syncthreads();
+  // trace (for the shift and the pivot guard)
+  double t = 0;
+  for (int i = tid; i < k; i += blockDim.x) t += fabs(P[pidx(i, i)]);
+  t = warp_sum2(t);
+  if (lane == 0) s_red[warp] = t;
+  __syncthreads();
+  if (tid == 0) {
+    double s = 0;
+    for (int w = 0; w < nw; ++w) s += s_red[w];
+    s_tr = s;
+  }
+  __syncthreads();
+  const double shift = shift_factor > 0 ? shift_factor * s_tr : 0.0;
+  if (shift > 0)
+    for (int i = tid; i < k; i += blockDim.x) P[pidx(i, i)] += shift;
+  const double tiny = 1e-300 + 1e-32 * (s_tr + shift * k);
+  __syncthreads();
+  // right-looking Cholesky, one column of R per step
+  for (int j = 0; j < k; ++j) {
+    const double d = P[pidx(j, j)];
+    const double piv = d > tiny ? sqrt(d) : 0.0;
+    __syncthreads();
+    for (int l = j + 1 + tid; l < k; l += blockDim.x) P[pidx(j, l)] = piv > 0 ? P[pidx(j, l)] / piv : 0.0;
+    if (tid == 0) P[pidx(j, j)] = piv > 0 ? piv : 1.0;
+    __syncthreads();
+    for (int l = j + 1 + warp; l < k; l += nw) {
+      const double rjl = P[pidx(j, l)];
+      for (int i = j + 1 + lane; i <= l; i += 32) P[pidx(i, l)] -= P[pidx(j, i)] * rjl;
+    }
+    __syncthreads();
+  }
+  for (int j = warp; j < k; j += nw)
+    for (int i = lane; i < k; i += 32) G[i + int64_t(j) * ldg] = (i <= j) ? P[pidx(i, j)] : 0.0;
+  // in-place inverse of the upper-triangular R, column by column:
+  // X[0:j, j] = -X[0:j, 0:j] * R[0:j, j] / R[j, j], X[j, j] = 1 / R[j, j]
+  for (int j = 0; j < k; ++j) {
+    for (int i = tid; i < j; i += blockDim.x) tmp[i] = P[pidx(i, j)];
+    __syncthreads();
+    const double inv = 1.0 / P[pidx(j, j)];
+    for (int i = warp; i < j; i += nw) {
+      double s = 0;
+      for (int l = i + lane; l < j; l += 32) s = fma(P[pidx(i, l)], tmp[l], s);
+      s = warp_sum2(s);
+      if (lane == 0) P[pidx(i, j)] = -inv * s;
+    }
+    __syncthreads();
+    if (tid == 0) P[pidx(j, j)] = inv;
+  }
+  __syncthreads();
+  for (int j = warp; j < k; j += nw)
+    for (int i = lane; i < k; i += 32) Rinv[i + int64_t(j) * ldr] = (i <= j) ? P[pidx(i, j)] : 0.0;
+}
+
+// One-sided Jacobi with the m x k matrix X resident in shared memory (J in
+// global memory).  Same ordering and rotation as jacobi_kernel.
+__global__ void __launch_bounds__(1024) jacobi_smem_kernel(double* Xg, int m, int k, int64_t ldx, double* J,
+                                                           int64_t ldj, double* S, int max_sweeps, double tol,
+                                                           int* status, int* sweeps_out) {
+  extern __shared__ double X[];
+  __shared__ double s_off;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+  for (int j = warp; j < k; j += nwarps)
+    for (int i = lane; i < m; i += 32) X[i + j * m] = Xg[i + int64_t(j) * ldx];
+  for (int64_t t = threadIdx.x; t < int64_t(k) * k; t += blockDim.x) {
+    int i = int(t % k), j = int(t / k);
+    J[i + j * ldj] = (i == j) ? 1.0 : 0.0;
+  }
+  __syncthreads();
+  const int kk = (k + 1) & ~1;
+  int sweep = 0;
+  bool converged = (k < 2);
+  for (; sweep < max_sweeps && !converged; ++sweep) {
+    if (threadIdx.x == 0) s_off = 0.0;
+    __syncthreads();
+    for (int r = 0; r < kk - 1; ++r) {
+      for (int pi = warp; pi < kk / 2; pi += nwarps) {
+        int p = (pi == 0) ? 0 : 1 + (pi - 1 + r) % (kk - 1);
+        int q = 1 + (kk - 2 - pi + r) % (kk - 1);
+        if (p >= k || q >= k) continue;
+        if (p > q) { int t = p; p = q; q = t; }
+        double a = 0, b = 0, cc = 0;
+        for (int i = lane; i < m; i += 32) {
+          double xp = X[i + p * m], xq = X[i + q * m];
+          a = fma(xp, xp, a);
+          b = fma(xq, xq, b);
+          cc = fma(xp, xq, cc);
+        }
+        a = warp_sum2(a);
+        b = warp_sum2(b);
+        cc = warp_sum2(cc);
+        if (cc == 0.0 || a == 0.0 || b == 0.0) continue;
+        const double rel = fabs(cc) / sqrt(a * b);
+        if (rel <= tol) continue;
+        if (lane == 0)
+          atomicMax(reinterpret_cast<unsigned long long*>(&s_off),
+                    static_cast<unsigned long long>(__double_as_longlong(rel)));
+        const double zeta = (b - a) / (2.0 * cc);
+        const double t = copysign(1.0, zeta) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+        const double cs = 1.0 / sqrt(1.0 + t * t), sn = cs * t;
+        for (int i = lane; i < m; i += 32) {
+          double xp = X[i + p * m], xq = X[i + q * m];
+          X[i + p * m] = cs * xp - sn * xq;
+          X[i + q * m] = sn * xp + cs * xq;
+        }
+        for (int i = lane; i < k; i += 32) {
+          double jp = J[i + p * ldj], jq = J[i + q * ldj];
+          J[i + p * ldj] = cs * jp - sn * jq;
+          J[i + q * ldj] = sn * jp + cs * jq;
+        }
+      }
+      __syncthreads();
+    }
+    converged = (s_off <= tol);
+    __syncthreads();
+  }
+  for (int j = warp; j < k; j += nwarps) {
+    double a = 0;
+    for (int i = lane; i < m; i += 32) {
+      const double x = X[i + j * m];
+      a = fma(x, x, a);
+      Xg[i + int64_t(j) * ldx] = x;
+    }
+    a = warp_sum2(a);
+    if (lane == 0) S[j] = sqrt(a);
+  }
+  if (threadIdx.x == 0) {
+    if (!converged) atomicOr(status, 4);
+    if (sweeps_out) *sweeps_out = sweep;
+  }
+}
+
+// opt-in limit per block is 227 KB including static shared memory; keep 1 KB for the kernels' own
+constexpr size_t kMaxDynSmem = 226 * 1024;
+bool g_cholinv_attr = false, g_jacobi_attr = false;
+
+}  // namespace
+
+bool cholinv_fits(int k) { return (size_t(k) * (k + 1) / 2 + k) * 8 <= kMaxDynSmem; }
+
+void chol_inv_upper(Ctx& c, double* G, int k, int64_t ldg, double shift_factor, double* Rinv, int64_t ldr) {
+  IPEPS_CHECK(cholinv_fits(k), "chol_inv_upper: k too large for shared memory");
+  if (!g_cholinv_attr) {
+    IPEPS_CUDA(cudaFuncSetAttribute(cholinv_packed_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kMaxDynSmem)));
+    g_cholinv_attr = true;
+  }
+  ProfScope ps(c, KFam::SmallLinalg);
+  const size_t smem = (size_t(k) * (k + 1) / 2 + k) * 8;
+  cholinv_packed_kernel<<<1, 1024, smem, c.stream>>>(G, k, ldg, shift_factor, Rinv, ldr);
+  IPEPS_LAUNCH_CHECK();
+  c.count(KFam::SmallLinalg, 2.0 * double(k) * k * k / 3.0);
+}
+
+void jacobi_svd_auto(Ctx& c, double* X, int m, int k, int64_t ldx, double* J, int64_t ldj, double* S,
+                     int max_sweeps, double tol, int* d_sweeps) {
+  const size_t smem = size_t(m) * k * 8;
+  if (tol <= 0) tol = double(m) * 2.220446049250313e-16;  // rounding level of the column dot products
+  if (smem <= kMaxDynSmem) {
+    if (!g_jacobi_attr) {
+      IPEPS_CUDA(cudaFuncSetAttribute(jacobi_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kMaxDynSmem)));
+      g_jacobi_attr = true;
+    }
+    ProfScope ps(c, KFam::Jacobi);
+    jacobi_smem_kernel<<<1, 1024, smem, c.stream>>>(X, m, k, ldx, J, ldj, S, max_sweeps, tol, c.d_status, d_sweeps);
+    IPEPS_LAUNCH_CHECK();
+    c.count(KFam::Jacobi, 6.0 * double(m + k) * k * k / 2.0);
+  } else {
+    jacobi_svd(c, X, m, k, ldx, J, ldj, S, max_sweeps, tol, d_sweeps);
+  }
+}
+
+}  // namespace ipeps

@@ -16,6 +16,14 @@ void trace(Ctx& c, const double* G, int k, int64_t ldg, double* d_out);
 // J accumulated (k x k), S = column norms (unsorted).
 void jacobi_svd(Ctx& c, double* X, int m, int k, int64_t ldx, double* J, int64_t ldj, double* S,
                 int max_sweeps, double tol, int* d_sweeps);
+// Fused Cholesky + triangular inverse in shared memory (packed upper triangle):
+// G <- R (G = R^T R after adding shift_factor * trace(G) to the diagonal when
+// shift_factor > 0), Rinv <- R^-1.  Requires cholinv_fits(k).
+bool cholinv_fits(int k);
+void chol_inv_upper(Ctx& c, double* G, int k, int64_t ldg, double shift_factor, double* Rinv, int64_t ldr);
+// jacobi_svd with X held in shared memory when it fits; tol <= 0 means m * eps
+void jacobi_svd_auto(Ctx& c, double* X, int m, int k, int64_t ldx, double* J, int64_t ldj, double* S,
+                     int max_sweeps, double tol, int* d_sweeps);
 // Descending sort with permutation (ties: later index first)
 void sort_desc(Ctx& c, const double* S, int k, double* S_out, int* perm);
 // out[:, j] = in[:, perm[j]] * f(scale[j]); scale_mode 0: 1, 1: scale, 2: 1/scale

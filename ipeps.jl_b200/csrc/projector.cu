@@ -53,16 +53,23 @@ Tensor orth(Ctx& c, const Tensor& Y0, int passes, Tensor* Rout) {
   Tensor Racc;
   double* d_tr = reinterpret_cast<double*>(c.scal->p) + 8;
   const double u = 1.1102230246251565e-16;
+  const bool fused = cholinv_fits(k);
   for (int pass = 0; pass < passes; ++pass) {
     // G = Y^T Y  (FP64 always: the Gram matrix is where precision is lost)
     gemm(c, DType::F64, 'T', 'N', k, k, N, cplx(1), Y.data(), N, Y.data(), N, cplx(0), G.data(), k, true);
-    if (pass == 0) {
-      trace(c, G.f64(), k, k, d_tr);
-      chol_upper(c, G.f64(), k, k, d_tr, 11.0 * (double(N) * k + double(k) * (k + 1)) * u);
+    // shifted CholeskyQR: the first pass adds 11 (N k + k (k+1)) u trace(G) to the diagonal
+    const double sf = (pass == 0) ? 11.0 * (double(N) * k + double(k) * (k + 1)) * u : 0.0;
+    if (fused) {
+      chol_inv_upper(c, G.f64(), k, k, sf, Ri.f64(), k);
     } else {
-      chol_upper(c, G.f64(), k, k, nullptr, 0.0);
+      if (pass == 0) {
+        trace(c, G.f64(), k, k, d_tr);
+        chol_upper(c, G.f64(), k, k, d_tr, sf);
+      } else {
+        chol_upper(c, G.f64(), k, k, nullptr, 0.0);
+      }
+      triinv_upper(c, G.f64(), k, k, Ri.f64(), k);
     }
-    triinv_upper(c, G.f64(), k, k, Ri.f64(), k);
     Tensor Yn = c.alloc(DType::F64, {N, k});
     gemm(c, DType::F64, 'N', 'N', N, k, k, cplx(1), Y.data(), N, Ri.data(), k, cplx(0), Yn.data(), N, true);
     Y = Yn;
@@ -117,7 +124,7 @@ ProjResult get_projector(Ctx& c, const MatRef& R1, const MatRef& R2, int chi, co
   Tensor J = c.alloc(DType::F64, {k, k});
   Tensor S = c.alloc(DType::F64, {k});
   int* d_sweeps = reinterpret_cast<int*>(static_cast<char*>(c.scal->p) + 3900);
-  jacobi_svd(c, X.f64(), k, k, k, J.f64(), k, S.f64(), sp.jacobi_max_sweeps, sp.jacobi_tol, d_sweeps);
+  jacobi_svd_auto(c, X.f64(), k, k, k, J.f64(), k, S.f64(), sp.jacobi_max_sweeps, sp.jacobi_tol, d_sweeps);
   Tensor Ss = c.alloc(DType::F64, {k});
   Tensor perm = c.alloc(DType::F64, {(k + 1) / 2});  // int storage
   int* d_perm = static_cast<int*>(perm.data());
@@ -131,6 +138,8 @@ ProjResult get_projector(Ctx& c, const MatRef& R1, const MatRef& R2, int chi, co
   IPEPS_CUDA(cudaMemcpyAsync(&sweeps, d_sweeps, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
   c.sync();
   r.sweeps = sweeps;
+  c.jacobi_sweeps += uint64_t(sweeps);
+  c.projector_calls++;
 
   // cutoff_matrix (wrapper.jl:37-55)
   const double smax = r.s_host[0];

@@ -21,7 +21,7 @@ struct SvdParams {
   int power_iters_warm = 2; // when the previous V of this direction seeds the sketch
   bool warm_start = true;
   int jacobi_max_sweeps = 40;
-  double jacobi_tol = 1e-15;
+  double jacobi_tol = 0.0;  // <= 0: m * eps (rounding level of the column dot products)
 };
 
 // Cache of the last right singular vectors of one direction (warm start).

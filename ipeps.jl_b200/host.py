@@ -52,14 +52,16 @@ class IPEPSError(RuntimeError):
 
 class Stats(ct.Structure):
     _fields_ = [("launches", ct.c_uint64 * 8), ("flops", ct.c_double * 8), ("bytes", ct.c_double * 8),
-                ("moves", ct.c_uint64), ("move_seconds", ct.c_double)]
+                ("moves", ct.c_uint64), ("move_seconds", ct.c_double), ("projector_calls", ct.c_uint64),
+                ("jacobi_sweeps", ct.c_uint64)]
 
     FAMILIES = ["permute", "gemm_f64", "gemm_tf32x3", "reduce", "elementwise", "small_linalg", "jacobi"]
 
     def as_dict(self):
         fam = {n: {"launches": int(self.launches[i]), "flops": float(self.flops[i]), "bytes": float(self.bytes[i])}
                for i, n in enumerate(self.FAMILIES)}
-        return {"families": fam, "moves": int(self.moves), "move_seconds": float(self.move_seconds)}
+        return {"families": fam, "moves": int(self.moves), "move_seconds": float(self.move_seconds),
+                "projector_calls": int(self.projector_calls), "jacobi_sweeps": int(self.jacobi_sweeps)}
 
 
 _lib = None
