@@ -124,6 +124,16 @@ IPEPS_API int ipeps_energy(ipeps_env* env, const double* Hh, const double* Hv, i
 /* get_gs_norm (evaluation.jl:47-59) */
 IPEPS_API int ipeps_gs_norm(ipeps_env* env, double* nrm);
 
+/* ---- energy + gradient: the pullback of run_gs (optim_gs.jl:133-143) as
+ * used by fg! (optim_gs.jl:53-91).  Starting from the environment currently
+ * held (normally converged by ipeps_ctm_run), runs ad_iters CTMRG iterations
+ * with A as the variable, then get_gs_energy; returns real(E) and dE/dA
+ * (D,D,D,D,d, real A only; A and Ad = conj(A) both contribute).  The
+ * environment is advanced by those iterations.  C/T are checkpointed per
+ * iteration and the moves recomputed in the backward pass. */
+IPEPS_API int ipeps_energy_grad(ipeps_env* env, const double* Hh, const double* Hv, int d2, int ad_iters, double* E,
+                                double* dA);
+
 /* ---- nested-tensor (excited-state) move, optim_es (src/optimize/optim_es.jl:167-210) */
 /* setproperties(ts, B=B, Bd=conj(B)) + Params px, py (in radians); B complex (D,D,D,D,d).
  * Clears the B/Bd/BB environment slots (EmptyT). */

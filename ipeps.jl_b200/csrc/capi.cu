@@ -452,3 +452,23 @@ int ipeps_all_norm(ipeps_env* env, double* Nb, double* envB) {
 }
 
 }  // extern "C"
+
+#include "ad.cuh"
+
+extern "C" int ipeps_energy_grad(ipeps_env* env, const double* Hh, const double* Hv, int d2, int ad_iters, double* E,
+                                 double* dA) {
+  if (!env) return IPEPS_EINVAL;
+  return guarded(env->owner, [&] {
+    IPEPS_CHECK(ad_iters >= 1, "ad_iters must be >= 1");
+    auto& c = *env->e.ctx;
+    Tensor th = upload_H(c, Hh, d2), tv = upload_H(c, Hv, d2);
+    uint64_t m0 = env->e.moves;
+    double s0 = env->e.move_seconds;
+    Tensor g;
+    double e = ipeps::energy_grad(env->e, th, tv, ad_iters, &g);
+    account(env, m0, s0);
+    if (E) *E = e;
+    if (dA) download(c, dA, g);
+    return IPEPS_OK;
+  });
+}

@@ -1,10 +1,11 @@
 // CTMRG engine: nested-tensor algebra, the four directional moves, the
-// energy and run_ctm.  Contraction labels follow the reference verbatim
-// (file:line cited per function) so that every fused leg order is identical;
-// only the renormalisation of the edge tensor (proj_*) uses a cheaper
-// contraction order than the reference (same result, see proj_edge).
+// energy and run_ctm.  The contraction sequences live in moves.cuh
+// (reference labels verbatim); this file instantiates them on NT tensors
+// (plain or 4-component nested) and adds the projector, max-abs
+// renormalisation, the phase shift of the nested move and the run loop.
 #include "ctm.cuh"
 #include "linalg.cuh"
+#include "moves.cuh"
 
 #include <chrono>
 #include <cmath>
@@ -20,14 +21,8 @@ void add_into(Ctx& c, Tensor& acc, const Tensor& t) {
     acc = t;
     return;
   }
-  if (acc.dt != t.dt) {
-    if (acc.dt == DType::F64) acc = to_complex(c, acc);
-    else {
-      axpy(c, cplx(1), t, acc);  // real into complex handled by axpy_rc
-      return;
-    }
-  }
-  axpy(c, cplx(1), t, acc);
+  if (acc.dt == DType::F64 && t.dt == DType::C128) acc = to_complex(c, acc);
+  axpy(c, cplx(1), t, acc);  // real into complex handled by axpy_rc
 }
 
 }  // namespace
@@ -116,6 +111,17 @@ void nrenormalize(Ctx& c, NT& A) {
     }
 }
 
+// Forward policy for moves.cuh on NT tensors
+struct NTPolicy {
+  using T = NT;
+  Ctx& c;
+  T tc(const T& a, const std::vector<int>& la, const T& b, const std::vector<int>& lb) { return ntcon(c, a, la, b, lb); }
+  T rs(const T& a, const std::vector<int64_t>& s) { return nreshape(a, s); }
+  T pm(const T& a, const std::vector<int>& perm) { return npermute(c, a, perm); }
+  T mm(const T& a, const T& b) { return nmatmul(c, a, 'N', b, 'N'); }
+  int64_t dim(const T& a, int i) const { return a.c[0].dims[i]; }
+};
+
 // ------------------------------------------------------------ environment
 NT Env::all_A() const {  // ctm_tensor.jl:20-27
   if (!nested) return NT(A);
@@ -168,185 +174,53 @@ void init_ctm1(Env& e) {
   for (int i = 0; i < 4; ++i) e.cache[i].V = Tensor();
 }
 
-// ------------------------------------------------------------ projectors
-namespace {
-
-int64_t prod3(const Tensor& t) { return t.dims[0] * t.dims[1] * t.dims[2]; }
-
-// ctmrg.jl:122-153
-void quarters_left(Ctx& c, Env& e, MatRef& R1, MatRef& R2) {
-  const Tensor &C1 = e.Cs[0], &C4 = e.Cs[3], &E1 = e.Es[0], &E3 = e.Es[2], &E4 = e.Es[3];
-  const Tensor &A = e.A, &Ad = e.Ad;
-  Tensor C1E1 = tcon(c, C1, {-1, 1}, E1, {1, -2, -3, -4});
-  Tensor CEE4 = tcon(c, C1E1, {1, -2, -5, -3}, E4, {1, -1, -6, -4});
-  Tensor CEEA = tcon(c, CEE4, {-1, -2, -3, -4, 1, 2}, A, {1, 2, -5, -6, -7});
-  Tensor LU = tcon(c, CEEA, {-1, -4, 1, 2, -2, -5, 3}, Ad, {1, 2, -3, -6, 3});
-  R1 = MatRef{LU.reshape({prod3(LU), -1}), true};
-  Tensor C4E3 = tcon(c, C4, {-1, 1}, E3, {1, -2, -3, -4});
-  Tensor CEE4b = tcon(c, C4E3, {1, -2, -6, -4}, E4, {-1, 1, -5, -3});
-  Tensor CEEAb = tcon(c, CEE4b, {-1, -2, -3, -4, 1, 2}, A, {-5, 1, 2, -6, -7});
-  Tensor LB = tcon(c, CEEAb, {-1, -4, 1, 2, -2, -5, 3}, Ad, {-3, 1, 2, -6, 3});
-  R2 = MatRef{LB.reshape({prod3(LB), -1}), false};
-}
-
-// ctmrg.jl:155-186
-void quarters_right(Ctx& c, Env& e, MatRef& R1, MatRef& R2) {
-  const Tensor &C2 = e.Cs[1], &C3 = e.Cs[2], &E1 = e.Es[0], &E2 = e.Es[1], &E3 = e.Es[2];
-  const Tensor &A = e.A, &Ad = e.Ad;
-  Tensor C2E1 = tcon(c, C2, {1, -2}, E1, {-1, 1, -3, -4});
-  Tensor CEE2 = tcon(c, C2E1, {-1, 1, -5, -3}, E2, {1, -2, -6, -4});
-  Tensor CEEA = tcon(c, CEE2, {-1, -2, -3, -4, 1, 2}, A, {1, -5, -6, 2, -7});
-  Tensor RU = tcon(c, CEEA, {-1, -4, 1, 2, -2, -5, 3}, Ad, {1, -3, -6, 2, 3});
-  R1 = MatRef{RU.reshape({prod3(RU), -1}), false};
-  Tensor C3E3 = tcon(c, C3, {-1, 1}, E3, {-2, 1, -3, -4});
-  Tensor CEE2b = tcon(c, C3E3, {1, -2, -5, -3}, E2, {-1, 1, -6, -4});
-  Tensor CEEAb = tcon(c, CEE2b, {-1, -2, -5, -6, 1, 2}, A, {-3, -4, 1, 2, -7});
-  Tensor RB = tcon(c, CEEAb, {-1, -4, -2, -5, 1, 2, 3}, Ad, {-3, -6, 1, 2, 3});
-  R2 = MatRef{RB.reshape({prod3(RB), -1}), false};
-}
-
-// ctmrg.jl:188-219
-void quarters_top(Ctx& c, Env& e, MatRef& R1, MatRef& R2) {
-  const Tensor &C1 = e.Cs[0], &C2 = e.Cs[1], &E1 = e.Es[0], &E2 = e.Es[1], &E4 = e.Es[3];
-  const Tensor &A = e.A, &Ad = e.Ad;
-  Tensor C1E4 = tcon(c, C1, {1, -2}, E4, {1, -1, -3, -4});
-  Tensor CEE1 = tcon(c, C1E4, {-1, 1, -6, -4}, E1, {1, -2, -5, -3});
-  Tensor CEEA = tcon(c, CEE1, {-1, -2, -5, -6, 1, 2}, A, {1, 2, -3, -4, -7});
-  Tensor UL = tcon(c, CEEA, {-1, -4, -2, -5, 1, 2, 3}, Ad, {1, 2, -3, -6, 3});
-  R1 = MatRef{UL.reshape({prod3(UL), -1}), false};
-  Tensor C2E2 = tcon(c, C2, {-1, 1}, E2, {1, -2, -3, -4});
-  Tensor CEE1b = tcon(c, C2E2, {1, -2, -6, -4}, E1, {-1, 1, -5, -3});
-  Tensor CEEAb = tcon(c, CEE1b, {-1, -2, -5, -6, 1, 2}, A, {1, -3, -4, 2, -7});
-  Tensor UR = tcon(c, CEEAb, {-1, -4, -2, -5, 1, 2, 3}, Ad, {1, -3, -6, 2, 3});
-  R2 = MatRef{UR.reshape({prod3(UR), -1}), false};
-}
-
-// ctmrg.jl:221-252
-void quarters_bottom(Ctx& c, Env& e, MatRef& R1, MatRef& R2) {
-  const Tensor &C3 = e.Cs[2], &C4 = e.Cs[3], &E2 = e.Es[1], &E3 = e.Es[2], &E4 = e.Es[3];
-  const Tensor &A = e.A, &Ad = e.Ad;
-  Tensor C4E4 = tcon(c, C4, {1, -2}, E4, {-1, 1, -3, -4});
-  Tensor CEE3 = tcon(c, C4E4, {-1, 1, -5, -3}, E3, {1, -2, -6, -4});
-  Tensor CEEA = tcon(c, CEE3, {-1, -2, -5, -6, 1, 2}, A, {-3, 1, 2, -4, -7});
-  Tensor BL = tcon(c, CEEA, {-1, -4, -2, -5, 1, 2, 3}, Ad, {-3, 1, 2, -6, 3});
-  R1 = MatRef{BL.reshape({prod3(BL), -1}), false};
-  Tensor C3E2 = tcon(c, C3, {1, -2}, E2, {-1, 1, -3, -4});
-  Tensor CEE3b = tcon(c, C3E2, {-1, 1, -6, -4}, E3, {-2, 1, -5, -3});
-  Tensor CEEAb = tcon(c, CEE3b, {-1, -2, -5, -6, 1, 2}, A, {-3, -4, 1, 2, -7});
-  Tensor BR = tcon(c, CEEAb, {-1, -4, -2, -5, 1, 2, 3}, Ad, {-3, -6, 1, 2, 3});
-  R2 = MatRef{BR.reshape({prod3(BR), -1}), true};
-}
-
-// New edge tensor of a move.  The reference (ctmrg.jl:284-290 and the right,
-// top and bottom analogues) forms T*A*A' (chi^2 D^6 elements) and then
-// contracts Pd and P (2 chi^3 D^6 flops).  The same tensor
-//   newE[c,c2,o,o'] = sum Pd[c,(a,g,g')] E[a,b,k,k'] A[..g..k..h..o..s] A'[..g'..k'..h'..o'..s] P[(b,h,h'),c2]
-// is contracted here as ((Pd*E)*A)*A' then *P, which costs
-// 4 chi^3 D^4 + 4 chi^2 D^6 d flops and never materialises chi^2 D^6.
-// Legs of A are (up, left, down, right, phys) = 0..4; lg/le/lh/lo are the
-// legs grouped with Pd, contracted with E, grouped with P, and left open.
-NT proj_edge(Ctx& c, const NT& E, const NT& A, const NT& Ad, const Tensor& P, const Tensor& Pd, int lg,
-             int le, int lh, int lo) {
-  const int64_t chiE = E.c[0].dims[0], D = A.c[0].dims[0];
-  NT Pdr(Pd.reshape({Pd.dims[0], chiE, D, D}));
-  NT X2 = ntcon(c, Pdr, {-1, 1, -2, -3}, E, {1, -4, -5, -6});  // (c, g, g', b, k, k')
-  std::vector<int> la(5);
-  la[lg] = 1;
-  la[le] = 2;
-  la[lh] = -5;
-  la[lo] = -6;
-  la[4] = -7;
-  NT X3 = ntcon(c, X2, {-1, 1, -2, -3, 2, -4}, A, la);  // (c, g', b, k', h, o, s)
-  std::vector<int> lad(5);
-  lad[lg] = 1;
-  lad[le] = 2;
-  lad[lh] = -5;
-  lad[lo] = -6;
-  lad[4] = 3;
-  NT X4 = ntcon(c, X3, {-1, 1, -2, 2, -3, -4, 3}, Ad, lad);  // (c, b, h, o, h', o')
-  const int64_t chiB = E.c[0].dims[1];
-  NT Pr(P.reshape({chiB, D, D, P.dims[1]}));
-  return ntcon(c, X4, {-1, 1, 2, -3, 3, -4}, Pr, {1, 2, 3, -2});  // (c, c2, o, o')
-}
-
-}  // namespace
-
 // One directional move: *_rg (ctmrg.jl:66-120) = projector + proj_* +
 // renormalize + up_*.
-std::vector<double> ctm_move(Env& e, int dir) {
+std::vector<double> ctm_move(Env& e, int dir, ProjResult* keep) {
   Ctx& c = *e.ctx;
   IPEPS_CHECK(e.dt == DType::F64, "ctm_move: complex A needs the complex projector (not built)");
   auto t0 = std::chrono::steady_clock::now();
-  MatRef R1, R2;
-  switch (dir) {
-    case 0: quarters_left(c, e, R1, R2); break;
-    case 1: quarters_right(c, e, R1, R2); break;
-    case 2: quarters_top(c, e, R1, R2); break;
-    default: quarters_bottom(c, e, R1, R2); break;
+  NTPolicy p{c};
+  Arr4<NTPolicy> Cs0, Es0;
+  for (int i = 0; i < 4; ++i) {
+    Cs0[i] = NT(e.Cs[i]);
+    Es0[i] = NT(e.Es[i]);
   }
-  ProjResult pr = get_projector(c, R1, R2, e.prm.chi, e.prm.svd, &e.cache[dir]);
-  R1 = MatRef();
-  R2 = MatRef();
-  const Tensor& P = pr.P1;
-  const Tensor& Pd = pr.P2;
-  NT A = e.all_A(), Ad = e.all_Ad();
-  NT nC_a, nE, nC_b;
-  if (dir == 0) {  // proj_left ctmrg.jl:267-293
-    NT C1 = e.all_C(0), C4 = e.all_C(3), E1 = e.all_E(0), E3 = e.all_E(2), E4 = e.all_E(3);
-    NT C1E1 = ntcon(c, C1, {-2, 1}, E1, {1, -1, -3, -4});
-    nC_a = npermute(c, nmatmul(c, nreshape(C1E1, {C1E1.c[0].dims[0], -1}), 'N', NT(P), 'N'), {1, 0});
-    NT C4E3 = ntcon(c, C4, {-1, 1}, E3, {1, -4, -2, -3});
-    nC_b = nmatmul(c, NT(Pd), 'N', nreshape(C4E3, {-1, C4E3.c[0].dims[3]}), 'N');
-    nE = proj_edge(c, E4, A, Ad, P, Pd, 0, 1, 2, 3);
-  } else if (dir == 1) {  // proj_right ctmrg.jl:295-320
-    NT C2 = e.all_C(1), C3 = e.all_C(2), E1 = e.all_E(0), E2 = e.all_E(1), E3 = e.all_E(2);
-    NT C2E1 = ntcon(c, C2, {1, -2}, E1, {-1, 1, -3, -4});
-    nC_a = nmatmul(c, nreshape(C2E1, {C2E1.c[0].dims[0], -1}), 'N', NT(P), 'N');
-    NT C3E3 = ntcon(c, C3, {-1, 1}, E3, {-4, 1, -2, -3});
-    nC_b = nmatmul(c, NT(Pd), 'N', nreshape(C3E3, {-1, C3E3.c[0].dims[3]}), 'N');
-    nE = proj_edge(c, E2, A, Ad, P, Pd, 0, 3, 2, 1);
-  } else if (dir == 2) {  // proj_top ctmrg.jl:322-347
-    NT C1 = e.all_C(0), C2 = e.all_C(1), E1 = e.all_E(0), E2 = e.all_E(1), E4 = e.all_E(3);
-    NT C1E4 = ntcon(c, C1, {1, -2}, E4, {1, -1, -3, -4});
-    nC_a = nmatmul(c, nreshape(C1E4, {C1E4.c[0].dims[0], -1}), 'N', NT(P), 'N');
-    NT C2E2 = ntcon(c, C2, {-1, 1}, E2, {1, -4, -2, -3});
-    nC_b = nmatmul(c, NT(Pd), 'N', nreshape(C2E2, {-1, C2E2.c[0].dims[3]}), 'N');
-    nE = proj_edge(c, E1, A, Ad, P, Pd, 1, 0, 3, 2);
-  } else {  // proj_bottom ctmrg.jl:349-375
-    NT C3 = e.all_C(2), C4 = e.all_C(3), E2 = e.all_E(1), E3 = e.all_E(2), E4 = e.all_E(3);
-    NT C4E4 = ntcon(c, C4, {1, -2}, E4, {-1, 1, -3, -4});
-    nC_a = nmatmul(c, nreshape(C4E4, {C4E4.c[0].dims[0], -1}), 'N', NT(P), 'N');
-    NT C3E2 = ntcon(c, C3, {1, -1}, E2, {-4, 1, -2, -3});
-    nC_b = npermute(c, nmatmul(c, NT(Pd), 'N', nreshape(C3E2, {-1, C3E2.c[0].dims[3]}), 'N'), {1, 0});
-    nE = proj_edge(c, E3, A, Ad, P, Pd, 1, 2, 3, 0);
+  ProjResult pr;
+  {
+    QuarterPair<NTPolicy> q = quarters(p, dir, Cs0, Es0, NT(e.A), NT(e.Ad));
+    MatRef R1{q.R1.c[0], q.t1}, R2{q.R2.c[0], q.t2};
+    pr = get_projector(c, R1, R2, e.prm.chi, e.prm.svd, &e.cache[dir], keep != nullptr);
   }
-  nrenormalize(c, nC_a);
-  nrenormalize(c, nE);
-  nrenormalize(c, nC_b);
-  // up_* (ctmrg.jl:377-491): slots per direction
+  Arr4<NTPolicy> Cs, Es;
+  for (int i = 0; i < 4; ++i) {
+    Cs[i] = e.all_C(i);
+    Es[i] = e.all_E(i);
+  }
+  Projected<NTPolicy> np = project(p, dir, Cs, Es, e.all_A(), e.all_Ad(), NT(pr.P1), NT(pr.P2));
+  nrenormalize(c, np.Ca);
+  nrenormalize(c, np.E);
+  nrenormalize(c, np.Cb);
   int ia, ib, ie;
-  double phi;
-  switch (dir) {
-    case 0: ia = 0; ib = 3; ie = 3; phi = -e.px; break;  // C1, C4, E4
-    case 1: ia = 1; ib = 2; ie = 1; phi = e.px; break;   // C2, C3, E2
-    case 2: ia = 0; ib = 1; ie = 0; phi = -e.py; break;  // C1, C2, E1
-    default: ia = 3; ib = 2; ie = 2; phi = e.py; break;  // C4, C3, E3
-  }
+  move_slots(dir, &ia, &ib, &ie);
   if (e.nested) {
-    nC_a = nshift(c, nC_a, phi);
-    nC_b = nshift(c, nC_b, phi);
-    nE = nshift(c, nE, phi);
-    e.B_Cs[ia] = nC_a.c[1]; e.Bd_Cs[ia] = nC_a.c[2]; e.BB_Cs[ia] = nC_a.c[3];
-    e.B_Cs[ib] = nC_b.c[1]; e.Bd_Cs[ib] = nC_b.c[2]; e.BB_Cs[ib] = nC_b.c[3];
-    e.B_Es[ie] = nE.c[1]; e.Bd_Es[ie] = nE.c[2]; e.BB_Es[ie] = nE.c[3];
+    const double phi = (dir == 0) ? -e.px : (dir == 1) ? e.px : (dir == 2) ? -e.py : e.py;
+    np.Ca = nshift(c, np.Ca, phi);
+    np.Cb = nshift(c, np.Cb, phi);
+    np.E = nshift(c, np.E, phi);
+    e.B_Cs[ia] = np.Ca.c[1]; e.Bd_Cs[ia] = np.Ca.c[2]; e.BB_Cs[ia] = np.Ca.c[3];
+    e.B_Cs[ib] = np.Cb.c[1]; e.Bd_Cs[ib] = np.Cb.c[2]; e.BB_Cs[ib] = np.Cb.c[3];
+    e.B_Es[ie] = np.E.c[1]; e.Bd_Es[ie] = np.E.c[2]; e.BB_Es[ie] = np.E.c[3];
   }
-  e.Cs[ia] = nC_a.c[0];
-  e.Cs[ib] = nC_b.c[0];
-  e.Es[ie] = nE.c[0];
+  e.Cs[ia] = np.Ca.c[0];
+  e.Cs[ib] = np.Cb.c[0];
+  e.Es[ie] = np.E.c[0];
   e.moves++;
   auto t1 = std::chrono::steady_clock::now();
   e.move_seconds += std::chrono::duration<double>(t1 - t0).count();
-  return pr.s_host;
+  std::vector<double> s = pr.s_host;
+  if (keep) *keep = std::move(pr);
+  return s;
 }
 
 // ctmrg.jl:57-64
@@ -362,51 +236,8 @@ std::vector<double> rg_step(Env& e) {
 // ------------------------------------------------------------ observables
 namespace {
 
-// evaluation.jl:169-200
-NT get_dm_h(Ctx& c, const NT& C1, const NT& C2, const NT& C3, const NT& C4, const NT& E1l, const NT& E1r,
-            const NT& E2, const NT& E3l, const NT& E3r, const NT& E4, const NT& Al, const NT& Ar, const NT& Adl,
-            const NT& Adr) {
-  NT C1E1 = ntcon(c, C1, {-1, 1}, E1l, {1, -2, -3, -4});
-  NT LU = ntcon(c, C1E1, {-1, -2, -3, 1}, Adl, {1, -4, -5, -6, -7});
-  NT C4E3 = ntcon(c, C4, {-1, 1}, E3l, {1, -2, -3, -4});
-  NT CEE4 = ntcon(c, E4, {-1, 1, -3, -5}, C4E3, {1, -2, -4, -6});
-  NT LB = ntcon(c, CEE4, {-1, -2, 1, 2, -4, -5}, Al, {-3, 1, 2, -6, -7});
-  NT L = ntcon(c, LB, {1, -2, 2, 3, 4, -3, -5}, LU, {1, -1, 2, 3, 4, -4, -6});
-  NT C2E1 = ntcon(c, C2, {1, -2}, E1r, {-1, 1, -3, -4});
-  NT RU = ntcon(c, C2E1, {-1, -2, 1, -3}, Ar, {1, -4, -5, -6, -7});
-  NT C3E3 = ntcon(c, C3, {-1, 1}, E3r, {-2, 1, -3, -4});
-  NT CEE2 = ntcon(c, C3E3, {1, -2, -3, -5}, E2, {-1, 1, -4, -6});
-  NT RB = ntcon(c, CEE2, {-1, -2, -3, -4, 1, 2}, Adr, {-5, -6, 1, 2, -7});
-  NT R = ntcon(c, RU, {-1, 1, 2, -3, 3, 4, -5}, RB, {1, -2, 3, 4, 2, -4, -6});
-  NT roh = ntcon(c, L, {1, 2, 3, 4, -1, -3}, R, {1, 2, 3, 4, -2, -4});
-  const int64_t d = Al.c[0].dims[4];
-  return nreshape(roh, {d * d, d * d});
-}
-
-// evaluation.jl:217-248
-NT get_dm_v(Ctx& c, const NT& C1, const NT& C2, const NT& C3, const NT& C4, const NT& E1, const NT& E2u,
-            const NT& E2d, const NT& E3, const NT& E4u, const NT& E4d, const NT& Au, const NT& Ad, const NT& Adu,
-            const NT& Add) {
-  NT C1E1 = ntcon(c, C1, {-1, 1}, E1, {1, -2, -3, -4});
-  NT CEE4 = ntcon(c, C1E1, {1, -2, -3, -5}, E4u, {1, -1, -4, -6});
-  NT UL = ntcon(c, CEE4, {-1, -2, 1, 2, -3, -4}, Au, {1, 2, -5, -6, -7});
-  NT C2E2 = ntcon(c, C2, {-1, 1}, E2u, {1, -2, -3, -4});
-  NT UR = ntcon(c, C2E2, {-1, -2, -3, 1}, Adu, {-4, -5, -6, 1, -7});
-  NT U = ntcon(c, UL, {-1, 1, 3, 4, -3, 2, -5}, UR, {1, -2, 2, 3, 4, -4, -6});
-  NT C4E3 = ntcon(c, C4, {-1, 1}, E3, {1, -2, -3, -4});
-  NT CEE4b = ntcon(c, C4E3, {1, -2, -4, -6}, E4d, {-1, 1, -3, -5});
-  NT BL = ntcon(c, CEE4b, {-1, -2, -3, -4, 1, 2}, Add, {-5, 1, 2, -6, -7});
-  NT C3E2 = ntcon(c, C3, {1, -2}, E2d, {-1, 1, -3, -4});
-  NT BR = ntcon(c, C3E2, {-1, -2, 1, -3}, Ad, {-4, -5, -6, 1, -7});
-  NT B = ntcon(c, BL, {-1, 1, 2, 3, -4, 4, -6}, BR, {-2, 1, 4, -3, 2, 3, -5});
-  NT rov = ntcon(c, U, {1, 2, 3, 4, -1, -3}, B, {1, 2, 3, 4, -2, -4});
-  const int64_t d = Au.c[0].dims[4];
-  return nreshape(rov, {d * d, d * d});
-}
-
 // out[0..1] = tr(H rho) (complex), out[2..3] = tr(rho) (complex); FP64
 __global__ void dm_trace_kernel(const double* rho, int rho_complex, const double2* H, int n, double* out) {
-  // one warp
   double hr = 0, hi = 0, tr = 0, ti = 0;
   for (int t = threadIdx.x; t < n * n; t += 32) {
     int i = t % n, j = t / n;  // tr(H rho) = sum_ij H[i,j] rho[j,i]
@@ -428,9 +259,7 @@ __global__ void dm_trace_kernel(const double* rho, int rho_complex, const double
   if (threadIdx.x == 0) { out[0] = hr; out[1] = hi; out[2] = tr; out[3] = ti; }
 }
 
-struct Traces {
-  std::complex<double> trH, tr;
-};
+}  // namespace
 
 // traces of several (rho, H) pairs in one host round trip
 std::vector<Traces> dm_traces(Ctx& c, const std::vector<std::pair<Tensor, Tensor>>& items) {
@@ -458,16 +287,15 @@ std::vector<Traces> dm_traces(Ctx& c, const std::vector<std::pair<Tensor, Tensor
   return r;
 }
 
-}  // namespace
-
 // evaluation.jl:15-29 with get_dms (only_gs) evaluation.jl:124-156
 void gs_energy(Env& e, const Tensor& Hh, const Tensor& Hv, std::complex<double>* E, std::complex<double>* Na) {
   Ctx& c = *e.ctx;
+  NTPolicy p{c};
   NT C1(e.Cs[0]), C2(e.Cs[1]), C3(e.Cs[2]), C4(e.Cs[3]);
   NT E1(e.Es[0]), E2(e.Es[1]), E3(e.Es[2]), E4(e.Es[3]);
   NT A(e.A), Ad(e.Ad);
-  NT roh = get_dm_h(c, C1, C2, C3, C4, E1, E1, E2, E3, E3, E4, A, A, Ad, Ad);
-  NT rov = get_dm_v(c, C1, C2, C3, C4, E1, E2, E2, E3, E4, E4, A, A, Ad, Ad);
+  NT roh = get_dm_h(p, C1, C2, C3, C4, E1, E1, E2, E3, E3, E4, A, A, Ad, Ad);
+  NT rov = get_dm_v(p, C1, C2, C3, C4, E1, E2, E2, E3, E4, E4, A, A, Ad, Ad);
   auto t = dm_traces(c, {{roh.c[0], Hh}, {rov.c[0], Hv}});
   const std::complex<double> Nh = t[0].tr, Nv = t[1].tr;
   *Na = (Nh + Nv) / 2.0;
@@ -478,22 +306,21 @@ void gs_energy(Env& e, const Tensor& Hh, const Tensor& Hv, std::complex<double>*
 double es_energy(Env& e, const Tensor& Hh, const Tensor& Hv) {
   Ctx& c = *e.ctx;
   IPEPS_CHECK(e.nested, "es_energy: no B set");
+  NTPolicy p{c};
   NT C1 = e.all_C(0), C2 = e.all_C(1), C3 = e.all_C(2), C4 = e.all_C(3);
   NT E1 = e.all_E(0), E2 = e.all_E(1), E3 = e.all_E(2), E4 = e.all_E(3);
   NT A = e.all_A(), Ad = e.all_Ad();
   const double px = e.px, py = e.py;
-  NT roh = get_dm_h(c, C1, nshift(c, C2, px), nshift(c, C3, px), C4, E1, nshift(c, E1, px), nshift(c, E2, px), E3,
+  NT roh = get_dm_h(p, C1, nshift(c, C2, px), nshift(c, C3, px), C4, E1, nshift(c, E1, px), nshift(c, E2, px), E3,
                     nshift(c, E3, px), E4, A, nshift(c, A, px), Ad, nshift(c, Ad, px));
-  NT rov = get_dm_v(c, C1, C2, nshift(c, C3, py), nshift(c, C4, py), E1, E2, nshift(c, E2, py), nshift(c, E3, py),
+  NT rov = get_dm_v(p, C1, C2, nshift(c, C3, py), nshift(c, C4, py), E1, E2, nshift(c, E2, py), nshift(c, E3, py),
                     E4, nshift(c, E4, py), A, nshift(c, A, py), Ad, nshift(c, Ad, py));
   std::vector<std::pair<Tensor, Tensor>> items;
   std::vector<int> which;
-  for (int i = 0; i < 4; ++i) {
+  for (int i = 0; i < 4; ++i)
     if (roh.has(i)) { items.push_back({roh.c[i], Hh}); which.push_back(i); }
-  }
-  for (int i = 0; i < 4; ++i) {
+  for (int i = 0; i < 4; ++i)
     if (rov.has(i)) { items.push_back({rov.c[i], Hv}); which.push_back(4 + i); }
-  }
   auto t = dm_traces(c, items);
   std::complex<double> trHh[4] = {}, trHv[4] = {}, trh0 = 0, trv0 = 0;
   for (size_t i = 0; i < items.size(); ++i) {
@@ -506,18 +333,6 @@ double es_energy(Env& e, const Tensor& Hh, const Tensor& Hv) {
   return E4v.real();
 }
 
-// evaluation.jl:110-122
-static NT get_single_dm(Ctx& c, const NT& C1, const NT& C2, const NT& C3, const NT& C4, const NT& E1, const NT& E2,
-                        const NT& E3, const NT& E4) {
-  NT C1E1 = ntcon(c, C1, {-1, 1}, E1, {1, -2, -3, -4});
-  NT CEC2 = ntcon(c, C1E1, {-1, 1, -3, -4}, C2, {1, -2});
-  NT CECE4 = ntcon(c, CEC2, {1, -2, -3, -5}, E4, {1, -1, -4, -6});
-  NT C4E3 = ntcon(c, C4, {-1, 1}, E3, {1, -2, -3, -4});
-  NT CEC3 = ntcon(c, C4E3, {-1, 1, -3, -4}, C3, {-2, 1});
-  NT CECE2 = ntcon(c, CEC3, {-1, 1, -3, -5}, E2, {-2, 1, -4, -6});
-  return ntcon(c, CECE4, {1, 2, -1, -2, -5, -6}, CECE2, {1, 2, -3, -4, -7, -8});
-}
-
 static std::complex<double> scalar_of(Ctx& c, const Tensor& t) {
   double h[2] = {0, 0};
   IPEPS_CUDA(cudaMemcpyAsync(h, t.data(), t.dt == DType::F64 ? 8 : 16, cudaMemcpyDeviceToHost, c.stream));
@@ -528,7 +343,9 @@ static std::complex<double> scalar_of(Ctx& c, const Tensor& t) {
 // evaluation.jl:47-59
 std::complex<double> gs_norm(Env& e) {
   Ctx& c = *e.ctx;
-  NT n_dm = get_single_dm(c, e.Cs[0], e.Cs[1], e.Cs[2], e.Cs[3], e.Es[0], e.Es[1], e.Es[2], e.Es[3]);
+  NTPolicy p{c};
+  NT n_dm = get_single_dm(p, NT(e.Cs[0]), NT(e.Cs[1]), NT(e.Cs[2]), NT(e.Cs[3]), NT(e.Es[0]), NT(e.Es[1]),
+                          NT(e.Es[2]), NT(e.Es[3]));
   Tensor ndm_Ad = tcon(c, n_dm.c[0], {-1, -2, -3, -4, 1, 2, 3, 4}, e.Ad, {1, 2, 3, 4, -5});
   Tensor nrm0 = tcon(c, ndm_Ad, {1, 2, 3, 4, 5}, e.A, {1, 2, 3, 4, 5});
   return scalar_of(c, nrm0);
@@ -538,7 +355,8 @@ std::complex<double> gs_norm(Env& e) {
 std::complex<double> all_norm(Env& e, Tensor* envB) {
   Ctx& c = *e.ctx;
   IPEPS_CHECK(e.nested, "all_norm: no B set");
-  NT n_dm = get_single_dm(c, e.all_C(0), e.all_C(1), e.all_C(2), e.all_C(3), e.all_E(0), e.all_E(1), e.all_E(2),
+  NTPolicy p{c};
+  NT n_dm = get_single_dm(p, e.all_C(0), e.all_C(1), e.all_C(2), e.all_C(3), e.all_E(0), e.all_E(1), e.all_E(2),
                           e.all_E(3));
   NT ndm_A = ntcon(c, n_dm, {1, 2, 3, 4, -1, -2, -3, -4}, e.all_A(), {1, 2, 3, 4, -5});
   NT all = ntcon(c, ndm_A, {1, 2, 3, 4, 5}, e.all_Ad(), {1, 2, 3, 4, 5});

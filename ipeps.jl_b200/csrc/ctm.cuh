@@ -67,8 +67,15 @@ struct Env {
 };
 
 void init_ctm1(Env& e);
-// one directional move; dir 0=left 1=right 2=top 3=bottom; returns s (host)
-std::vector<double> ctm_move(Env& e, int dir);
+// one directional move; dir 0=left 1=right 2=top 3=bottom; returns s (host).
+// keep (optional) receives the projector with its resolved singular triplets.
+std::vector<double> ctm_move(Env& e, int dir, ProjResult* keep = nullptr);
+
+struct Traces {
+  std::complex<double> trH, tr;
+};
+// tr(H rho) and tr(rho) of several (rho, H) pairs (FP64, one host round trip)
+std::vector<Traces> dm_traces(Ctx& c, const std::vector<std::pair<Tensor, Tensor>>& items);
 std::vector<double> rg_step(Env& e);
 // energy (evaluation.jl:15-29): E (complex) and Na (complex)
 void gs_energy(Env& e, const Tensor& Hh, const Tensor& Hv, std::complex<double>* E, std::complex<double>* Na);

@@ -42,6 +42,7 @@ struct Ctx {
   std::array<KStat, int(KFam::Count)> stats{};
   uint64_t jacobi_sweeps = 0;
   uint64_t projector_calls = 0;
+  uint64_t projector_extra_passes = 0;
   // split-K partial sums live here (grown on demand, stream ordered)
   std::shared_ptr<DBuf> ws;
   // small device scalars (max-abs, traces, status words)

@@ -379,11 +379,15 @@ __global__ void __launch_bounds__(1024) cholinv_packed_kernel(double* G, int k, 
 
 // One-sided Jacobi with the m x k matrix X resident in shared memory (J in
 // global memory).  Same ordering and rotation as jacobi_kernel.
-__global__ void __launch_bounds__(1024) jacobi_smem_kernel(double* Xg, int m, int k, int64_t ldx, double* J,
-                                                           int64_t ldj, double* S, int max_sweeps, double tol,
+template <bool J_SMEM>
+__global__ void __launch_bounds__(1024) jacobi_smem_kernel(double* Xg, int m, int k, int64_t ldx, double* Jg,
+                                                           int64_t ldjg, double* S, int max_sweeps, double tol,
                                                            int* status, int* sweeps_out) {
   extern __shared__ double X[];
   __shared__ double s_off;
+  // J lives after X in shared memory when it fits, else in global memory
+  double* J = J_SMEM ? X + int64_t(m) * k : Jg;
+  const int64_t ldj = J_SMEM ? k : ldjg;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
   for (int j = warp; j < k; j += nwarps)
     for (int i = lane; i < m; i += 32) X[i + j * m] = Xg[i + int64_t(j) * ldx];
@@ -449,6 +453,11 @@ __global__ void __launch_bounds__(1024) jacobi_smem_kernel(double* Xg, int m, in
     a = warp_sum2(a);
     if (lane == 0) S[j] = sqrt(a);
   }
+  if (J_SMEM)
+    for (int64_t t = threadIdx.x; t < int64_t(k) * k; t += blockDim.x) {
+      const int i = int(t % k), j = int(t / k);
+      Jg[i + j * ldjg] = J[i + j * ldj];
+    }
   if (threadIdx.x == 0) {
     if (!converged) atomicOr(status, 4);
     if (sweeps_out) *sweeps_out = sweep;
@@ -457,7 +466,7 @@ __global__ void __launch_bounds__(1024) jacobi_smem_kernel(double* Xg, int m, in
 
 // opt-in limit per block is 227 KB including static shared memory; keep 1 KB for the kernels' own
 constexpr size_t kMaxDynSmem = 226 * 1024;
-bool g_cholinv_attr = false, g_jacobi_attr = false;
+bool g_cholinv_attr = false, g_jacobi_attr = false, g_jacobi2_attr = false;
 
 }  // namespace
 
@@ -471,7 +480,8 @@ void chol_inv_upper(Ctx& c, double* G, int k, int64_t ldg, double shift_factor, 
   }
   ProfScope ps(c, KFam::SmallLinalg);
   const size_t smem = (size_t(k) * (k + 1) / 2 + k) * 8;
-  cholinv_packed_kernel<<<1, 1024, smem, c.stream>>>(G, k, ldg, shift_factor, Rinv, ldr);
+  // four warps: the two barriers per column dominate and are cheap for 128 threads
+  cholinv_packed_kernel<<<1, 128, smem, c.stream>>>(G, k, ldg, shift_factor, Rinv, ldr);
   IPEPS_LAUNCH_CHECK();
   c.count(KFam::SmallLinalg, 2.0 * double(k) * k * k / 3.0);
 }
@@ -479,14 +489,28 @@ void chol_inv_upper(Ctx& c, double* G, int k, int64_t ldg, double shift_factor, 
 void jacobi_svd_auto(Ctx& c, double* X, int m, int k, int64_t ldx, double* J, int64_t ldj, double* S,
                      int max_sweeps, double tol, int* d_sweeps) {
   const size_t smem = size_t(m) * k * 8;
+  const size_t smem2 = smem + size_t(k) * k * 8;
   if (tol <= 0) tol = double(m) * 2.220446049250313e-16;  // rounding level of the column dot products
-  if (smem <= kMaxDynSmem) {
+  if (smem2 <= kMaxDynSmem) {
+    if (!g_jacobi2_attr) {
+      IPEPS_CUDA(cudaFuncSetAttribute(jacobi_smem_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      int(kMaxDynSmem)));
+      g_jacobi2_attr = true;
+    }
+    ProfScope ps(c, KFam::Jacobi);
+    jacobi_smem_kernel<true><<<1, 1024, smem2, c.stream>>>(X, m, k, ldx, J, ldj, S, max_sweeps, tol, c.d_status,
+                                                           d_sweeps);
+    IPEPS_LAUNCH_CHECK();
+    c.count(KFam::Jacobi, 6.0 * double(m + k) * k * k / 2.0);
+  } else if (smem <= kMaxDynSmem) {
     if (!g_jacobi_attr) {
-      IPEPS_CUDA(cudaFuncSetAttribute(jacobi_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kMaxDynSmem)));
+      IPEPS_CUDA(cudaFuncSetAttribute(jacobi_smem_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      int(kMaxDynSmem)));
       g_jacobi_attr = true;
     }
     ProfScope ps(c, KFam::Jacobi);
-    jacobi_smem_kernel<<<1, 1024, smem, c.stream>>>(X, m, k, ldx, J, ldj, S, max_sweeps, tol, c.d_status, d_sweeps);
+    jacobi_smem_kernel<false><<<1, 1024, smem, c.stream>>>(X, m, k, ldx, J, ldj, S, max_sweeps, tol, c.d_status,
+                                                           d_sweeps);
     IPEPS_LAUNCH_CHECK();
     c.count(KFam::Jacobi, 6.0 * double(m + k) * k * k / 2.0);
   } else {

@@ -5,11 +5,14 @@
 // randomized range finder with power iterations works on R1 (R2 X) and
 // R2^T (R1^T X) (all GEMMs), the sketches are orthonormalised by shifted
 // CholeskyQR in FP64, and the projected k x k matrix is diagonalised by a
-// one-sided Jacobi SVD in FP64 (k = n+1 plus oversampling).  The previous
-// right singular vectors of the same direction seed the sketch (warm start),
-// which near the CTMRG fixed point leaves the Jacobi almost nothing to do.
-// Sorting, the relative cutoff 1e-12 and the degenerate-pair rule are applied
-// exactly as in cutoff_matrix.
+// one-sided Jacobi SVD in FP64 (k = n+1 plus oversampling).  Accuracy is
+// checked a posteriori: the residual ||M v_i - s_i u_i|| of every kept
+// triplet (the part of M v_i outside the sketch) must be below
+// resid_tol * s_1, otherwise one more power iteration runs, warm-started from
+// the current vectors.  The resolved right vectors of the last call of the
+// same direction seed the next sketch, which near the CTMRG fixed point makes
+// one pass sufficient.  Sorting, the relative cutoff 1e-12 and the
+// degenerate-pair rule follow cutoff_matrix exactly.
 #include "linalg.cuh"
 #include "projector.cuh"
 
@@ -87,8 +90,58 @@ Tensor orth(Ctx& c, const Tensor& Y0, int passes, Tensor* Rout) {
   return Y;
 }
 
+namespace {
+
+// max over columns j < nc of ||X[:, j]|| (FP64, one warp per column)
+__global__ void colnorm_max_kernel(const double* X, int64_t m, int nc, unsigned long long* out) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (warp >= nc) return;
+  double s = 0;
+  for (int64_t i = lane; i < m; i += 32) s = fma(X[i + warp * m], X[i + warp * m], s);
+  for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (lane == 0) atomicMax(out, static_cast<unsigned long long>(__double_as_longlong(sqrt(s))));
+}
+
+// One sketch pass: range finder with q power iterations from Omega, Rayleigh-Ritz, Jacobi.
+struct Sketch {
+  Tensor Q, Q2, X, J, Ss;  // Q, Q2: N x k; X = W (k x k); J (k x k); Ss sorted S (k)
+  Tensor perm;             // int[k] stored in a double buffer
+  int sweeps = 0;
+};
+
+Sketch sketch_pass(Ctx& c, const MatRef& R1, const MatRef& R2, const Tensor& Om, int q, const SvdParams& sp) {
+  const int64_t N = R1.rows();
+  const int k = int(Om.dims[1]);
+  Sketch s;
+  Tensor Y = apply(c, R1, 'N', apply(c, R2, 'N', Om));
+  for (int it = 0; it < q; ++it) {
+    Tensor Q = orth(c, Y, 2, nullptr);
+    Tensor Z = orth(c, apply(c, R2, 'T', apply(c, R1, 'T', Q)), 2, nullptr);
+    Y = apply(c, R1, 'N', apply(c, R2, 'N', Z));
+  }
+  s.Q = orth(c, Y, 3, nullptr);
+  // B^T = M^T Q (N x k);  B^T = Q2 R  =>  B = R^T Q2^T
+  Tensor Bt = apply(c, R2, 'T', apply(c, R1, 'T', s.Q));
+  Tensor Rm;
+  s.Q2 = orth(c, Bt, 3, &Rm);
+  // X = R^T ; one-sided Jacobi: X J = W = Ux S  =>  U = Q Ux, V = Q2 J
+  s.X = permute(c, Rm, {1, 0});
+  s.J = c.alloc(DType::F64, {k, k});
+  Tensor S = c.alloc(DType::F64, {k});
+  int* d_sweeps = reinterpret_cast<int*>(static_cast<char*>(c.scal->p) + 3900);
+  jacobi_svd_auto(c, s.X.f64(), k, k, k, s.J.f64(), k, S.f64(), sp.jacobi_max_sweeps, sp.jacobi_tol, d_sweeps);
+  s.Ss = c.alloc(DType::F64, {k});
+  s.perm = c.alloc(DType::F64, {(k + 1) / 2});
+  sort_desc(c, S.f64(), k, s.Ss.f64(), static_cast<int*>(s.perm.data()));
+  IPEPS_CUDA(cudaMemcpyAsync(&s.sweeps, d_sweeps, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+  (void)N;
+  return s;
+}
+
+}  // namespace
+
 ProjResult get_projector(Ctx& c, const MatRef& R1, const MatRef& R2, int chi, const SvdParams& sp,
-                         ProjCache* cache) {
+                         ProjCache* cache, bool keep_factors) {
   const int64_t N = R1.rows();
   IPEPS_CHECK(R1.cols() == R2.rows() && R2.cols() == N, "get_projector: R1*R2 must be square");
   IPEPS_CHECK(R1.t.dt == DType::F64 && R2.t.dt == DType::F64, "get_projector: real operands expected");
@@ -97,7 +150,7 @@ ProjResult get_projector(Ctx& c, const MatRef& R1, const MatRef& R2, int chi, co
   int over = std::max(sp.min_oversample, want * sp.oversample_num / std::max(sp.oversample_den, 1));
   const int k = int(std::min<int64_t>(N, int64_t(want) + over));
 
-  // sketch Omega (N x k): previous V of this direction first, then Gaussian columns
+  // sketch Omega (N x k): resolved right vectors of the previous call first, then Gaussian columns
   Tensor Om = c.alloc(DType::F64, {N, k});
   randn(c, Om);
   bool warm = false;
@@ -106,69 +159,99 @@ ProjResult get_projector(Ctx& c, const MatRef& R1, const MatRef& R2, int chi, co
     IPEPS_CUDA(cudaMemcpyAsync(Om.data(), cache->V.data(), size_t(N) * nv * 8, cudaMemcpyDeviceToDevice, c.stream));
     warm = true;
   }
-  const int q = (k == N) ? 0 : (warm ? sp.power_iters_warm : sp.power_iters);
-
-  Tensor Y = apply(c, R1, 'N', apply(c, R2, 'N', Om));
-  for (int it = 0; it < q; ++it) {
-    Tensor Q = orth(c, Y, 2, nullptr);
-    Tensor Z = orth(c, apply(c, R2, 'T', apply(c, R1, 'T', Q)), 2, nullptr);
-    Y = apply(c, R1, 'N', apply(c, R2, 'N', Z));
-  }
-  Tensor Q = orth(c, Y, 3, nullptr);
-  // B^T = M^T Q (N x k);  B^T = Q2 R  =>  B = R^T Q2^T
-  Tensor Bt = apply(c, R2, 'T', apply(c, R1, 'T', Q));
-  Tensor Rm;
-  Tensor Q2 = orth(c, Bt, 3, &Rm);
-  // X = R^T ; one-sided Jacobi: X J = W = Ux S  =>  U = Q Ux, V = Q2 J
-  Tensor X = permute(c, Rm, {1, 0});
-  Tensor J = c.alloc(DType::F64, {k, k});
-  Tensor S = c.alloc(DType::F64, {k});
-  int* d_sweeps = reinterpret_cast<int*>(static_cast<char*>(c.scal->p) + 3900);
-  jacobi_svd_auto(c, X.f64(), k, k, k, J.f64(), k, S.f64(), sp.jacobi_max_sweeps, sp.jacobi_tol, d_sweeps);
-  Tensor Ss = c.alloc(DType::F64, {k});
-  Tensor perm = c.alloc(DType::F64, {(k + 1) / 2});  // int storage
-  int* d_perm = static_cast<int*>(perm.data());
-  sort_desc(c, S.f64(), k, Ss.f64(), d_perm);
+  int q = (k == N) ? 0 : (warm ? sp.power_iters_warm : sp.power_iters);
 
   ProjResult r;
   r.k = k;
-  r.s_host.resize(k);
-  int sweeps = 0;
-  IPEPS_CUDA(cudaMemcpyAsync(r.s_host.data(), Ss.data(), size_t(k) * 8, cudaMemcpyDeviceToHost, c.stream));
-  IPEPS_CUDA(cudaMemcpyAsync(&sweeps, d_sweeps, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
-  c.sync();
-  r.sweeps = sweeps;
-  c.jacobi_sweeps += uint64_t(sweeps);
-  c.projector_calls++;
-
-  // cutoff_matrix (wrapper.jl:37-55)
-  const double smax = r.s_host[0];
-  int n_above = 0;
-  for (int i = 0; i < k; ++i)
-    if (smax > 0 && r.s_host[i] / smax > 1e-12) n_above++;
-  int n = std::min(new_chi, n_above);
-  IPEPS_CHECK(n >= 1, "get_projector: no singular value above the cutoff (zero enlarged corner?)");
-  // the reference's s has length N (full SVD); ours is the top-k part, k > n whenever N > n
-  if (int64_t(N) > n && k > n) {
-    if (std::fabs(r.s_host[n] - r.s_host[n - 1]) < 1e-10) n = n + 1;
+  Sketch sk;
+  std::vector<double> all(k);
+  int n = 0;
+  Tensor Ux, Vk;
+  int* d_perm = nullptr;
+  double* d_res = reinterpret_cast<double*>(c.scal->p) + 48;
+  for (int attempt = 0;; ++attempt) {
+    sk = sketch_pass(c, R1, R2, Om, q, sp);
+    d_perm = static_cast<int*>(sk.perm.data());
+    IPEPS_CUDA(cudaMemcpyAsync(all.data(), sk.Ss.data(), size_t(k) * 8, cudaMemcpyDeviceToHost, c.stream));
+    c.sync();
+    c.jacobi_sweeps += uint64_t(sk.sweeps);
+    // cutoff_matrix (wrapper.jl:37-55)
+    const double smax = all[0];
+    int n_above = 0;
+    for (int i = 0; i < k; ++i)
+      if (smax > 0 && all[i] / smax > 1e-12) n_above++;
+    n = std::min(new_chi, n_above);
+    IPEPS_CHECK(n >= 1, "get_projector: no singular value above the cutoff (zero enlarged corner?)");
+    // the reference's s has length N (full SVD); ours is the top-k part, k > n whenever N > n
+    if (int64_t(N) > n && k > n) {
+      if (std::fabs(all[n] - all[n - 1]) < 1e-10) n = n + 1;
+    }
+    IPEPS_CHECK(n <= k, "get_projector: truncation beyond the sketch");
+    // Ux[:, j] = W[:, perm[j]] / S_sorted[j] (kept + one), Vk = Q2 J[:, perm]
+    const int nc = std::min(n + 1, k);
+    Ux = c.alloc(DType::F64, {k, nc});
+    gather_cols(c, sk.X.f64(), k, k, d_perm, nc, sk.Ss.f64(), 2, Ux.f64(), k);
+    Tensor Js = c.alloc(DType::F64, {k, k});
+    gather_cols(c, sk.J.f64(), k, k, d_perm, k, nullptr, 0, Js.f64(), k);
+    Vk = c.alloc(DType::F64, {N, k});
+    gemm(c, DType::F64, 'N', 'N', N, k, k, cplx(1), sk.Q2.data(), N, Js.data(), k, cplx(0), Vk.data(), N, true);
+    if (q == 0 && k == N) break;  // the sketch spans everything: exact
+    if (attempt >= sp.max_extra_passes) break;
+    // residual of the kept triplets: ||M v_i - s_i u_i|| <= resid_tol * s_1
+    Tensor Vc = c.alloc(DType::F64, {N, nc});
+    IPEPS_CUDA(cudaMemcpyAsync(Vc.data(), Vk.data(), size_t(N) * nc * 8, cudaMemcpyDeviceToDevice, c.stream));
+    Tensor Res = apply(c, R1, 'N', apply(c, R2, 'N', Vc));
+    Tensor Us = c.alloc(DType::F64, {k, nc});
+    gather_cols(c, sk.X.f64(), k, k, d_perm, nc, nullptr, 0, Us.f64(), k);  // W = Ux S
+    gemm(c, DType::F64, 'N', 'N', N, nc, k, cplx(-1), sk.Q.data(), N, Us.data(), k, cplx(1), Res.data(), N, true);
+    IPEPS_CUDA(cudaMemsetAsync(d_res, 0, 8, c.stream));
+    colnorm_max_kernel<<<(nc * 32 + 255) / 256, 256, 0, c.stream>>>(Res.f64(), N, nc,
+                                                                    reinterpret_cast<unsigned long long*>(d_res));
+    IPEPS_LAUNCH_CHECK();
+    double res = 0;
+    IPEPS_CUDA(cudaMemcpyAsync(&res, d_res, 8, cudaMemcpyDeviceToHost, c.stream));
+    c.sync();
+    if (res <= sp.resid_tol * smax) break;
+    // not converged: one more power iteration from the current right vectors
+    Om = Vk;
+    q = 1;
+    c.projector_extra_passes++;
   }
-  IPEPS_CHECK(n <= k, "get_projector: truncation beyond the sketch");
+  r.sweeps = sk.sweeps;
+  c.projector_calls++;
   r.n = n;
-  r.s_host.resize(n);
+  r.s_host.assign(all.begin(), all.begin() + n);
 
-  // Ux[:, j] = W[:, perm[j]] / S_sorted[j] ; Js[:, j] = J[:, perm[j]]
-  Tensor Ux = c.alloc(DType::F64, {k, n});
-  gather_cols(c, X.f64(), k, k, d_perm, n, Ss.f64(), 2, Ux.f64(), k);
-  Tensor Js = c.alloc(DType::F64, {k, n});
-  gather_cols(c, J.f64(), k, k, d_perm, n, nullptr, 0, Js.f64(), k);
   Tensor U = c.alloc(DType::F64, {N, n});
-  gemm(c, DType::F64, 'N', 'N', N, n, k, cplx(1), Q.data(), N, Ux.data(), k, cplx(0), U.data(), N, true);
+  gemm(c, DType::F64, 'N', 'N', N, n, k, cplx(1), sk.Q.data(), N, Ux.data(), k, cplx(0), U.data(), N, true);
   Tensor V = c.alloc(DType::F64, {N, n});
-  gemm(c, DType::F64, 'N', 'N', N, n, k, cplx(1), Q2.data(), N, Js.data(), k, cplx(0), V.data(), N, true);
-  if (cache) cache->V = clone(c, V);
+  IPEPS_CUDA(cudaMemcpyAsync(V.data(), Vk.data(), size_t(N) * n * 8, cudaMemcpyDeviceToDevice, c.stream));
+  // resolved part of the sketch: s_a > 1e-13 s_1 (W/s is accurate there)
+  int rr = 0;
+  while (rr < k && all[rr] > 1e-13 * all[0]) ++rr;
+  rr = std::max(rr, n);
+  if (cache) {
+    // seed for the next call of this direction: the resolved right vectors only
+    // (near-null directions of this M say nothing about the next one)
+    Tensor Vc = c.alloc(DType::F64, {N, rr});
+    IPEPS_CUDA(cudaMemcpyAsync(Vc.data(), Vk.data(), size_t(N) * rr * 8, cudaMemcpyDeviceToDevice, c.stream));
+    cache->V = Vc;
+  }
+  if (keep_factors) {
+    r.r = rr;
+    r.sr_host.assign(all.begin(), all.begin() + rr);
+    Tensor Uxr = c.alloc(DType::F64, {k, rr});
+    gather_cols(c, sk.X.f64(), k, k, d_perm, rr, sk.Ss.f64(), 2, Uxr.f64(), k);
+    r.Ur = c.alloc(DType::F64, {N, rr});
+    gemm(c, DType::F64, 'N', 'N', N, rr, k, cplx(1), sk.Q.data(), N, Uxr.data(), k, cplx(0), r.Ur.data(), N, true);
+    r.Vr = c.alloc(DType::F64, {N, rr});
+    IPEPS_CUDA(cudaMemcpyAsync(r.Vr.data(), Vk.data(), size_t(N) * rr * 8, cudaMemcpyDeviceToDevice, c.stream));
+    r.Sr = c.alloc(DType::F64, {rr});
+    IPEPS_CUDA(cudaMemcpyAsync(r.Sr.data(), sk.Ss.data(), size_t(rr) * 8, cudaMemcpyDeviceToDevice, c.stream));
+  }
 
   r.S = c.alloc(DType::F64, {n});
-  IPEPS_CUDA(cudaMemcpyAsync(r.S.data(), Ss.data(), size_t(n) * 8, cudaMemcpyDeviceToDevice, c.stream));
+  IPEPS_CUDA(cudaMemcpyAsync(r.S.data(), sk.Ss.data(), size_t(n) * 8, cudaMemcpyDeviceToDevice, c.stream));
   // P1 = R2 V S^-1/2 ; P2 = S^-1/2 U^T R1
   scale_cols(c, V.f64(), N, N, n, r.S.f64(), 1);
   scale_cols(c, U.f64(), N, N, n, r.S.f64(), 1);

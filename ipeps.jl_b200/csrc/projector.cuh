@@ -15,10 +15,12 @@ struct MatRef {
 
 struct SvdParams {
   int oversample_num = 1;   // k = want + max(min_oversample, want*num/den)
-  int oversample_den = 1;
+  int oversample_den = 2;
   int min_oversample = 16;
-  int power_iters = 4;      // cold start
-  int power_iters_warm = 2; // when the previous V of this direction seeds the sketch
+  int power_iters = 3;      // cold start
+  int power_iters_warm = 1; // when the previous V of this direction seeds the sketch
+  int max_extra_passes = 6; // extra power iterations while the residual check fails
+  double resid_tol = 1e-13; // ||M v_i - s_i u_i|| <= resid_tol * s_1 for the kept triplets
   bool warm_start = true;
   int jacobi_max_sweeps = 40;
   double jacobi_tol = 0.0;  // <= 0: m * eps (rounding level of the column dot products)
@@ -37,13 +39,18 @@ struct ProjResult {
   int n = 0;
   int k = 0;
   int sweeps = 0;
+  // resolved singular triplets of the sketch (kept ones first), for the
+  // adjoint: r columns with s_a > 1e-13 s_1
+  int r = 0;
+  Tensor Ur, Vr, Sr;  // N x r, N x r, r
+  std::vector<double> sr_host;
 };
 
 // Returns P1 = R2 V S^-1/2, P2 = S^-1/2 U^T R1 with (U,S,V) the truncated
 // SVD of R1*R2 following wrap_svd/cutoff_matrix (keep min(chi, #{s/smax >
 // 1e-12}), plus one when |s[n+1]-s[n]| < 1e-10).
 ProjResult get_projector(Ctx& c, const MatRef& R1, const MatRef& R2, int chi, const SvdParams& sp,
-                         ProjCache* cache);
+                         ProjCache* cache, bool keep_factors = false);
 
 // op(R)*X with R a MatRef; op in {'N','T'}
 Tensor apply(Ctx& c, const MatRef& R, char op, const Tensor& X);

@@ -40,7 +40,7 @@ EXPORTED = [
     "ipeps_env_get_CT", "ipeps_env_set_CT", "ipeps_ctm_move", "ipeps_ctm_step", "ipeps_ctm_run",
     "ipeps_ctm_log", "ipeps_energy", "ipeps_gs_norm", "ipeps_nested_set_B", "ipeps_es_energy",
     "ipeps_all_norm", "ipeps_tcon", "ipeps_projector", "ipeps_ctx_stream", "ipeps_prof_enable",
-    "ipeps_prof_query",
+    "ipeps_prof_query", "ipeps_energy_grad",
 ]
 
 
@@ -109,6 +109,7 @@ def load_library(path: str = LIB_PATH) -> ct.CDLL:
         "ipeps_ctx_stream": [P, ct.POINTER(P)],
         "ipeps_prof_enable": [P, I],
         "ipeps_prof_query": [P, dp, ct.POINTER(ct.c_uint64), dp, dp],
+        "ipeps_energy_grad": [P, dp, dp, I, I, dp, dp],
     }
     for name, args in sig.items():
         f = getattr(lib, name)
@@ -264,8 +265,8 @@ class CTMTensors:
         self.engine.check(self.lib.ipeps_env_set_params(
             self.h, int(p.get("chi", 30)), int(p.get("min_iter", 4)), int(p.get("max_iter", 20)),
             int(p.get("ad_max_iter", 4)), float(p.get("rg_tol", 1e-6))))
-        over = p.get("svd_oversample", (1, 1, 16))
-        pit = p.get("svd_power_iters", (4, 2))
+        over = p.get("svd_oversample", (1, 2, 16))
+        pit = p.get("svd_power_iters", (3, 1))
         self.engine.check(self.lib.ipeps_env_set_svd_params(
             self.h, int(over[0]), int(over[1]), int(over[2]), int(pit[0]), int(pit[1]),
             int(bool(p.get("svd_warm_start", True)))))
@@ -459,6 +460,32 @@ def get_all_norm(ts: CTMTensors):
     envB = np.empty(ts.A.shape, dtype=np.complex128, order="F")
     ts.engine.check(ts.lib.ipeps_all_norm(ts.h, _dp(nb), _dp(envB)))
     return complex(nb[0], nb[1]), envB
+
+
+def energy_grad(ts: CTMTensors, H, ad_iters: Optional[int] = None):
+    """Pullback of run_gs (optim_gs.jl:133-143) from the environment held by ts:
+    returns (real(E), dE/dA) with dE/dA a real (D,D,D,D,d) array."""
+    Hh, Hv, d2 = _H_pair(H)
+    n = int(ts.Params.get("ad_max_iter", 4) if ad_iters is None else ad_iters)
+    ts._push_params()
+    E = np.zeros(1)
+    g = np.empty(ts.A.shape, dtype=np.float64, order="F")
+    ts.engine.check(ts.lib.ipeps_energy_grad(ts.h, _dp(Hh), _dp(Hv), d2, n, _dp(E), _dp(g)))
+    return float(E[0]), g
+
+
+def fg(x, H, cfg, engine: Optional[Engine] = None):
+    """E+grad unit of optim_gs (fg!, optim_gs.jl:53-91): x is renormalised
+    (max-abs), CTMRG converges from init_ctm1 with the energy criterion
+    (get_conv_boundary, :120-131), then the pullback of ad_max_iter further
+    iterations + get_gs_energy gives (E, dE/dx).  Returns (E, g, info)."""
+    x = np.asarray(x, dtype=np.float64)
+    x = x / np.abs(x).max()
+    ts = CTMTensors(x, cfg, engine=engine)
+    ts, info = run_ctm(ts, conv_fun="energy", H=H)
+    E, g = energy_grad(ts, H)
+    ts.close()
+    return E, g, info
 
 
 def compute_gs_energy(A, H, cfg, engine: Optional[Engine] = None):
