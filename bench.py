@@ -1,17 +1,22 @@
 """Benchmark of the CTMRG hot path on B200.
 
 Workload (default): spin-1/2 Heisenberg (sublattice-rotated), single-site
-iPEPS A of shape (4,4,4,4,2), i.i.d. N(0,1) seeded, max|A| = 1, chi = 64;
-one step = init_ctm1 + 30 CTMRG iterations (4 directional moves each) with the
-energy evaluated every iteration (the reference's conv_fun), i.e. 120 moves.
+iPEPS A of shape (4,4,4,4,2), i.i.d. N(0,1) seeded, max|A| = 1, chi = 64.
+One step = one energy+gradient evaluation (fg! of optim_gs): init_ctm1, 30
+CTMRG iterations (4 directional moves each) with the energy every iteration
+(the reference's conv_fun), then the pullback of ad_max_iter = 4 further
+iterations + the energy.  CTMRG moves/s is measured on the forward part alone
+and reported beside it.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|mixed]
     python bench.py --impl reference ...   # CPU arm (see below)
 
 Timing: K steps timed with CUDA events recorded on the engine's own stream,
-L2 flushed (512 MB write) between steps, max over ranks; value = moves/s of the
-whole job.  e2e = the same metric through the public API with host buffers
-(A and H copied in, energy copied out, inside the timed region).
+L2 flushed (512 MB write) between steps, max over ranks; value = E+grad
+evaluations/s of the whole job.  e2e = the same metric through the public API
+(fg) with host buffers: A and H copied in, energy and gradient copied out,
+inside the timed region.  Under torchrun each rank runs an independent
+replica (CTMRG does not shard).
 
 Reference arm: the reference is Julia, which is not installed, so
 ``--impl reference`` times the CPU FP64 oracle (a restatement of the
@@ -72,12 +77,14 @@ def heisenberg(Jz=1.0):
     return [H, H]
 
 
-WORKLOAD = dict(model="heisenberg", D=4, d=2, chi=64, iters=30)
+WORKLOAD = dict(model="heisenberg", D=4, d=2, chi=64, iters=30, ad_iters=4)
+WORKLOAD_NAME = ("heisenberg D=4 d=2 chi=64: E+grad evaluation = init_ctm1 + 30 CTMRG iterations with the energy "
+                 "per iteration + pullback of 4 iterations and the energy")
 
 
-def workload_cfg(pkg, chi, iters):
+def workload_cfg(pkg, chi, iters, ad_iters):
     cfg = pkg.default_config()
-    cfg.update(chi=chi, min_iter=iters, max_iter=iters, rg_tol=0.0)
+    cfg.update(chi=chi, min_iter=iters, max_iter=iters, rg_tol=0.0, ad_max_iter=ad_iters)
     return cfg
 
 
@@ -170,9 +177,12 @@ def measure_fp64_peak(torch):
     return 2.0 * n ** 3 / best / 1e12
 
 
-def cpu_oracle_sample(D, d, chi, seed, budget_s=15.0, threads=None):
-    """Time the CPU oracle on a bounded sample of the workload: init_ctm1 + as
-    many CTMRG iterations (with the energy) as fit in ~budget_s.  Returns moves/s."""
+def cpu_oracle_eg_sample(D, d, chi, seed, budget_s=12.0, threads=None):
+    """CPU oracle on a bounded sample of the workload.  Times (a) forward CTMRG
+    iterations with the energy (~budget_s) and (b) the pullback of one CTMRG
+    iteration + the energy (torch autograd with the reference's svd_back), and
+    extrapolates one E+grad evaluation = iters forward + ad_iters pullback
+    iterations.  Returns (evals/s, moves/s, sample description, threads)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import torch
     import ipeps_oracle as O
@@ -181,21 +191,30 @@ def cpu_oracle_sample(D, d, chi, seed, budget_s=15.0, threads=None):
     A = torch.tensor(random_A(D, d, seed))
     H = O.heisenberg(1.0)
     cfg = O.default_config()
-    cfg.update(chi=chi, min_iter=1, max_iter=1, rg_tol=0.0)
+    cfg.update(chi=chi, min_iter=1, max_iter=1, rg_tol=0.0, ad_max_iter=1)
     ts = O.make_ctm_tensors(A, cfg)
-    moves = 0
-    # first iterations have small chi: run two untimed to reach the full bond dimension
-    for _ in range(2):
+    for _ in range(2):  # first iterations have small chi
         ts, _ = O.rg_step(ts, chi)
     t0 = time.perf_counter()
+    it = 0
     while True:
         ts, _ = O.rg_step(ts, chi)
         O.get_gs_energy(ts, H)
-        moves += 4
+        it += 1
         if time.perf_counter() - t0 > budget_s:
             break
-    dt = time.perf_counter() - t0
-    return moves / dt, moves, dt, torch.get_num_threads()
+    t_iter = (time.perf_counter() - t0) / it
+    ts1 = O._detach_ts(ts)
+    xv = A.clone().requires_grad_(True)
+    t0 = time.perf_counter()
+    y = O.run_gs(ts1, H, xv)
+    torch.autograd.grad(y.real, xv)
+    t_ad = time.perf_counter() - t0
+    t_eval = WORKLOAD["iters"] * t_iter + WORKLOAD["ad_iters"] * t_ad
+    sample = (f"CPU oracle (torch float64, {torch.get_num_threads()} threads): {it} forward iterations "
+              f"({t_iter:.2f} s each) and one pullback iteration ({t_ad:.1f} s) timed; one E+grad evaluation = "
+              f"{WORKLOAD['iters']} x forward + {WORKLOAD['ad_iters']} x pullback = {t_eval:.1f} s")
+    return 1.0 / t_eval, 4.0 / t_iter, sample, torch.get_num_threads(), t_eval
 
 
 # ---------------------------------------------------------------- arms
@@ -205,26 +224,24 @@ def run_reference(args):
         return 0
     D, d, chi = WORKLOAD["D"], WORKLOAD["d"], WORKLOAD["chi"]
     threads = os.cpu_count() or 1
-    per_step = []
-    total_moves = 0
-    total_t = 0.0
+    vals, moves, ts = [], [], []
+    sample = ""
     for i in range(args.warmup + args.steps):
-        v, moves, dt, nth = cpu_oracle_sample(D, d, chi, seed=1000 + i, budget_s=args.ref_budget, threads=threads)
+        v, mv, sample, nth, t_eval = cpu_oracle_eg_sample(D, d, chi, seed=1000, budget_s=args.ref_budget,
+                                                          threads=threads)
         if i >= args.warmup:
-            per_step.append(dt)
-            total_moves += moves
-            total_t += dt
-    value = total_moves / total_t
-    sample = (f"CPU oracle (torch float64, {nth} threads): init_ctm1 + 2 untimed iterations, then CTMRG "
-              f"iterations with the energy for ~{args.ref_budget:.0f} s per step")
-    line = {"impl": "reference", "metric": "CTMRG moves/s (Heisenberg D=4 chi=64, FP64)", "value": value,
-            "unit": "moves/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 1e3 * total_t / max(args.steps, 1), "higher_is_better": True, "scaling": "weak",
+            vals.append(v)
+            moves.append(mv)
+            ts.append(t_eval)
+    value = len(ts) / sum(ts)
+    line = {"impl": "reference", "metric": "E+grad evals/s (Heisenberg D=4 chi=64, FP64)", "value": value,
+            "unit": "evals/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * sum(ts) / max(len(ts), 1), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "heisenberg D=4 d=2 chi=64: CTMRG iterations from init_ctm1", "D": D,
-                       "chi": chi, "sample": "bounded CPU sample, see cpu_baseline"},
-            "cpu_baseline": {"value": value, "unit": "moves/s", "cores": nth, "kind": "port", "sample": sample},
-            "e2e": {"value": value, "unit": "moves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "config": {"workload": WORKLOAD_NAME, "D": D, "chi": chi, "sample": "bounded CPU sample, see cpu_baseline"},
+            "moves_per_s": statistics.mean(moves),
+            "cpu_baseline": {"value": value, "unit": "evals/s", "cores": nth, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "reference_note": "iPEPS.jl is Julia; no Julia toolchain on this machine, so the CPU arm is the "
                               "oracle restatement of its algorithm"}
     print(json.dumps(line))
@@ -245,11 +262,11 @@ def run_ours(args):
 
     pkg = load_pkg()
     eng = pkg.Engine(local, precision=args.precision)
-    D, d, chi, iters = WORKLOAD["D"], WORKLOAD["d"], WORKLOAD["chi"], WORKLOAD["iters"]
-    cfg = workload_cfg(pkg, chi, iters)
+    D, d, chi, iters, ad_iters = (WORKLOAD[k] for k in ("D", "d", "chi", "iters", "ad_iters"))
+    cfg = workload_cfg(pkg, chi, iters, ad_iters)
     H = heisenberg(1.0)
     A = random_A(D, d, seed=1000 + rank)
-    moves_per_step = 4 * iters
+    moves_per_fwd = 4 * iters
 
     ext = torch.cuda.ExternalStream(eng.stream_ptr())
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
@@ -259,112 +276,114 @@ def run_ours(args):
             dist.barrier()
         torch.cuda.synchronize()
 
+    def max_over_ranks(t):
+        if world > 1:
+            tt = torch.tensor([t], device="cuda", dtype=torch.float64)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            return float(tt.item())
+        return t
+
     ts = pkg.CTMTensors(A, cfg, engine=eng)
 
-    def device_step():
+    def forward_step():
         # inputs resident: A already on the device; re-initialise and iterate
         eng.check(eng.lib.ipeps_env_init(ts.h))
         pkg.run_ctm(ts, conv_fun="energy", H=H)
+
+    def device_step():
+        forward_step()
+        return pkg.energy_grad(ts, H, ad_iters)
+
+    def timed(fn, k):
+        times = []
+        for _ in range(k):
+            flush.zero_()
+            torch.cuda.synchronize()
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record(ext)
+            fn()
+            e.record(ext)
+            e.synchronize()
+            times.append(s.elapsed_time(e) / 1e3)
+        return times
 
     for _ in range(args.warmup):
         device_step()
     barrier()
 
-    # ---- timed region (device): K steps, events on the engine stream, L2 flushed between steps
+    # ---- timed region: K E+grad evaluations, events on the engine stream, L2 flushed between steps
     eng.reset_stats()
     sampler = ClockSampler(local)
     sampler.start()
-    times = []
-    for _ in range(args.steps):
-        flush.zero_()
-        torch.cuda.synchronize()
-        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        s.record(ext)
-        device_step()
-        e.record(ext)
-        e.synchronize()
-        times.append(s.elapsed_time(e) / 1e3)
+    times = timed(device_step, args.steps)
     barrier()
     clocks = sampler.stop()
     st = eng.stats()
     launches = sum(f["launches"] for f in st["families"].values())
-    t_local = sum(times)
-    t_max = t_local
-    if world > 1:
-        tt = torch.tensor([t_local], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_max = float(tt.item())
-    total_moves = moves_per_step * args.steps * world
-    value = total_moves / t_max
+    t_max = max_over_ranks(sum(times))
+    value = args.steps * world / t_max
 
-    # ---- e2e: public API with host buffers (A, H in; energy out) each step
-    e2e_times = []
-    for _ in range(max(1, args.steps)):
-        flush.zero_()
-        torch.cuda.synchronize()
-        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        s.record(ext)
-        (E, Na), ts2, info = pkg.compute_gs_energy(A, H, cfg, engine=eng)
-        e.record(ext)
-        e.synchronize()
-        e2e_times.append(s.elapsed_time(e) / 1e3)
-        ts2.close()
+    # ---- forward only: CTMRG moves/s on the same workload
+    tf = max_over_ranks(sum(timed(forward_step, args.steps)))
+    moves_value = moves_per_fwd * args.steps * world / tf
+
+    # ---- e2e: public API with host buffers (A, H in; energy, gradient out) each step
+    def e2e_step():
+        pkg.fg(A, H, cfg, engine=eng)
+
+    te = max_over_ranks(sum(timed(e2e_step, max(1, args.steps))))
+    e2e_value = max(1, args.steps) * world / te
+    h2d = A.nbytes + 2 * H[0].nbytes * 2   # A, and H for the run and for the gradient call
+    d2h = A.nbytes + 8 + 32 * iters        # gradient, energy, per-iteration log
     barrier()
-    te = sum(e2e_times)
-    if world > 1:
-        tt = torch.tensor([te], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        te = float(tt.item())
-    e2e_value = moves_per_step * len(e2e_times) * world / te
-    h2d = A.nbytes + 2 * H[0].nbytes * (iters + 2)   # A once, H per energy call
-    d2h = 16 * 2 * (iters + 1) + 8 * 4 * chi * iters  # energies + left spectra
 
-    # ---- live per-kernel roofline: one profiled step (events around each launch)
+    # ---- live per-kernel profile of one E+grad step (events around each launch)
     eng.prof_enable(True)
     device_step()
     prof = eng.prof_query()
     eng.prof_enable(False)
 
-    out = None
     if rank == 0:
         peaks, peak_kind = measured_peaks()
         fp64_peak = measure_fp64_peak(torch)
-        g = prof["gemm_f64"] if args.precision == "fp64" else prof["gemm_tf32x3"]
+        total_ms = sum(f["ms"] for f in prof.values())
+        dom = max(prof.items(), key=lambda kv: kv[1]["ms"])
+        gname = "gemm_f64" if args.precision == "fp64" else "gemm_tf32x3"
+        g = prof[gname]
         achieved = g["flops"] / (g["ms"] / 1e3) / 1e12 if g["ms"] > 0 else 0.0
         if args.precision == "fp64":
             peak, peak_note = fp64_peak, "cuBLAS DGEMM 8192^3 measured in this run (FP64 has no entry in MEASURED_PEAKS.json)"
         else:
             peak, peak_note = peaks["bf16_tflops"] / 2 / 3, f"{peak_kind} bf16 / 2 (TF32) / 3 (three products)"
-        total_ms = sum(f["ms"] for f in prof.values())
         cpu = None
         if not args.no_cpu_baseline:
-            v, moves, dt, nth = cpu_oracle_sample(D, d, chi, seed=1000, budget_s=args.cpu_budget, threads=os.cpu_count())
-            cpu = {"value": v, "unit": "moves/s", "cores": nth, "kind": "port",
-                   "sample": f"CPU oracle (torch float64): {moves} moves of the same workload in {dt:.1f} s "
-                             f"after 2 untimed iterations"}
+            v, mv, sample, nth, _ = cpu_oracle_eg_sample(D, d, chi, seed=1000, budget_s=args.cpu_budget,
+                                                         threads=os.cpu_count())
+            cpu = {"value": v, "unit": "evals/s", "cores": nth, "kind": "port", "sample": sample, "moves_per_s": mv}
         out = {
-            "metric": "CTMRG moves/s (Heisenberg D=4 chi=64; E+grad evals/s reported separately when built)",
-            "value": value, "unit": "moves/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "metric": "E+grad evals/s (Heisenberg D=4 chi=64); CTMRG moves/s in moves_per_s",
+            "value": value, "unit": "evals/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f64 (3xTF32 contractions)",
             "data": "synthetic",
-            "config": {"workload": "heisenberg D=4 d=2 chi=64: init_ctm1 + 30 CTMRG iterations with the energy "
-                                   "per iteration (120 moves per step)",
-                       "precision": args.precision, "l2": "flushed between steps (512 MB write)",
-                       "replicas": world},
-            "e2e": {"value": e2e_value, "unit": "moves/s", "h2d_bytes_per_step": int(h2d),
+            "config": {"workload": WORKLOAD_NAME, "precision": args.precision,
+                       "l2": "flushed between steps (512 MB write)", "replicas": world},
+            "moves_per_s": moves_value,
+            "e2e": {"value": e2e_value, "unit": "evals/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": int(launches),
-            "roofline": {"bound": "tensor" if args.precision == "mixed" else "fp64",
+            "roofline": {"bound": "fp64" if args.precision == "fp64" else "tensor",
                          "kernel": "gemm_f64 (register-tiled DFMA)" if args.precision == "fp64" else "gemm_tf32x3",
                          "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": achieved / peak if peak else None, "traffic": None,
-                         "peak_source": peak_note, "kernel_share_of_device_time": g["ms"] / total_ms if total_ms else None,
+                         "frac": achieved / peak if peak else None, "traffic": None, "peak_source": peak_note,
+                         "kernel_share_of_device_time": g["ms"] / total_ms if total_ms else None,
                          "launches_in_profiled_step": g["launches"]},
+            "dominant_family": {"name": dom[0], "share_of_device_time": dom[1]["ms"] / total_ms if total_ms else None},
             "kernel_families_ms_profiled_step": {k: round(v["ms"], 3) for k, v in prof.items()},
+            "projector": {"calls": st["projector_calls"], "jacobi_sweeps_per_call":
+                          st["jacobi_sweeps"] / max(1, st["projector_calls"])},
             "cpu_baseline": cpu,
             "clocks": clocks,
-            "energy_last": [E.real, E.imag],
         }
         print(json.dumps(out))
     if world > 1:
@@ -380,8 +399,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
-    ap.add_argument("--cpu-budget", type=float, default=15.0)
-    ap.add_argument("--ref-budget", type=float, default=10.0)
+    ap.add_argument("--cpu-budget", type=float, default=12.0)
+    ap.add_argument("--ref-budget", type=float, default=8.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":

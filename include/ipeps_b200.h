@@ -57,6 +57,7 @@ typedef struct {
   double move_seconds;  /* host wall time inside moves (synchronous) */
   uint64_t projector_calls; /* truncated-SVD projectors computed */
   uint64_t jacobi_sweeps;   /* one-sided Jacobi sweeps summed over those projectors */
+  uint64_t extra_passes;    /* extra power iterations triggered by the residual check */
 } ipeps_stats_t;
 
 /* ---- context (no reference counterpart: the reference is one CPU process) */
@@ -91,9 +92,18 @@ IPEPS_API int ipeps_env_create(ipeps_ctx* ctx, int D, int d, int chi, int is_com
 IPEPS_API int ipeps_env_destroy(ipeps_env* env);
 /* Params Dict keys chi/min_iter/max_iter/ad_max_iter/rg_tol (default_config.toml:9-17) */
 IPEPS_API int ipeps_env_set_params(ipeps_env* env, int chi, int min_iter, int max_iter, int ad_max_iter, double rg_tol);
-/* projector sketch: k = n+1 + max(min_over, (n+1)*num/den); power iterations cold/warm */
+/* projector sketch: k = n+1 + max(min_over, (n+1)*num/den); power iterations cold/warm;
+ * a posteriori check ||M v_i - s_i u_i|| <= resid_tol * s_1 with up to max_extra
+ * further power iterations; inter_passes CholeskyQR passes for intermediate sketches;
+ * seed_older: seed from the vectors of two calls back (period-2 cycles) */
 IPEPS_API int ipeps_env_set_svd_params(ipeps_env* env, int over_num, int over_den, int min_over, int power_iters,
-                             int power_iters_warm, int warm_start);
+                                       int power_iters_warm, int warm_start, double resid_tol, int max_extra,
+                                       int inter_passes, int seed_older);
+/* mixed form (IPEPS_PREC_MIXED contexts only): run_ctm switches to FP64 for the
+ * last polish_iters iterations, or once the change per iteration drops below
+ * polish_tol, and accepts convergence only after polish_iters FP64 iterations
+ * (0 = stay in the mixed form).  No counterpart in the reference (FP64 only). */
+IPEPS_API int ipeps_env_set_mixed(ipeps_env* env, int polish_iters, double polish_tol);
 /* A (D,D,D,D,d); Ad = NULL means conj(A) (CTMTensors(A, cfg), ctm_tensor.jl:63) */
 IPEPS_API int ipeps_env_set_A(ipeps_env* env, const double* A, const double* Ad);
 /* init_ctm1 (ctm_tensor.jl:97-130) */
@@ -123,6 +133,9 @@ IPEPS_API int ipeps_ctm_log(ipeps_env* env, double* out, int* n_iters);
 IPEPS_API int ipeps_energy(ipeps_env* env, const double* Hh, const double* Hv, int d2, double* E, double* Na);
 /* get_gs_norm (evaluation.jl:47-59) */
 IPEPS_API int ipeps_gs_norm(ipeps_env* env, double* nrm);
+/* ndm_Ad of get_tangent_basis (optim_es.jl:247-251): get_single_dm contracted
+ * with Ad, shape (D,D,D,D,d), dtype of A */
+IPEPS_API int ipeps_single_dm_Ad(ipeps_env* env, double* out);
 
 /* ---- energy + gradient: the pullback of run_gs (optim_gs.jl:133-143) as
  * used by fg! (optim_gs.jl:53-91).  Starting from the environment currently
@@ -142,6 +155,13 @@ IPEPS_API int ipeps_nested_set_B(ipeps_env* env, const double* B, double px, dou
 IPEPS_API int ipeps_es_energy(ipeps_env* env, const double* Hh, const double* Hv, int d2, double* E);
 /* get_all_norm (evaluation.jl:61-77): Nb (complex) and envB (complex, size of A) */
 IPEPS_API int ipeps_all_norm(ipeps_env* env, double* Nb, double* envB);
+/* pullback of run_es (optim_es.jl:184-188) from the nested environment held by
+ * env: runs ad_iters nested iterations, returns E = get_es_energy and
+ * gH = dE/dB (complex (D,D,D,D,d), convention dE/dRe B + i dE/dIm B).
+ * The environment is advanced by those iterations (get_all_norm afterwards
+ * gives gN = envB as in get_es_grad, optim_es.jl:189). */
+IPEPS_API int ipeps_es_energy_grad(ipeps_env* env, const double* Hh, const double* Hv, int d2, int ad_iters,
+                                   double* E, double* gB);
 
 /* ---- allocation-free FP64 GEMM (no counterpart in the reference).
  * C = alpha*op(A)*op(B) + beta*C, column-major, op in {'N','T'}; A, B, C are

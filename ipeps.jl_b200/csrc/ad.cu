@@ -248,8 +248,9 @@ int findl(const std::vector<int>& l, int x) {
 }  // namespace
 
 // ------------------------------------------------------------------ tape
-void Tape::acc(int id, const Tensor& gt) {
-  if (id < 0 || gt.empty()) return;
+void Tape::acc(int id, const Tensor& gt0) {
+  if (id < 0 || gt0.empty()) return;
+  Tensor gt = gt0;
   Tensor& G = g_[id];
   if (G.empty()) {
     G = gt;
@@ -257,6 +258,7 @@ void Tape::acc(int id, const Tensor& gt) {
   }
   IPEPS_CHECK(G.numel() == gt.numel(), "tape: gradient size mismatch");
   if (G.buf.use_count() > 1) G = clone(c_, G);
+  if (G.dt == DType::F64 && gt.dt == DType::C128) G = to_complex(c_, G);
   axpy(c_, cplx(1), gt, G);
 }
 

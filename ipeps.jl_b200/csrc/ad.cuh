@@ -68,4 +68,9 @@ void ad_projector(Tape& tp, const AV& R1, bool t1, const AV& R2, bool t2, const 
 // iteration is recomputed on a tape in the backward pass.
 double energy_grad(Env& e, const Tensor& Hh, const Tensor& Hv, int ad_iters, Tensor* gA);
 
+// Pullback of run_es (optim_es.jl:196-210) with respect to B from the nested
+// environment held by e: runs ad_iters nested iterations, returns
+// get_es_energy and gH = dE/dB (complex, convention dE/dRe + i dE/dIm).
+double es_energy_grad(Env& e, const Tensor& Hh, const Tensor& Hv, int ad_iters, Tensor* gB);
+
 }  // namespace ipeps

@@ -130,6 +130,7 @@ int ipeps_stats(ipeps_ctx* ctx, ipeps_stats_t* out) {
     out->move_seconds = ctx->move_seconds;
     out->projector_calls = ctx->c->projector_calls;
     out->jacobi_sweeps = ctx->c->jacobi_sweeps;
+    out->extra_passes = ctx->c->projector_extra_passes;
     return IPEPS_OK;
   });
 }
@@ -141,6 +142,7 @@ int ipeps_stats_reset(ipeps_ctx* ctx) {
     ctx->move_seconds = 0;
     ctx->c->projector_calls = 0;
     ctx->c->jacobi_sweeps = 0;
+    ctx->c->projector_extra_passes = 0;
     return IPEPS_OK;
   });
 }
@@ -246,11 +248,17 @@ int ipeps_env_set_params(ipeps_env* env, int chi, int min_iter, int max_iter, in
 }
 
 int ipeps_env_set_svd_params(ipeps_env* env, int over_num, int over_den, int min_over, int power_iters,
-                             int power_iters_warm, int warm_start) {
+                             int power_iters_warm, int warm_start, double resid_tol, int max_extra,
+                             int inter_passes, int seed_older) {
   if (!env) return IPEPS_EINVAL;
   return guarded(env->owner, [&] {
-    IPEPS_CHECK(over_num >= 0 && over_den > 0 && min_over >= 0 && power_iters >= 0 && power_iters_warm >= 0,
+    IPEPS_CHECK(over_num >= 0 && over_den > 0 && min_over >= 0 && power_iters >= 0 && power_iters_warm >= 0 &&
+                    resid_tol >= 0 && max_extra >= 0 && inter_passes >= 1,
                 "bad svd params");
+    env->e.prm.svd.resid_tol = resid_tol;
+    env->e.prm.svd.max_extra_passes = max_extra;
+    env->e.prm.svd.inter_passes = inter_passes;
+    env->e.prm.svd.seed_older = seed_older != 0;
     auto& s = env->e.prm.svd;
     s.oversample_num = over_num;
     s.oversample_den = over_den;
@@ -310,7 +318,7 @@ int ipeps_env_set_CT(ipeps_env* env, int k, const double* C, const int64_t* C_di
     IPEPS_CHECK(E_dims[2] == env->e.D && E_dims[3] == env->e.D, "E must be (chi_a, chi_b, D, D)");
     env->e.Cs[k - 1] = upload(c, C, env->e.dt, {C_dims[0], C_dims[1]});
     env->e.Es[k - 1] = upload(c, E, env->e.dt, {E_dims[0], E_dims[1], E_dims[2], E_dims[3]});
-    for (auto& cc : env->e.cache) cc.V = Tensor();
+    for (auto& cc : env->e.cache) cc = ipeps::ProjCache();
     return IPEPS_OK;
   });
 }
@@ -469,6 +477,44 @@ extern "C" int ipeps_energy_grad(ipeps_env* env, const double* Hh, const double*
     account(env, m0, s0);
     if (E) *E = e;
     if (dA) download(c, dA, g);
+    return IPEPS_OK;
+  });
+}
+
+extern "C" int ipeps_env_set_mixed(ipeps_env* env, int polish_iters, double polish_tol) {
+  if (!env) return IPEPS_EINVAL;
+  return guarded(env->owner, [&] {
+    IPEPS_CHECK(polish_iters >= 0 && polish_tol >= 0, "bad mixed-form parameters");
+    env->e.prm.polish_iters = polish_iters;
+    env->e.prm.polish_tol = polish_tol;
+    return IPEPS_OK;
+  });
+}
+
+extern "C" int ipeps_es_energy_grad(ipeps_env* env, const double* Hh, const double* Hv, int d2, int ad_iters,
+                                    double* E, double* gB) {
+  if (!env) return IPEPS_EINVAL;
+  return guarded(env->owner, [&] {
+    IPEPS_CHECK(ad_iters >= 1, "ad_iters must be >= 1");
+    auto& c = *env->e.ctx;
+    Tensor th = upload_H(c, Hh, d2), tv = upload_H(c, Hv, d2);
+    uint64_t m0 = env->e.moves;
+    double s0 = env->e.move_seconds;
+    Tensor g;
+    double e = ipeps::es_energy_grad(env->e, th, tv, ad_iters, &g);
+    account(env, m0, s0);
+    if (E) *E = e;
+    if (gB) download(c, gB, g);
+    return IPEPS_OK;
+  });
+}
+
+extern "C" int ipeps_single_dm_Ad(ipeps_env* env, double* out) {
+  if (!env) return IPEPS_EINVAL;
+  return guarded(env->owner, [&] {
+    IPEPS_CHECK(out, "null output");
+    Tensor t = ipeps::single_dm_Ad(env->e);
+    download(*env->e.ctx, out, t);
     return IPEPS_OK;
   });
 }

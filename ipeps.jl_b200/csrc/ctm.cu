@@ -171,7 +171,7 @@ void init_ctm1(Env& e) {
   e.Es[1] = mk({-1, -5, -3, 1, 2}, {-2, -6, -4, 1, 2}, {D2, D2, D, D});
   e.Es[2] = mk({-5, -1, 1, -3, 2}, {-6, -2, 1, -4, 2}, {D2, D2, D, D});
   e.Es[3] = mk({-1, 1, -3, -5, 2}, {-2, 1, -4, -6, 2}, {D2, D2, D, D});
-  for (int i = 0; i < 4; ++i) e.cache[i].V = Tensor();
+  for (int i = 0; i < 4; ++i) e.cache[i] = ProjCache();
 }
 
 // One directional move: *_rg (ctmrg.jl:66-120) = projector + proj_* +
@@ -340,6 +340,15 @@ static std::complex<double> scalar_of(Ctx& c, const Tensor& t) {
   return {h[0], t.dt == DType::F64 ? 0.0 : h[1]};
 }
 
+// ndm_Ad of get_tangent_basis (optim_es.jl:247-251): get_single_dm contracted with Ad
+Tensor single_dm_Ad(Env& e) {
+  Ctx& c = *e.ctx;
+  NTPolicy p{c};
+  NT n_dm = get_single_dm(p, NT(e.Cs[0]), NT(e.Cs[1]), NT(e.Cs[2]), NT(e.Cs[3]), NT(e.Es[0]), NT(e.Es[1]),
+                          NT(e.Es[2]), NT(e.Es[3]));
+  return tcon(c, n_dm.c[0], {-1, -2, -3, -4, 1, 2, 3, 4}, e.Ad, {1, 2, 3, 4, -5});
+}
+
 // evaluation.jl:47-59
 std::complex<double> gs_norm(Env& e) {
   Ctx& c = *e.ctx;
@@ -378,8 +387,26 @@ int run_ctm(Env& e, int conv_mode, const Tensor* Hh, const Tensor* Hv, double* l
   e.log.clear();
   int i = 1;
   bool done = false;
+  // Mixed form: 3xTF32 contractions while the environment is still moving, then
+  // FP64 for the last polish_iters iterations (or from the point where the
+  // change per iteration drops below polish_tol), and convergence is accepted
+  // only after that many FP64 iterations.  The CTMRG map contracts errors, so
+  // the FP32-level errors of the mixed iterations decay in the FP64 ones.
+  Ctx& c = *e.ctx;
+  const int prec0 = c.precision;
+  const bool polish = (prec0 == kPrecMixed) && e.prm.polish_iters > 0;
+  const int polish_start = polish ? std::max(1, e.prm.max_iter - e.prm.polish_iters + 1) : 1 << 30;
+  int fp64_done = 0;
+  struct Restore {
+    Ctx& c;
+    int p;
+    ~Restore() { c.precision = p; }
+  } restore{c, prec0};
   for (; i <= e.prm.max_iter; ++i) {
+    if (polish && c.precision != kPrecFP64 && (i >= polish_start || diffs.back() < e.prm.polish_tol))
+      c.precision = kPrecFP64;
     std::vector<double> s = rg_step(e);
+    if (polish && c.precision == kPrecFP64) fp64_done++;
     CtmLogEntry le{i, 0, 0, 0, int(s.size())};
     if (conv_mode == 0 || conv_mode == 2) {
       std::complex<double> old = conv;
@@ -405,7 +432,7 @@ int run_ctm(Env& e, int conv_mode, const Tensor* Hh, const Tensor* Hv, double* l
     }
     le.diff = diffs.back();
     e.log.push_back(le);
-    if (i >= e.prm.min_iter && diffs.back() < e.prm.rg_tol) {
+    if (i >= e.prm.min_iter && diffs.back() < e.prm.rg_tol && (!polish || fp64_done >= e.prm.polish_iters)) {
       done = true;
       break;
     }

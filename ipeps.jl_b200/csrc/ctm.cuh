@@ -31,6 +31,9 @@ struct CtmParams {
   int max_iter = 20;
   int ad_max_iter = 4;
   double rg_tol = 1e-6;
+  // mixed form: FP64 for the last polish_iters iterations (0 = stay mixed)
+  int polish_iters = 4;
+  double polish_tol = 1e-6;
   SvdParams svd;
 };
 
@@ -85,6 +88,8 @@ double es_energy(Env& e, const Tensor& Hh, const Tensor& Hv);
 std::complex<double> all_norm(Env& e, Tensor* envB);
 // get_gs_norm (evaluation.jl:47-59)
 std::complex<double> gs_norm(Env& e);
+// get_single_dm contracted with Ad (optim_es.jl:247-251), shape of A
+Tensor single_dm_Ad(Env& e);
 // run_ctm (ctmrg.jl:1-55). conv_mode 0: energy (gs), 1: spectrum, 2: es energy / all_norm.
 // Returns iterations done; *last_diff = diffs[end]; *converged.
 int run_ctm(Env& e, int conv_mode, const Tensor* Hh, const Tensor* Hv, double* last_diff, bool* converged);

@@ -115,8 +115,8 @@ Sketch sketch_pass(Ctx& c, const MatRef& R1, const MatRef& R2, const Tensor& Om,
   Sketch s;
   Tensor Y = apply(c, R1, 'N', apply(c, R2, 'N', Om));
   for (int it = 0; it < q; ++it) {
-    Tensor Q = orth(c, Y, 2, nullptr);
-    Tensor Z = orth(c, apply(c, R2, 'T', apply(c, R1, 'T', Q)), 2, nullptr);
+    Tensor Q = orth(c, Y, sp.inter_passes, nullptr);
+    Tensor Z = orth(c, apply(c, R2, 'T', apply(c, R1, 'T', Q)), sp.inter_passes, nullptr);
     Y = apply(c, R1, 'N', apply(c, R2, 'N', Z));
   }
   s.Q = orth(c, Y, 3, nullptr);
@@ -154,9 +154,10 @@ ProjResult get_projector(Ctx& c, const MatRef& R1, const MatRef& R2, int chi, co
   Tensor Om = c.alloc(DType::F64, {N, k});
   randn(c, Om);
   bool warm = false;
-  if (sp.warm_start && cache && !cache->V.empty() && cache->V.dims[0] == N) {
-    int nv = int(std::min<int64_t>(cache->V.dims[1], k));
-    IPEPS_CUDA(cudaMemcpyAsync(Om.data(), cache->V.data(), size_t(N) * nv * 8, cudaMemcpyDeviceToDevice, c.stream));
+  if (sp.warm_start && cache && !cache->seed(sp.seed_older).empty() && cache->seed(sp.seed_older).dims[0] == N) {
+    const Tensor& Vs = cache->seed(sp.seed_older);
+    int nv = int(std::min<int64_t>(Vs.dims[1], k));
+    IPEPS_CUDA(cudaMemcpyAsync(Om.data(), Vs.data(), size_t(N) * nv * 8, cudaMemcpyDeviceToDevice, c.stream));
     warm = true;
   }
   int q = (k == N) ? 0 : (warm ? sp.power_iters_warm : sp.power_iters);
@@ -169,6 +170,7 @@ ProjResult get_projector(Ctx& c, const MatRef& R1, const MatRef& R2, int chi, co
   Tensor Ux, Vk;
   int* d_perm = nullptr;
   double* d_res = reinterpret_cast<double*>(c.scal->p) + 48;
+  double prev_res = 1e300;
   for (int attempt = 0;; ++attempt) {
     sk = sketch_pass(c, R1, R2, Om, q, sp);
     d_perm = static_cast<int*>(sk.perm.data());
@@ -211,7 +213,10 @@ ProjResult get_projector(Ctx& c, const MatRef& R1, const MatRef& R2, int chi, co
     double res = 0;
     IPEPS_CUDA(cudaMemcpyAsync(&res, d_res, 8, cudaMemcpyDeviceToHost, c.stream));
     c.sync();
-    if (res <= sp.resid_tol * smax) break;
+    // done when below tolerance, or when it stopped decreasing (the FP64 floor of
+    // R1 (R2 v), ~eps ||R1|| ||R2||, can sit above resid_tol * s_1)
+    if (res <= sp.resid_tol * smax || res > 0.5 * prev_res) break;
+    prev_res = res;
     // not converged: one more power iteration from the current right vectors
     Om = Vk;
     q = 1;
@@ -235,6 +240,7 @@ ProjResult get_projector(Ctx& c, const MatRef& R1, const MatRef& R2, int chi, co
     // (near-null directions of this M say nothing about the next one)
     Tensor Vc = c.alloc(DType::F64, {N, rr});
     IPEPS_CUDA(cudaMemcpyAsync(Vc.data(), Vk.data(), size_t(N) * rr * 8, cudaMemcpyDeviceToDevice, c.stream));
+    cache->Vold = cache->V;
     cache->V = Vc;
   }
   if (keep_factors) {

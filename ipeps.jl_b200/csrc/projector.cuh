@@ -15,11 +15,13 @@ struct MatRef {
 
 struct SvdParams {
   int oversample_num = 1;   // k = want + max(min_oversample, want*num/den)
-  int oversample_den = 2;
+  int oversample_den = 1;
   int min_oversample = 16;
   int power_iters = 3;      // cold start
   int power_iters_warm = 1; // when the previous V of this direction seeds the sketch
   int max_extra_passes = 6; // extra power iterations while the residual check fails
+  int inter_passes = 1;     // CholeskyQR passes for the intermediate power-iteration sketches
+  bool seed_older = true;   // seed from the call before the previous one (period-2 cycles)
   double resid_tol = 1e-13; // ||M v_i - s_i u_i|| <= resid_tol * s_1 for the kept triplets
   bool warm_start = true;
   int jacobi_max_sweeps = 40;
@@ -27,8 +29,14 @@ struct SvdParams {
 };
 
 // Cache of the last right singular vectors of one direction (warm start).
+// Resolved right vectors of the last two calls of one direction (warm start).
+// The sketch is seeded from the older one: a CTMRG run that has settled into
+// a period-2 cycle returns to the same environment every second iteration,
+// and for a converging run both are equally close to the fixed point.
 struct ProjCache {
-  Tensor V;  // N x n
+  Tensor V;      // previous call
+  Tensor Vold;   // the call before
+  const Tensor& seed(bool older) const { return (older && !Vold.empty()) ? Vold : V; }
 };
 
 struct ProjResult {

@@ -1,0 +1,173 @@
+"""Host drivers above the engine: optim_gs, prepare_basis, optim_es, evaluate_es.
+
+These stay on the host in the reference too (Julia + Optim.jl + LAPACK on
+small matrices); only their calls into CTMRG go to the device.
+
+    optim_gs(H, A0, cfg)        src/optimize/optim_gs.jl:14-118 (L-BFGS on the sphere)
+    prepare_basis(H, A, cfg)    src/optimize/optim_es.jl:34-73
+    optim_es(px, py, prep, cfg) src/optimize/optim_es.jl:91-165
+    evaluate_es(effH, effN)     src/graph/expectation.jl:152-183
+
+The L-BFGS is a plain two-loop recursion with the sphere manifold of
+Optim.jl (gradient projected onto the tangent space, iterate retracted by
+normalisation) and a backtracking Armijo line search; the reference uses
+Optim's HagerZhang line search, so trajectories differ and only final energies
+are compared.
+"""
+from __future__ import annotations
+
+import math
+from typing import Any, Callable, Dict, List, Optional
+
+import numpy as np
+
+from . import host
+
+
+def _sphere_project(x, g):
+    return g - np.vdot(x, g).real * x
+
+
+def optim_gs(H, A0, cfg: Dict[str, Any], m: int = 10, g_tol: float = 1e-6, f_tol: float = 1e-7,
+             iterations: int = 200, engine: Optional[host.Engine] = None,
+             callback: Optional[Callable[[int, float, float], None]] = None):
+    """L-BFGS over A on the unit sphere with the device E+grad unit (fg!).
+
+    Returns dict(A, energies, gradnorms, evals)."""
+    x = np.asarray(A0, dtype=np.float64).ravel(order="F")
+    shape = np.asarray(A0).shape
+    x = x / np.linalg.norm(x)
+    evals = 0
+
+    def fg(xv):
+        nonlocal evals
+        evals += 1
+        A = xv.reshape(shape, order="F")
+        # fg! renormalises x by max|x| before the energy (optim_gs.jl:55); the
+        # energy is scale invariant, the gradient scales by max|x|
+        s = np.abs(A).max()
+        E, g, _ = host.fg(A, H, cfg, engine=engine)
+        return E, g.ravel(order="F") / s
+
+    f, g = fg(x)
+    gp = _sphere_project(x, g)
+    energies, gradnorms = [f], [float(np.linalg.norm(gp))]
+    S: List[np.ndarray] = []
+    Y: List[np.ndarray] = []
+    for it in range(iterations):
+        if np.linalg.norm(gp) < g_tol:
+            break
+        # two-loop recursion on the tangent space
+        q = gp.copy()
+        alphas = []
+        for s_, y_ in reversed(list(zip(S, Y))):
+            rho = 1.0 / np.dot(y_, s_)
+            a = rho * np.dot(s_, q)
+            alphas.append((a, rho, s_, y_))
+            q -= a * y_
+        if S:
+            q *= np.dot(S[-1], Y[-1]) / np.dot(Y[-1], Y[-1])
+        else:
+            q *= 0.1 / max(np.linalg.norm(q), 1e-300)
+        for a, rho, s_, y_ in reversed(alphas):
+            b = rho * np.dot(y_, q)
+            q += (a - b) * s_
+        d = -_sphere_project(x, q)
+        if np.dot(d, gp) >= 0:
+            d = -gp
+        # backtracking Armijo on the retraction x -> (x + t d)/|x + t d|
+        t = 1.0
+        slope = np.dot(d, gp)
+        while True:
+            xn = x + t * d
+            xn /= np.linalg.norm(xn)
+            fn, gn = fg(xn)
+            if fn <= f + 1e-4 * t * slope or t < 1e-8:
+                break
+            t *= 0.5
+        gpn = _sphere_project(xn, gn)
+        s_vec = xn - x
+        y_vec = gpn - gp
+        if np.dot(s_vec, y_vec) > 1e-16:
+            S.append(s_vec)
+            Y.append(y_vec)
+            if len(S) > m:
+                S.pop(0)
+                Y.pop(0)
+        df = abs(fn - f)
+        x, f, gp = xn, fn, gpn
+        energies.append(f)
+        gradnorms.append(float(np.linalg.norm(gp)))
+        if callback:
+            callback(it + 1, f, gradnorms[-1])
+        if df < f_tol * max(abs(f), 1.0):
+            break
+    return {"A": x.reshape(shape, order="F"), "energies": energies, "gradnorms": gradnorms, "evals": evals}
+
+
+def normalize_gs(ts: host.CTMTensors):
+    """optim_es.jl:212-222: A <- A / sqrt|<A|A>|, environment kept."""
+    nrm = host.get_gs_norm(ts)
+    A1 = ts.A / math.sqrt(abs(nrm))
+    ts.set_A(A1)
+    return ts
+
+
+def substract_gs_energy(ts: host.CTMTensors, H):
+    """optim_es.jl:224-234: H_i - (E0/2) I."""
+    E0, _ = host.get_gs_energy(ts, H)
+    e = (E0 / 2).real
+    return [np.asarray(h, dtype=np.complex128) - e * np.eye(h.shape[0]) for h in H]
+
+
+def tangent_basis(ts: host.CTMTensors, n_dm_Ad: np.ndarray):
+    """get_tangent_basis (optim_es.jl:236-258, "default"): null space of the
+    row vector vec(ndm_Ad) (D^4 d - 1 vectors), from its full SVD."""
+    row = n_dm_Ad.reshape(1, -1, order="F").astype(np.complex128)
+    _, _, vh = np.linalg.svd(row, full_matrices=True)
+    return vh.conj().T[:, 1:]
+
+
+def evaluate_es(effH: np.ndarray, effN: np.ndarray, nrmB_cut: float = 1e-3):
+    """evaluate_es (expectation.jl:152-183): symmetrise, keep the directions of
+    N above nrmB_cut (ratio to the largest eigenvalue, or a count when an int),
+    solve H x = E N x.  Returns the sorted real eigenvalues."""
+    H2 = (effH + effH.conj().T) / 2
+    N2 = (effN + effN.conj().T) / 2
+    ev, P = np.linalg.eigh(N2)
+    idx = np.argsort(ev)[::-1]
+    ev, P = ev[idx], P[:, idx]
+    if isinstance(nrmB_cut, int):
+        keep = slice(0, nrmB_cut)
+    else:
+        keep = ev / ev[0] > nrmB_cut
+    P = P[:, keep]
+    Hp = P.conj().T @ H2 @ P
+    Np = P.conj().T @ N2 @ P
+    w = np.linalg.eigvals(np.linalg.solve(Np, Hp))
+    return np.sort(w.real)
+
+
+def optim_es(px: float, py: float, ts: host.CTMTensors, H, basis: np.ndarray,
+             indices: Optional[List[int]] = None):
+    """optim_es (optim_es.jl:91-165) for one momentum (px, py in units of pi).
+
+    ts: normalised ground-state environment (copied per basis vector from its
+    C/T), H: Hamiltonian with E0/2 subtracted, basis: (D^4 d, nb) complex.
+    indices: which basis columns to compute (all by default; a rank of a
+    multi-GPU job takes its share).  Returns (effH, effN) columns for those
+    indices (others zero)."""
+    nb = basis.shape[1]
+    effH = np.zeros((nb, nb), dtype=np.complex128)
+    effN = np.zeros((nb, nb), dtype=np.complex128)
+    C = [ts.get_CT(k) for k in range(1, 5)]
+    for i in (range(nb) if indices is None else indices):
+        t = host.CTMTensors(ts.A, dict(ts.Params), engine=ts.engine, init=False)
+        for k in range(4):
+            t.set_CT(k + 1, *C[k])
+        t.Params["px"], t.Params["py"] = px * math.pi, py * math.pi
+        gH, gN = host.get_es_grad(t, H, basis[:, i])
+        effH[:, i] = basis.conj().T @ gH / 2
+        effN[:, i] = basis.conj().T @ gN
+        t.close()
+    return effH, effN

@@ -40,7 +40,8 @@ EXPORTED = [
     "ipeps_env_get_CT", "ipeps_env_set_CT", "ipeps_ctm_move", "ipeps_ctm_step", "ipeps_ctm_run",
     "ipeps_ctm_log", "ipeps_energy", "ipeps_gs_norm", "ipeps_nested_set_B", "ipeps_es_energy",
     "ipeps_all_norm", "ipeps_tcon", "ipeps_projector", "ipeps_ctx_stream", "ipeps_prof_enable",
-    "ipeps_prof_query", "ipeps_energy_grad",
+    "ipeps_prof_query", "ipeps_energy_grad", "ipeps_env_set_mixed", "ipeps_es_energy_grad",
+    "ipeps_single_dm_Ad",
 ]
 
 
@@ -53,7 +54,7 @@ class IPEPSError(RuntimeError):
 class Stats(ct.Structure):
     _fields_ = [("launches", ct.c_uint64 * 8), ("flops", ct.c_double * 8), ("bytes", ct.c_double * 8),
                 ("moves", ct.c_uint64), ("move_seconds", ct.c_double), ("projector_calls", ct.c_uint64),
-                ("jacobi_sweeps", ct.c_uint64)]
+                ("jacobi_sweeps", ct.c_uint64), ("extra_passes", ct.c_uint64)]
 
     FAMILIES = ["permute", "gemm_f64", "gemm_tf32x3", "reduce", "elementwise", "small_linalg", "jacobi"]
 
@@ -61,7 +62,8 @@ class Stats(ct.Structure):
         fam = {n: {"launches": int(self.launches[i]), "flops": float(self.flops[i]), "bytes": float(self.bytes[i])}
                for i, n in enumerate(self.FAMILIES)}
         return {"families": fam, "moves": int(self.moves), "move_seconds": float(self.move_seconds),
-                "projector_calls": int(self.projector_calls), "jacobi_sweeps": int(self.jacobi_sweeps)}
+                "projector_calls": int(self.projector_calls), "jacobi_sweeps": int(self.jacobi_sweeps),
+                "extra_passes": int(self.extra_passes)}
 
 
 _lib = None
@@ -90,7 +92,7 @@ def load_library(path: str = LIB_PATH) -> ct.CDLL:
         "ipeps_env_create": [P, I, I, I, I, ct.POINTER(P)],
         "ipeps_env_destroy": [P],
         "ipeps_env_set_params": [P, I, I, I, I, D],
-        "ipeps_env_set_svd_params": [P, I, I, I, I, I, I],
+        "ipeps_env_set_svd_params": [P, I, I, I, I, I, I, D, I, I, I],
         "ipeps_env_set_A": [P, dp, dp],
         "ipeps_env_init": [P],
         "ipeps_env_get_CT": [P, I, dp, lp, dp, lp],
@@ -110,6 +112,9 @@ def load_library(path: str = LIB_PATH) -> ct.CDLL:
         "ipeps_prof_enable": [P, I],
         "ipeps_prof_query": [P, dp, ct.POINTER(ct.c_uint64), dp, dp],
         "ipeps_energy_grad": [P, dp, dp, I, I, dp, dp],
+        "ipeps_env_set_mixed": [P, I, D],
+        "ipeps_es_energy_grad": [P, dp, dp, I, I, dp, dp],
+        "ipeps_single_dm_Ad": [P, dp],
     }
     for name, args in sig.items():
         f = getattr(lib, name)
@@ -265,11 +270,15 @@ class CTMTensors:
         self.engine.check(self.lib.ipeps_env_set_params(
             self.h, int(p.get("chi", 30)), int(p.get("min_iter", 4)), int(p.get("max_iter", 20)),
             int(p.get("ad_max_iter", 4)), float(p.get("rg_tol", 1e-6))))
-        over = p.get("svd_oversample", (1, 2, 16))
+        over = p.get("svd_oversample", (1, 1, 16))
         pit = p.get("svd_power_iters", (3, 1))
         self.engine.check(self.lib.ipeps_env_set_svd_params(
             self.h, int(over[0]), int(over[1]), int(over[2]), int(pit[0]), int(pit[1]),
-            int(bool(p.get("svd_warm_start", True)))))
+            int(bool(p.get("svd_warm_start", True))), float(p.get("svd_resid_tol", 1e-13)),
+            int(p.get("svd_max_extra", 6)), int(p.get("svd_inter_passes", 1)),
+            int(bool(p.get("svd_seed_older", True)))))
+        self.engine.check(self.lib.ipeps_env_set_mixed(
+            self.h, int(p.get("mixed_polish_iters", 4)), float(p.get("mixed_polish_tol", 1e-6))))
 
     def get_CT(self, k: int):
         """(C_k, E_k) as column-major numpy arrays, k = 1..4."""
@@ -446,6 +455,13 @@ def get_gs_norm(ts: CTMTensors):
     return complex(out[0], out[1])
 
 
+def single_dm_Ad(ts: CTMTensors) -> np.ndarray:
+    """ndm_Ad of get_tangent_basis (optim_es.jl:247-251)."""
+    out = np.empty(ts.A.shape, dtype=ts.dtype, order="F")
+    ts.engine.check(ts.lib.ipeps_single_dm_Ad(ts.h, _dp(out)))
+    return out
+
+
 def get_es_energy(ts: CTMTensors, H) -> float:
     """evaluation.jl:31-45"""
     Hh, Hv, d2 = _H_pair(H)
@@ -486,6 +502,33 @@ def fg(x, H, cfg, engine: Optional[Engine] = None):
     E, g = energy_grad(ts, H)
     ts.close()
     return E, g, info
+
+
+def es_energy_grad(ts: CTMTensors, H, ad_iters: Optional[int] = None):
+    """Pullback of run_es (optim_es.jl:196-210) w.r.t. B from the nested
+    environment held by ts: returns (E, gH) with gH complex (D,D,D,D,d)."""
+    Hh, Hv, d2 = _H_pair(H)
+    n = int(ts.Params.get("ad_max_iter", 4) if ad_iters is None else ad_iters)
+    ts._push_params()
+    E = np.zeros(1)
+    g = np.empty(ts.A.shape, dtype=np.complex128, order="F")
+    ts.engine.check(ts.lib.ipeps_es_energy_grad(ts.h, _dp(Hh), _dp(Hv), d2, n, _dp(E), _dp(g)))
+    return float(E[0]), g
+
+
+def get_es_grad(ts: CTMTensors, H, Bi):
+    """get_es_grad (optim_es.jl:167-194) on the device.
+
+    ts holds the (normalised) ground-state environment; it is modified in
+    place (B set, nested iterations run).  Returns (gH, gN) as flat complex
+    vectors in column-major order, gN = envB of get_all_norm after the
+    pullback iterations (optim_es.jl:189)."""
+    B = np.asarray(Bi, dtype=np.complex128).reshape(ts.A.shape, order="F")
+    ts.set_B(B, ts.Params.get("px", 0.0), ts.Params.get("py", 0.0))
+    run_ctm(ts, conv_fun="es", H=H)
+    E, gH = es_energy_grad(ts, H)
+    Nb, gN = get_all_norm(ts)
+    return gH.reshape(-1, order="F"), gN.reshape(-1, order="F")
 
 
 def compute_gs_energy(A, H, cfg, engine: Optional[Engine] = None):

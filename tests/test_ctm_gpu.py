@@ -153,3 +153,22 @@ def test_nested_energy_and_norm(engine, pkg):
     assert abs(E - Eo) <= 1e-9 * max(1.0, abs(Eo))
     assert abs(Nb - complex(Nbo.item())) <= 1e-9 * max(1.0, abs(complex(Nbo.item())))
     assert np.allclose(envB, npa(envBo), rtol=1e-8, atol=1e-10 * np.abs(npa(envBo)).max())
+
+
+def test_bench_workload_trajectory(engine, pkg):
+    """The bench workload (Heisenberg D=4 chi=64, 30 iterations): every
+    per-iteration energy against the oracle's, |dE| <= 1e-10."""
+    with open(os.path.join(GOLD, "bench_workload.json")) as f:
+        g = json.load(f)
+    rng = np.random.default_rng(g["seed"])
+    D, d, chi = g["D"], g["d"], g["chi"]
+    A = rng.standard_normal(D ** 4 * d).reshape((D, D, D, D, d), order="F")
+    A = np.asfortranarray(A / np.abs(A).max())
+    H = [npa(h) for h in O.heisenberg(1.0)]
+    cfg = pkg.default_config()
+    cfg.update(chi=chi, min_iter=30, max_iter=30, rg_tol=0.0)
+    ts = pkg.CTMTensors(A, cfg, engine=engine)
+    ts, info = pkg.run_ctm(ts, conv_fun="energy", H=H)
+    got = [l["obj"].real for l in info["log"]]
+    err = max(abs(a - b) for a, b in zip(got, g["energies"]))
+    assert err <= 1e-10, err

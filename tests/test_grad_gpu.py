@@ -57,3 +57,32 @@ def test_energy_grad_finite_difference(engine, pkg):
         # the reference adjoint broadens 1/(s_i^2 - s_j^2) (eta = 1e-12), so it is
         # not the exact derivative; agreement is at the 1e-4 level
         assert abs(fd - an) <= 1e-3 * abs(an) + 1e-7, (fd, an)
+
+
+def test_es_grad_matches_oracle(engine, pkg):
+    """Nested pullback w.r.t. B (get_es_grad, optim_es.jl:167-194): gH and gN
+    against the oracle on a small ground-state environment (D=2, chi=8).
+    Bars: gH and gN 1e-6 relative (2-norm)."""
+    D, chi = 2, 8
+    A = O.random_A(D, 2, seed=4)
+    H = O.heisenberg(1.0)
+    cfg = O.default_config()
+    cfg.update(chi=chi, min_iter=4, max_iter=30, rg_tol=1e-10, ad_max_iter=4)
+    ts_o = O.make_ctm_tensors(A, cfg)
+    with torch.no_grad():
+        ts_o, _ = O.run_ctm(ts_o, conv_fun=lambda t: O.get_gs_energy(t, H)[0])
+    ts_o = O._detach_ts(ts_o)
+    g = np.random.default_rng(11)
+    Bi = g.standard_normal(A.numel()) + 1j * g.standard_normal(A.numel())
+    px, py = 0.5 * np.pi, 0.25 * np.pi
+    ts_o.Params.update(px=px, py=py, max_iter=12, rg_tol=1e-8)
+    gH_o, gN_o = O.get_es_grad(ts_o, H, torch.tensor(Bi))
+
+    Hn = [h.numpy() for h in H]
+    ts = pkg.CTMTensors(A.numpy(), cfg, engine=engine)
+    pkg.run_ctm(ts, conv_fun="energy", H=Hn)
+    ts.Params.update(px=px, py=py, max_iter=12, rg_tol=1e-8)
+    gH, gN = pkg.get_es_grad(ts, Hn, Bi)
+    gH_o, gN_o = gH_o.numpy(), gN_o.numpy()
+    assert np.linalg.norm(gH - gH_o) <= 1e-6 * np.linalg.norm(gH_o), np.linalg.norm(gH - gH_o) / np.linalg.norm(gH_o)
+    assert np.linalg.norm(gN - gN_o) <= 1e-6 * np.linalg.norm(gN_o)
