@@ -16,7 +16,8 @@ L2 flushed (512 MB write) between steps, max over ranks; value = E+grad
 evaluations/s of the whole job.  e2e = the same metric through the public API
 (fg) with host buffers: A and H copied in, energy and gradient copied out,
 inside the timed region.  Under torchrun each rank runs an independent
-replica (CTMRG does not shard).
+replica: a CTMRG run of one iPEPS is a sequential chain of dependent moves
+with no data-parallel split, so N GPUs run N independent evaluations.
 
 Reference arm: the reference is Julia, which is not installed, so
 ``--impl reference`` times the CPU FP64 oracle (a restatement of the

@@ -296,354 +296,3 @@ void scale_rows(Ctx& c, double* X, int64_t ldx, int64_t m, int64_t ncols, const 
 }
 
 }  // namespace ipeps
-
-// ---------------------------------------------------------------------------
-// Shared-memory kernels for the projector's k x k problems.
-// ---------------------------------------------------------------------------
-namespace ipeps {
-namespace {
-
-__device__ __forceinline__ int pidx(int i, int j) { return j * (j + 1) / 2 + i; }  // packed upper, i <= j
-
-__device__ __forceinline__ double warp_sum2(double v) {
-  for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
-}
-
-// Fused guarded Cholesky + in-place triangular inverse on the packed upper
-// triangle held in shared memory.  On exit G holds R (G = R^T R after the
-// optional shift, strict lower triangle zeroed) and Rinv = R^-1.
-// shift_factor > 0 adds shift_factor * trace(G) to the diagonal first.
-__global__ void __launch_bounds__(1024) cholinv_packed_kernel(double* G, int k, int64_t ldg, double shift_factor,
-                                                              double* Rinv, int64_t ldr) {
-  extern __shared__ double P[];
-  double* tmp = P + k * (k + 1) / 2;
-  double* rowj = tmp + k;
-  __shared__ double s_red[32];
-  __shared__ double s_tr;
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
-  for (int j = warp; j < k; j += nw)
-    for (int i = lane; i <= j; i += 32) P[pidx(i, j)] = G[i + int64_t(j) * ldg];
-  __syncthreads();
-  // trace (for the shift and the pivot guard)
-  double t = 0;
-  for (int i = tid; i < k; i += blockDim.x) t += fabs(P[pidx(i, i)]);
-  t = warp_sum2(t);
-  if (lane == 0) s_red[warp] = t;
-  __syncthreads();
-  if (tid == 0) {
-    double s = 0;
-    for (int w = 0; w < nw; ++w) s += s_red[w];
-    s_tr = s;
-  }
-  __syncthreads();
-  const double shift = shift_factor > 0 ? shift_factor * s_tr : 0.0;
-  if (shift > 0)
-    for (int i = tid; i < k; i += blockDim.x) P[pidx(i, i)] += shift;
-  const double tiny = 1e-300 + 1e-32 * (s_tr + shift * k);
-  __syncthreads();
-  // right-looking Cholesky, one column of R per step
-  for (int j = 0; j < k; ++j) {
-    const double d = P[pidx(j, j)];
-    const double piv = d > tiny ? sqrt(d) : 0.0;
-    const double ipiv = piv > 0 ? 1.0 / piv : 0.0;
-    __syncthreads();
-    // row j of R, also staged in rowj so that the update below reads a
-    // separate array (its loads can then be issued ahead of the stores)
-    for (int l = j + 1 + tid; l < k; l += blockDim.x) {
-      const double v = P[pidx(j, l)] * ipiv;
-      P[pidx(j, l)] = v;
-      rowj[l] = v;
-    }
-    if (tid == 0) P[pidx(j, j)] = piv > 0 ? piv : 1.0;
-    __syncthreads();
-    // one thread per trailing column l: P[i,l] -= R[j,i] R[j,l] for j < i <= l
-    // (rowj[i] is read by every thread at once: a shared-memory broadcast)
-    for (int l = j + 1 + tid; l < k; l += blockDim.x) {
-      const double rjl = rowj[l];
-      double* col = P + l * (l + 1) / 2;
-      int i = j + 1;
-      for (; i + 3 <= l; i += 4) {
-        const double r0 = rowj[i], r1 = rowj[i + 1], r2 = rowj[i + 2], r3 = rowj[i + 3];
-        const double c0 = col[i], c1 = col[i + 1], c2 = col[i + 2], c3 = col[i + 3];
-        col[i] = fma(-r0, rjl, c0);
-        col[i + 1] = fma(-r1, rjl, c1);
-        col[i + 2] = fma(-r2, rjl, c2);
-        col[i + 3] = fma(-r3, rjl, c3);
-      }
-      for (; i <= l; ++i) col[i] = fma(-rowj[i], rjl, col[i]);
-    }
-    __syncthreads();
-  }
-  for (int j = warp; j < k; j += nw)
-    for (int i = lane; i < k; i += 32) G[i + int64_t(j) * ldg] = (i <= j) ? P[pidx(i, j)] : 0.0;
-  // in-place inverse of the upper-triangular R, column by column:
-  // X[0:j, j] = -X[0:j, 0:j] * R[0:j, j] / R[j, j], X[j, j] = 1 / R[j, j]
-  for (int j = 0; j < k; ++j) {
-    for (int i = tid; i < j; i += blockDim.x) tmp[i] = P[pidx(i, j)];
-    __syncthreads();
-    const double inv = 1.0 / P[pidx(j, j)];
-    // one thread per row i < j: X[i,j] = -inv * sum_{l=i}^{j-1} X[i,l] R[l,j]
-    for (int i = tid; i < j; i += blockDim.x) {
-      double s = 0;
-      for (int l = i; l < j; ++l) s = fma(P[pidx(i, l)], tmp[l], s);
-      P[pidx(i, j)] = -inv * s;
-    }
-    __syncthreads();
-    if (tid == 0) P[pidx(j, j)] = inv;
-  }
-  __syncthreads();
-  for (int j = warp; j < k; j += nw)
-    for (int i = lane; i < k; i += 32) Rinv[i + int64_t(j) * ldr] = (i <= j) ? P[pidx(i, j)] : 0.0;
-}
-
-__device__ __forceinline__ double hsum16(double v) {
-  for (int o = 8; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
-}
-
-// One-sided Jacobi, X (m x k) in shared memory, J in shared memory when it
-// fits.  One half-warp per column pair (up to 64 pairs rotate at once), and
-// the squared column norms are carried in shared memory: after a rotation
-// that zeroes c = x_p.x_q they are a - t c and b + t c exactly in exact
-// arithmetic, and they are recomputed from X at the start of every sweep, so
-// each pair costs one dot product instead of three.
-template <bool J_SMEM>
-__global__ void __launch_bounds__(1024) jacobi_hw_kernel(double* Xg, int m, int k, int64_t ldx, double* Jg,
-                                                         int64_t ldjg, double* S, int max_sweeps, double tol,
-                                                         int* status, int* sweeps_out) {
-  extern __shared__ double X[];
-  double* nrm = X + int64_t(m) * k;  // k squared norms
-  double* J = J_SMEM ? nrm + k : Jg;
-  const int64_t ldj = J_SMEM ? k : ldjg;
-  __shared__ int s_rot;
-  const int tid = threadIdx.x, grp = tid >> 4, l16 = tid & 15, ngrp = blockDim.x >> 4;
-  const int warp = tid >> 5, lane = tid & 31, nwarps = blockDim.x >> 5;
-  for (int j = warp; j < k; j += nwarps)
-    for (int i = lane; i < m; i += 32) X[i + j * m] = Xg[i + int64_t(j) * ldx];
-  for (int64_t t = tid; t < int64_t(k) * k; t += blockDim.x) {
-    const int i = int(t % k), j = int(t / k);
-    J[i + j * ldj] = (i == j) ? 1.0 : 0.0;
-  }
-  __syncthreads();
-  const int kk = (k + 1) & ~1;
-  const double tol2 = tol * tol;
-  int sweep = 0;
-  bool converged = (k < 2);
-  for (; sweep < max_sweeps && !converged; ++sweep) {
-    for (int j = warp; j < k; j += nwarps) {
-      double a = 0;
-      for (int i = lane; i < m; i += 32) a = fma(X[i + j * m], X[i + j * m], a);
-      a = warp_sum2(a);
-      if (lane == 0) nrm[j] = a;
-    }
-    if (tid == 0) s_rot = 0;
-    __syncthreads();
-    for (int r = 0; r < kk - 1; ++r) {
-      // every lane runs the same trip count (the half-warp shuffles use the full mask);
-      // out-of-range pairs contribute zeros and skip the rotation
-      for (int base = 0; base < kk / 2; base += ngrp) {
-        const int pi = base + grp;
-        int p = 0, q = 0;
-        bool valid = pi < kk / 2;
-        if (valid) {
-          p = (pi == 0) ? 0 : 1 + (pi - 1 + r) % (kk - 1);
-          q = 1 + (kk - 2 - pi + r) % (kk - 1);
-          valid = p < k && q < k;
-          if (p > q) { int t = p; p = q; q = t; }
-        }
-        double cc = 0;
-        if (valid)
-          for (int i = l16; i < m; i += 16) cc = fma(X[i + p * m], X[i + q * m], cc);
-        cc = hsum16(cc);
-        if (!valid) continue;
-        const double a = nrm[p], b = nrm[q];
-        if (cc == 0.0 || a <= 0.0 || b <= 0.0 || cc * cc <= tol2 * (a * b)) continue;
-        const double zeta = (b - a) / (2.0 * cc);
-        const double t = copysign(1.0, zeta) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
-        const double cs = rsqrt(1.0 + t * t), sn = cs * t;
-        for (int i = l16; i < m; i += 16) {
-          const double xp = X[i + p * m], xq = X[i + q * m];
-          X[i + p * m] = cs * xp - sn * xq;
-          X[i + q * m] = sn * xp + cs * xq;
-        }
-        for (int i = l16; i < k; i += 16) {
-          const double jp = J[i + p * ldj], jq = J[i + q * ldj];
-          J[i + p * ldj] = cs * jp - sn * jq;
-          J[i + q * ldj] = sn * jp + cs * jq;
-        }
-        if (l16 == 0) {
-          nrm[p] = a - t * cc;
-          nrm[q] = b + t * cc;
-          s_rot = 1;
-        }
-      }
-      __syncthreads();
-    }
-    converged = (s_rot == 0);
-    __syncthreads();
-  }
-  for (int j = warp; j < k; j += nwarps) {
-    double a = 0;
-    for (int i = lane; i < m; i += 32) {
-      const double x = X[i + j * m];
-      a = fma(x, x, a);
-      Xg[i + int64_t(j) * ldx] = x;
-    }
-    a = warp_sum2(a);
-    if (lane == 0) S[j] = sqrt(a);
-  }
-  if (J_SMEM)
-    for (int64_t t = tid; t < int64_t(k) * k; t += blockDim.x) {
-      const int i = int(t % k), j = int(t / k);
-      Jg[i + j * ldjg] = J[i + j * ldj];
-    }
-  if (tid == 0) {
-    if (!converged) atomicOr(status, 4);
-    if (sweeps_out) *sweeps_out = sweep;
-  }
-}
-
-// One-sided Jacobi with the m x k matrix X resident in shared memory (J in
-// global memory).  Same ordering and rotation as jacobi_kernel.
-template <bool J_SMEM>
-__global__ void __launch_bounds__(1024) jacobi_smem_kernel(double* Xg, int m, int k, int64_t ldx, double* Jg,
-                                                           int64_t ldjg, double* S, int max_sweeps, double tol,
-                                                           int* status, int* sweeps_out) {
-  extern __shared__ double X[];
-  __shared__ double s_off;
-  // J lives after X in shared memory when it fits, else in global memory
-  double* J = J_SMEM ? X + int64_t(m) * k : Jg;
-  const int64_t ldj = J_SMEM ? k : ldjg;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
-  for (int j = warp; j < k; j += nwarps)
-    for (int i = lane; i < m; i += 32) X[i + j * m] = Xg[i + int64_t(j) * ldx];
-  for (int64_t t = threadIdx.x; t < int64_t(k) * k; t += blockDim.x) {
-    int i = int(t % k), j = int(t / k);
-    J[i + j * ldj] = (i == j) ? 1.0 : 0.0;
-  }
-  __syncthreads();
-  const int kk = (k + 1) & ~1;
-  int sweep = 0;
-  bool converged = (k < 2);
-  for (; sweep < max_sweeps && !converged; ++sweep) {
-    if (threadIdx.x == 0) s_off = 0.0;
-    __syncthreads();
-    for (int r = 0; r < kk - 1; ++r) {
-      for (int pi = warp; pi < kk / 2; pi += nwarps) {
-        int p = (pi == 0) ? 0 : 1 + (pi - 1 + r) % (kk - 1);
-        int q = 1 + (kk - 2 - pi + r) % (kk - 1);
-        if (p >= k || q >= k) continue;
-        if (p > q) { int t = p; p = q; q = t; }
-        double a = 0, b = 0, cc = 0;
-        for (int i = lane; i < m; i += 32) {
-          double xp = X[i + p * m], xq = X[i + q * m];
-          a = fma(xp, xp, a);
-          b = fma(xq, xq, b);
-          cc = fma(xp, xq, cc);
-        }
-        a = warp_sum2(a);
-        b = warp_sum2(b);
-        cc = warp_sum2(cc);
-        if (cc == 0.0 || a == 0.0 || b == 0.0) continue;
-        // |c| / sqrt(a b) <= tol, without a square root or a division
-        if (cc * cc <= tol * tol * (a * b)) continue;
-        if (lane == 0) s_off = 1.0;  // a rotation in this sweep: not converged yet
-        const double zeta = (b - a) / (2.0 * cc);
-        const double t = copysign(1.0, zeta) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
-        const double cs = 1.0 / sqrt(1.0 + t * t), sn = cs * t;
-        for (int i = lane; i < m; i += 32) {
-          double xp = X[i + p * m], xq = X[i + q * m];
-          X[i + p * m] = cs * xp - sn * xq;
-          X[i + q * m] = sn * xp + cs * xq;
-        }
-        for (int i = lane; i < k; i += 32) {
-          double jp = J[i + p * ldj], jq = J[i + q * ldj];
-          J[i + p * ldj] = cs * jp - sn * jq;
-          J[i + q * ldj] = sn * jp + cs * jq;
-        }
-      }
-      __syncthreads();
-    }
-    converged = (s_off <= tol);
-    __syncthreads();
-  }
-  for (int j = warp; j < k; j += nwarps) {
-    double a = 0;
-    for (int i = lane; i < m; i += 32) {
-      const double x = X[i + j * m];
-      a = fma(x, x, a);
-      Xg[i + int64_t(j) * ldx] = x;
-    }
-    a = warp_sum2(a);
-    if (lane == 0) S[j] = sqrt(a);
-  }
-  if (J_SMEM)
-    for (int64_t t = threadIdx.x; t < int64_t(k) * k; t += blockDim.x) {
-      const int i = int(t % k), j = int(t / k);
-      Jg[i + j * ldjg] = J[i + j * ldj];
-    }
-  if (threadIdx.x == 0) {
-    if (!converged) atomicOr(status, 4);
-    if (sweeps_out) *sweeps_out = sweep;
-  }
-}
-
-// opt-in limit per block is 227 KB including static shared memory; keep 1 KB for the kernels' own
-constexpr size_t kMaxDynSmem = 226 * 1024;
-bool g_cholinv_attr = false, g_jacobi_attr = false, g_jacobi2_attr = false;
-
-}  // namespace
-
-bool cholinv_fits(int k) { return (size_t(k) * (k + 1) / 2 + 2 * size_t(k)) * 8 <= kMaxDynSmem; }
-
-void chol_inv_upper(Ctx& c, double* G, int k, int64_t ldg, double shift_factor, double* Rinv, int64_t ldr) {
-  IPEPS_CHECK(cholinv_fits(k), "chol_inv_upper: k too large for shared memory");
-  if (!g_cholinv_attr) {
-    IPEPS_CUDA(cudaFuncSetAttribute(cholinv_packed_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kMaxDynSmem)));
-    g_cholinv_attr = true;
-  }
-  ProfScope ps(c, KFam::SmallLinalg);
-  const size_t smem = (size_t(k) * (k + 1) / 2 + 2 * size_t(k)) * 8;
-  // four warps: the two barriers per column dominate and are cheap for 128 threads
-  // one thread per column (Cholesky update) / row (inverse): k threads, rounded to warps, at most 256
-  const int nt = std::min(256, std::max(32, (k + 31) / 32 * 32));
-  cholinv_packed_kernel<<<1, nt, smem, c.stream>>>(G, k, ldg, shift_factor, Rinv, ldr);
-  IPEPS_LAUNCH_CHECK();
-  c.count(KFam::SmallLinalg, 2.0 * double(k) * k * k / 3.0);
-}
-
-void jacobi_svd_auto(Ctx& c, double* X, int m, int k, int64_t ldx, double* J, int64_t ldj, double* S,
-                     int max_sweeps, double tol, int* d_sweeps) {
-  // X, the k squared norms and (when it fits) J in shared memory
-  const size_t smem = (size_t(m) * k + k) * 8;
-  const size_t smem2 = smem + size_t(k) * k * 8;
-  if (tol <= 0) tol = double(m) * 2.220446049250313e-16;  // rounding level of the column dot products
-  if (smem2 <= kMaxDynSmem) {
-    if (!g_jacobi2_attr) {
-      IPEPS_CUDA(cudaFuncSetAttribute(jacobi_hw_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      int(kMaxDynSmem)));
-      g_jacobi2_attr = true;
-    }
-    ProfScope ps(c, KFam::Jacobi);
-    jacobi_hw_kernel<true><<<1, 1024, smem2, c.stream>>>(X, m, k, ldx, J, ldj, S, max_sweeps, tol, c.d_status,
-                                                         d_sweeps);
-    IPEPS_LAUNCH_CHECK();
-    c.count(KFam::Jacobi, 6.0 * double(m + k) * k * k / 2.0);
-  } else if (smem <= kMaxDynSmem) {
-    if (!g_jacobi_attr) {
-      IPEPS_CUDA(cudaFuncSetAttribute(jacobi_hw_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      int(kMaxDynSmem)));
-      g_jacobi_attr = true;
-    }
-    ProfScope ps(c, KFam::Jacobi);
-    jacobi_hw_kernel<false><<<1, 1024, smem, c.stream>>>(X, m, k, ldx, J, ldj, S, max_sweeps, tol, c.d_status,
-                                                         d_sweeps);
-    IPEPS_LAUNCH_CHECK();
-    c.count(KFam::Jacobi, 6.0 * double(m + k) * k * k / 2.0);
-  } else {
-    jacobi_svd(c, X, m, k, ldx, J, ldj, S, max_sweeps, tol, d_sweeps);
-  }
-}
-
-}  // namespace ipeps

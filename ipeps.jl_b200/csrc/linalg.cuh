@@ -16,12 +16,19 @@ void trace(Ctx& c, const double* G, int k, int64_t ldg, double* d_out);
 // J accumulated (k x k), S = column norms (unsorted).
 void jacobi_svd(Ctx& c, double* X, int m, int k, int64_t ldx, double* J, int64_t ldj, double* S,
                 int max_sweeps, double tol, int* d_sweeps);
-// Fused Cholesky + triangular inverse in shared memory (packed upper triangle):
-// G <- R (G = R^T R after adding shift_factor * trace(G) to the diagonal when
-// shift_factor > 0), Rinv <- R^-1.  Requires cholinv_fits(k).
-bool cholinv_fits(int k);
-void chol_inv_upper(Ctx& c, double* G, int k, int64_t ldg, double shift_factor, double* Rinv, int64_t ldr);
-// jacobi_svd with X held in shared memory when it fits; tol <= 0 means m * eps
+// Blocked guarded Cholesky in shared memory (packed upper triangle, 32-column
+// panels): G <- R with G = R^T R after adding shift_factor * trace(G) to the
+// diagonal when shift_factor > 0; a pivot at or below 1e-32 trace(G) gives
+// R[j][j] = 1 and a zero row.  Requires chol_fits(k).
+bool chol_fits(int k);
+void chol_blocked(Ctx& c, double* G, int k, int64_t ldg, double shift_factor);
+// Q = Y R^-1 (Y: N x k, R: k x k upper triangular), one warp per row of Y.
+// Requires trsm_fits(k).
+bool trsm_fits(int k);
+void trsm_right_upper(Ctx& c, const double* Y, int64_t ldy, int64_t N, int k, const double* R, int64_t ldr,
+                      double* Q, int64_t ldq);
+// jacobi_svd with X held in shared memory and J formed from the logged
+// rotations when it fits; tol <= 0 means m * eps
 void jacobi_svd_auto(Ctx& c, double* X, int m, int k, int64_t ldx, double* J, int64_t ldj, double* S,
                      int max_sweeps, double tol, int* d_sweeps);
 // Descending sort with permutation (ties: later index first)

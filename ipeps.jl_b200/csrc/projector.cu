@@ -56,14 +56,16 @@ Tensor orth(Ctx& c, const Tensor& Y0, int passes, Tensor* Rout) {
   Tensor Racc;
   double* d_tr = reinterpret_cast<double*>(c.scal->p) + 8;
   const double u = 1.1102230246251565e-16;
-  const bool fused = cholinv_fits(k);
+  const bool blocked = chol_fits(k) && trsm_fits(k);
   for (int pass = 0; pass < passes; ++pass) {
     // G = Y^T Y  (FP64 always: the Gram matrix is where precision is lost)
     gemm(c, DType::F64, 'T', 'N', k, k, N, cplx(1), Y.data(), N, Y.data(), N, cplx(0), G.data(), k, true);
     // shifted CholeskyQR: the first pass adds 11 (N k + k (k+1)) u trace(G) to the diagonal
     const double sf = (pass == 0) ? 11.0 * (double(N) * k + double(k) * (k + 1)) * u : 0.0;
-    if (fused) {
-      chol_inv_upper(c, G.f64(), k, k, sf, Ri.f64(), k);
+    Tensor Yn = c.alloc(DType::F64, {N, k});
+    if (blocked) {
+      chol_blocked(c, G.f64(), k, k, sf);
+      trsm_right_upper(c, Y.f64(), N, N, k, G.f64(), k, Yn.f64(), N);
     } else {
       if (pass == 0) {
         trace(c, G.f64(), k, k, d_tr);
@@ -72,9 +74,8 @@ Tensor orth(Ctx& c, const Tensor& Y0, int passes, Tensor* Rout) {
         chol_upper(c, G.f64(), k, k, nullptr, 0.0);
       }
       triinv_upper(c, G.f64(), k, k, Ri.f64(), k);
+      gemm(c, DType::F64, 'N', 'N', N, k, k, cplx(1), Y.data(), N, Ri.data(), k, cplx(0), Yn.data(), N, true);
     }
-    Tensor Yn = c.alloc(DType::F64, {N, k});
-    gemm(c, DType::F64, 'N', 'N', N, k, k, cplx(1), Y.data(), N, Ri.data(), k, cplx(0), Yn.data(), N, true);
     Y = Yn;
     if (Rout) {
       if (pass == 0) {
@@ -148,7 +149,11 @@ ProjResult get_projector(Ctx& c, const MatRef& R1, const MatRef& R2, int chi, co
   const int new_chi = int(std::min<int64_t>(chi, R1.cols()));
   const int want = int(std::min<int64_t>(N, new_chi + 1));
   int over = std::max(sp.min_oversample, want * sp.oversample_num / std::max(sp.oversample_den, 1));
-  const int k = int(std::min<int64_t>(N, int64_t(want) + over));
+  int kw = int(std::min<int64_t>(N, int64_t(want) + over));
+  // at most 128 columns when the minimum oversampling allows it: the Jacobi
+  // then rotates all of its pairs (64) in one pass of its 64 half-warps
+  if (kw > 128 && want + sp.min_oversample <= 128) kw = 128;
+  const int k = kw;
 
   // sketch Omega (N x k): resolved right vectors of the previous call first, then Gaussian columns
   Tensor Om = c.alloc(DType::F64, {N, k});
