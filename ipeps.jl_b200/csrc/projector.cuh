@@ -22,7 +22,7 @@ struct SvdParams {
   int max_extra_passes = 6; // extra power iterations while the residual check fails
   int inter_passes = 1;     // CholeskyQR passes for the intermediate power-iteration sketches
   bool seed_older = true;   // seed from the call before the previous one (period-2 cycles)
-  double resid_tol = 1e-13; // ||M v_i - s_i u_i|| <= resid_tol * s_1 for the kept triplets
+  double resid_tol = 1e-11; // ||M v_i - s_i u_i|| <= resid_tol * s_1 for the kept triplets
   bool warm_start = true;
   int jacobi_max_sweeps = 40;
   double jacobi_tol = 0.0;  // <= 0: m * eps (rounding level of the column dot products)

@@ -274,7 +274,7 @@ class CTMTensors:
         pit = p.get("svd_power_iters", (3, 1))
         self.engine.check(self.lib.ipeps_env_set_svd_params(
             self.h, int(over[0]), int(over[1]), int(over[2]), int(pit[0]), int(pit[1]),
-            int(bool(p.get("svd_warm_start", True))), float(p.get("svd_resid_tol", 1e-13)),
+            int(bool(p.get("svd_warm_start", True))), float(p.get("svd_resid_tol", 1e-11)),
             int(p.get("svd_max_extra", 6)), int(p.get("svd_inter_passes", 1)),
             int(bool(p.get("svd_seed_older", True)))))
         self.engine.check(self.lib.ipeps_env_set_mixed(

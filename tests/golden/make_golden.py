@@ -42,34 +42,36 @@ def main():
         json.dump({"generator": "tests/golden/make_golden.py (CPU oracle, torch float64)", "cases": out}, f, indent=1)
 
 
-if __name__ == "__main__":
-    main()
-
-
-def bench_workload(path=os.path.join(HERE, "bench_workload.json")):
-    """Energy trajectory of the bench workload (Heisenberg D=4 chi=64, seed 1000,
-    30 iterations from init_ctm1); ~1 min of CPU.  This workload does not
-    converge: it settles into a period-2 cycle, which makes it sensitive to
-    the accuracy of the truncated SVD near the cut."""
+def bench_workload(path=os.path.join(HERE, "bench_workload.json"), D=4, chi=64, iters=30, seed=1000):
+    """Energy trajectory of a Heisenberg workload from init_ctm1 (default: D=4
+    chi=64, seed 1000, 30 iterations; ~1 min of CPU).  The D=4 workload does
+    not converge: it settles into a period-2 cycle, which makes it sensitive
+    to the accuracy of the truncated SVD near the cut.  D=5 chi=100 with 8
+    iterations (N = 2500 enlarged corners) takes several minutes."""
     import numpy as np
     import torch
-    rng = np.random.default_rng(1000)
-    D, d, chi = 4, 2, 64
+    rng = np.random.default_rng(seed)
+    d = 2
     A = rng.standard_normal(D ** 4 * d).reshape((D, D, D, D, d), order="F")
     A = torch.tensor(np.asfortranarray(A / np.abs(A).max()))
     H = O.heisenberg(1.0)
     cfg = O.default_config()
-    cfg.update(chi=chi, min_iter=30, max_iter=30, rg_tol=0.0)
+    cfg.update(chi=chi, min_iter=iters, max_iter=iters, rg_tol=0.0)
     ts = O.make_ctm_tensors(A, cfg)
     traj = []
-    for i in range(30):
+    for i in range(iters):
         ts, s = O.rg_step(ts, chi)
         traj.append(complex(O.get_gs_energy(ts, H)[0]).real)
     with open(path, "w") as f:
         json.dump({"generator": "tests/golden/make_golden.py:bench_workload (CPU oracle)", "model": "heisenberg",
-                   "D": D, "d": d, "chi": chi, "seed": 1000, "energies": traj}, f, indent=1)
+                   "D": D, "d": d, "chi": chi, "seed": seed, "energies": traj}, f, indent=1)
     print("bench workload", traj[-2:])
 
 
-if __name__ == "__main__" and "--bench-workload" in sys.argv:
-    bench_workload()
+if __name__ == "__main__":
+    if "--bench-workload" in sys.argv:
+        bench_workload()
+    elif "--d5" in sys.argv:
+        bench_workload(os.path.join(HERE, "d5_chi100.json"), D=5, chi=100, iters=8, seed=1000)
+    else:
+        main()
