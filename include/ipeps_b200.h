@@ -82,10 +82,15 @@ IPEPS_API int ipeps_prof_query(ipeps_ctx* ctx, double* ms, uint64_t* launches, d
 IPEPS_API int ipeps_tcon(ipeps_ctx* ctx, int is_complex, const double* A, int nA, const int64_t* dimsA, const int* la,
                const double* B, int nB, const int64_t* dimsB, const int* lb, double* out, int64_t out_cap,
                int64_t* out_dims, int* out_nd);
-/* ---- projector: get_projector(R1, R2, chi) (ctmrg.jl:254-265) for real N x N R1, R2.
- * P1 (N x n) and P2 (n x N) need capacity N*(chi+1); s capacity chi+1; *n = kept count. */
-IPEPS_API int ipeps_projector(ipeps_ctx* ctx, const double* R1, const double* R2, int64_t N, int chi, double* P1,
-                    double* P2, double* s, int* n);
+/* ---- projector: get_projector(R1, R2, chi) (ctmrg.jl:254-265) for real R1 (N1 x K1) and
+ * R2 (K1 x N2), column-major.  P1 (K1 x n) and P2 (n x K1) need capacity K1*(chi+1); s capacity
+ * chi+1; *n = kept count (at most min(chi, K1) + 1, by the degenerate-pair rule of cutoff_matrix). */
+IPEPS_API int ipeps_projector(ipeps_ctx* ctx, const double* R1, const double* R2, int64_t N1, int64_t K1, int64_t N2,
+                    int chi, double* P1, double* P2, double* s, int* n);
+/* The same for ComplexF64 R1, R2 (interleaved re, im): P1 = R2 V S^-1/2, P2 = S^-1/2 U' R1
+ * with U' the conjugate transpose (ctmrg.jl:262-263); P1, P2 complex, s real. */
+IPEPS_API int ipeps_projector_c(ipeps_ctx* ctx, const double* R1, const double* R2, int64_t N1, int64_t K1,
+                      int64_t N2, int chi, double* P1, double* P2, double* s, int* n);
 
 /* ---- environment state: CTMTensors (src/ctm/ctm_tensor.jl:3-18, ctors :57-69) */
 IPEPS_API int ipeps_env_create(ipeps_ctx* ctx, int D, int d, int chi, int is_complex, ipeps_env** out);

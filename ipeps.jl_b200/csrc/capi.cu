@@ -196,13 +196,30 @@ int ipeps_tcon(ipeps_ctx* ctx, int is_complex, const double* A, int nA, const in
   });
 }
 
-int ipeps_projector(ipeps_ctx* ctx, const double* R1, const double* R2, int64_t N, int chi, double* P1,
-                    double* P2, double* s, int* n) {
+int ipeps_projector(ipeps_ctx* ctx, const double* R1, const double* R2, int64_t N1, int64_t K1, int64_t N2, int chi,
+                     double* P1, double* P2, double* s, int* n) {
   return guarded(ctx, [&] {
-    IPEPS_CHECK(R1 && R2 && N > 0 && chi > 0 && n, "bad projector arguments");
+    IPEPS_CHECK(R1 && R2 && N1 > 0 && K1 > 0 && N2 > 0 && chi > 0 && n, "bad projector arguments");
     auto& c = *ctx->c;
-    ipeps::MatRef r1{upload(c, R1, DType::F64, {N, N}), false};
-    ipeps::MatRef r2{upload(c, R2, DType::F64, {N, N}), false};
+    ipeps::MatRef r1{upload(c, R1, DType::F64, {N1, K1}), false};
+    ipeps::MatRef r2{upload(c, R2, DType::F64, {K1, N2}), false};
+    ipeps::SvdParams sp;
+    ipeps::ProjResult pr = ipeps::get_projector(c, r1, r2, chi, sp, nullptr);
+    *n = pr.n;
+    if (P1) download(c, P1, pr.P1);
+    if (P2) download(c, P2, pr.P2);
+    if (s) for (int i = 0; i < pr.n; ++i) s[i] = pr.s_host[i];
+    return IPEPS_OK;
+  });
+}
+
+int ipeps_projector_c(ipeps_ctx* ctx, const double* R1, const double* R2, int64_t N1, int64_t K1, int64_t N2, int chi,
+                       double* P1, double* P2, double* s, int* n) {
+  return guarded(ctx, [&] {
+    IPEPS_CHECK(R1 && R2 && N1 > 0 && K1 > 0 && N2 > 0 && chi > 0 && n, "bad projector arguments");
+    auto& c = *ctx->c;
+    ipeps::MatRef r1{upload(c, R1, DType::C128, {N1, K1}), false};
+    ipeps::MatRef r2{upload(c, R2, DType::C128, {K1, N2}), false};
     ipeps::SvdParams sp;
     ipeps::ProjResult pr = ipeps::get_projector(c, r1, r2, chi, sp, nullptr);
     *n = pr.n;

@@ -178,7 +178,6 @@ void init_ctm1(Env& e) {
 // renormalize + up_*.
 std::vector<double> ctm_move(Env& e, int dir, ProjResult* keep) {
   Ctx& c = *e.ctx;
-  IPEPS_CHECK(e.dt == DType::F64, "ctm_move: complex A needs the complex projector (not built)");
   auto t0 = std::chrono::steady_clock::now();
   NTPolicy p{c};
   Arr4<NTPolicy> Cs0, Es0;

@@ -185,7 +185,7 @@ __global__ void gather_cols_kernel(const double* in, int64_t ldi, int64_t m, con
     int j = int(t / m);
     double s = 1.0;
     if (scale_mode == 1) s = scale_v[j];
-    else if (scale_mode == 2) s = 1.0 / scale_v[j];
+    else if (scale_mode == 2) s = scale_v[j] != 0.0 ? 1.0 / scale_v[j] : 0.0;  // a null column stays zero
     out[i + j * ldo] = in[i + int64_t(perm[j]) * ldi] * s;
   }
 }

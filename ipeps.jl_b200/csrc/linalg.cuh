@@ -31,6 +31,13 @@ void trsm_right_upper(Ctx& c, const double* Y, int64_t ldy, int64_t N, int k, co
 // rotations when it fits; tol <= 0 means m * eps
 void jacobi_svd_auto(Ctx& c, double* X, int m, int k, int64_t ldx, double* J, int64_t ldj, double* S,
                      int max_sweeps, double tol, int* d_sweeps);
+// Complex (complex128) counterparts for complex iPEPS tensors, one CTA each;
+// complex_small_fits(m, k) says whether all three fit in shared memory.
+bool complex_small_fits(int m, int k);
+void chol_c(Ctx& c, void* G, int k, int64_t ldg, double shift_factor);
+void trsm_c(Ctx& c, const void* Y, int64_t ldy, int64_t N, int k, const void* R, int64_t ldr, void* Q, int64_t ldq);
+void jacobi_c_svd(Ctx& c, void* X, int m, int k, int64_t ldx, void* J, int64_t ldj, double* S, int max_sweeps,
+                  double tol, int* d_sweeps);
 // Descending sort with permutation (ties: later index first)
 void sort_desc(Ctx& c, const double* S, int k, double* S_out, int* perm);
 // out[:, j] = in[:, perm[j]] * f(scale[j]); scale_mode 0: 1, 1: scale, 2: 1/scale

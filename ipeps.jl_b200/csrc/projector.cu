@@ -1,4 +1,4 @@
-// Projector of the directional CTMRG move.
+// Projector of the directional CTMRG move (real and complex enlarged corners).
 //
 // The reference forms M = R1*R2 (N x N, N = chi*D^2) and takes its full LAPACK
 // SVD (ctmrg.jl:254-265, wrapper.jl:25-55).  Here M is never formed: a
@@ -103,81 +103,196 @@ __global__ void colnorm_max_kernel(const double* X, int64_t m, int nc, unsigned 
   if (lane == 0) atomicMax(out, static_cast<unsigned long long>(__double_as_longlong(sqrt(s))));
 }
 
+// ------------------------------------------------------------------ backends
+// The projector logic below is written once over two backends: real (FP64)
+// and complex (complex128) enlarged corners.  M = R1 R2 is N1 x N2 with
+// R1 (N1 x K1), R2 (K1 x N2); it is rectangular while the corner dimensions of
+// an environment still differ (first iterations from init_ctm1).  words is the
+// number of doubles per element, so that the gathers and column scalings can
+// treat a complex column as a real column of twice the height.
+
+struct RealOps {
+  Ctx& c;
+  const MatRef& R1;
+  const MatRef& R2;
+  static constexpr DType dt = DType::F64;
+  static constexpr int words = 1;
+  int64_t N1() const { return R1.rows(); }
+  int64_t K1() const { return R1.cols(); }
+  int64_t N2() const { return R2.cols(); }
+  Tensor M(const Tensor& X) { return apply(c, R1, 'N', apply(c, R2, 'N', X)); }   // M X
+  Tensor MH(const Tensor& X) { return apply(c, R2, 'T', apply(c, R1, 'T', X)); }  // M^T X
+  Tensor orth_(const Tensor& Y, int passes) { return orth(c, Y, passes, nullptr); }
+  // X = Bh^H Q2 (k x k) for Bh = M^H Q (N2 x k)
+  Tensor small(const Tensor& Bh, const Tensor& Q2, int k) {
+    Tensor X = c.alloc(dt, {k, k});
+    gemm(c, dt, 'T', 'N', k, k, N2(), cplx(1), Bh.data(), N2(), Q2.data(), N2(), cplx(0), X.data(), k, true);
+    return X;
+  }
+  void jacobi(Tensor& X, Tensor& J, Tensor& S, int k, const SvdParams& sp, int* d_sweeps) {
+    jacobi_svd_auto(c, X.f64(), k, k, k, J.f64(), k, S.f64(), sp.jacobi_max_sweeps, sp.jacobi_tol, d_sweeps);
+  }
+  // sketch width: 128 columns when that still oversamples by want/2 (the
+  // Jacobi then rotates all of its 64 pairs in one pass of its 8-lane groups),
+  // else at most 160 (the widest sketch whose Jacobi fits in shared memory)
+  int width(int want, int kw, const SvdParams& sp) const {
+    if (kw > 128 && want + std::max(sp.min_oversample, want / 2) <= 128) return 128;
+    if (kw > 160 && want + sp.min_oversample <= 160) return 160;
+    return kw;
+  }
+  Tensor P1(const Tensor& V) { return apply(c, R2, 'N', V); }          // R2 V      (K1 x n)
+  Tensor P2(const Tensor& U) { return apply_left_T(c, U, R1, 'N'); }   // U^T R1    (n x K1)
+};
+
+Tensor cmm(Ctx& c, char oa, char ob, int64_t m, int64_t n, int64_t k, const Tensor& A, int64_t lda, const Tensor& B,
+           int64_t ldb) {
+  Tensor Y = c.alloc(DType::C128, {m, n});
+  gemm(c, DType::C128, oa, ob, m, n, k, cplx(1), A.data(), lda, B.data(), ldb, cplx(0), Y.data(), m, true);
+  return Y;
+}
+
+Tensor orth_c(Ctx& c, const Tensor& Y0, int passes) {
+  const int64_t N = Y0.dims[0];
+  const int k = int(Y0.dims[1]);
+  Tensor Y = Y0;
+  Tensor G = c.alloc(DType::C128, {k, k});
+  const double u = 1.1102230246251565e-16;
+  for (int pass = 0; pass < passes; ++pass) {
+    gemm(c, DType::C128, 'C', 'N', k, k, N, cplx(1), Y.data(), N, Y.data(), N, cplx(0), G.data(), k, true);
+    const double sf = (pass == 0) ? 11.0 * (double(N) * k + double(k) * (k + 1)) * u : 0.0;
+    chol_c(c, G.data(), k, k, sf);
+    Tensor Yn = c.alloc(DType::C128, {N, k});
+    trsm_c(c, Y.data(), N, N, k, G.data(), k, Yn.data(), N);
+    Y = Yn;
+  }
+  return Y;
+}
+
+struct ComplexOps {
+  Ctx& c;
+  Tensor R1, R2;  // materialised (untransposed) complex128
+  static constexpr DType dt = DType::C128;
+  static constexpr int words = 2;
+  ComplexOps(Ctx& cc, const MatRef& a, const MatRef& b)
+      : c(cc),
+        R1(to_complex(cc, a.trans ? permute(cc, a.t, {1, 0}) : a.t)),
+        R2(to_complex(cc, b.trans ? permute(cc, b.t, {1, 0}) : b.t)) {}
+  int64_t N1() const { return R1.dims[0]; }
+  int64_t K1() const { return R1.dims[1]; }
+  int64_t N2() const { return R2.dims[1]; }
+  Tensor M(const Tensor& X) {
+    const int64_t n = X.dims[1];
+    return cmm(c, 'N', 'N', N1(), n, K1(), R1, N1(), cmm(c, 'N', 'N', K1(), n, N2(), R2, K1(), X, N2()), K1());
+  }
+  Tensor MH(const Tensor& X) {
+    const int64_t n = X.dims[1];
+    return cmm(c, 'C', 'N', N2(), n, K1(), R2, K1(), cmm(c, 'C', 'N', K1(), n, N1(), R1, N1(), X, N1()), K1());
+  }
+  Tensor orth_(const Tensor& Y, int passes) { return orth_c(c, Y, passes); }
+  Tensor small(const Tensor& Bh, const Tensor& Q2, int k) { return cmm(c, 'C', 'N', k, k, N2(), Bh, N2(), Q2, N2()); }
+  void jacobi(Tensor& X, Tensor& J, Tensor& S, int k, const SvdParams& sp, int* d_sweeps) {
+    jacobi_c_svd(c, X.data(), k, k, k, J.data(), k, S.f64(), sp.jacobi_max_sweeps, sp.jacobi_tol, d_sweeps);
+  }
+  int width(int want, int kw, const SvdParams& sp) const {
+    while (kw > want + sp.min_oversample && !complex_small_fits(kw, kw)) --kw;
+    IPEPS_CHECK(complex_small_fits(kw, kw), "get_projector: complex sketch too wide for the shared-memory kernels");
+    return kw;
+  }
+  Tensor P1(const Tensor& V) { return cmm(c, 'N', 'N', K1(), V.dims[1], N2(), R2, K1(), V, N2()); }
+  Tensor P2(const Tensor& U) { return cmm(c, 'C', 'N', U.dims[1], K1(), N1(), U, N1(), R1, N1()); }
+};
+
 // One sketch pass: range finder with q power iterations from Omega, Rayleigh-Ritz, Jacobi.
 struct Sketch {
-  Tensor Q, Q2, X, J, Ss;  // Q, Q2: N x k; X = W (k x k); J (k x k); Ss sorted S (k)
+  Tensor Q, Q2, X, J, Ss;  // Q: N1 x k, Q2: N2 x k; X = W (k x k); J (k x k); Ss sorted S (k)
   Tensor perm;             // int[k] stored in a double buffer
   int sweeps = 0;
 };
 
-Sketch sketch_pass(Ctx& c, const MatRef& R1, const MatRef& R2, const Tensor& Om, int q, const SvdParams& sp) {
-  const int64_t N = R1.rows();
+// inter: CholeskyQR passes of the intermediate sketches.  One shifted pass
+// suppresses directions below ~sqrt(shift) ~ 1e-6 s_1, which over the power
+// iterations then decay away; three passes (sCholQR3) keep them, as needed
+// when the truncation reaches down to the 1e-12 relative cutoff.
+template <class Ops>
+Sketch sketch_pass(Ctx& c, Ops& o, const Tensor& Om, int q, const SvdParams& sp, int inter) {
   const int k = int(Om.dims[1]);
   Sketch s;
-  Tensor Y = apply(c, R1, 'N', apply(c, R2, 'N', Om));
+  Tensor Y = o.M(Om);
   for (int it = 0; it < q; ++it) {
-    Tensor Q = orth(c, Y, sp.inter_passes, nullptr);
-    Tensor Z = orth(c, apply(c, R2, 'T', apply(c, R1, 'T', Q)), sp.inter_passes, nullptr);
-    Y = apply(c, R1, 'N', apply(c, R2, 'N', Z));
+    Tensor Q = o.orth_(Y, inter);
+    Tensor Z = o.orth_(o.MH(Q), inter);
+    Y = o.M(Z);
   }
-  s.Q = orth(c, Y, 3, nullptr);
-  // B^T = M^T Q (N x k);  B^T = Q2 R  =>  B = R^T Q2^T
-  Tensor Bt = apply(c, R2, 'T', apply(c, R1, 'T', s.Q));
-  Tensor Rm;
-  s.Q2 = orth(c, Bt, 3, &Rm);
-  // X = R^T ; one-sided Jacobi: X J = W = Ux S  =>  U = Q Ux, V = Q2 J
-  s.X = permute(c, Rm, {1, 0});
-  s.J = c.alloc(DType::F64, {k, k});
+  s.Q = o.orth_(Y, 3);
+  // B^H = M^H Q (N2 x k), Q2 = orth(B^H).  The Rayleigh-Ritz matrix is formed
+  // explicitly, X = B = (M^H Q)^H Q2, rather than taken as R^H from B^H = Q2 R:
+  // when M is numerically rank deficient the shifted first CholeskyQR pass
+  // leaves sqrt(shift)-sized entries in R for the null directions, which the
+  // later passes cannot normalise, and R^H would show them as spurious
+  // singular values far above the 1e-12 cutoff.
+  Tensor Bh = o.MH(s.Q);
+  s.Q2 = o.orth_(Bh, 3);
+  s.X = o.small(Bh, s.Q2, k);
+  // one-sided Jacobi: X J = W = Ux S  =>  U = Q Ux, V = Q2 J
+  s.J = c.alloc(Ops::dt, {k, k});
   Tensor S = c.alloc(DType::F64, {k});
   int* d_sweeps = reinterpret_cast<int*>(static_cast<char*>(c.scal->p) + 3900);
-  jacobi_svd_auto(c, s.X.f64(), k, k, k, s.J.f64(), k, S.f64(), sp.jacobi_max_sweeps, sp.jacobi_tol, d_sweeps);
+  o.jacobi(s.X, s.J, S, k, sp, d_sweeps);
   s.Ss = c.alloc(DType::F64, {k});
   s.perm = c.alloc(DType::F64, {(k + 1) / 2});
   sort_desc(c, S.f64(), k, s.Ss.f64(), static_cast<int*>(s.perm.data()));
   IPEPS_CUDA(cudaMemcpyAsync(&s.sweeps, d_sweeps, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
-  (void)N;
   return s;
 }
 
-}  // namespace
+void copy_cols(Ctx& c, Tensor& dst, const Tensor& src, int64_t rows, int ncols, int words) {
+  IPEPS_CUDA(cudaMemcpyAsync(dst.data(), src.data(), size_t(rows) * ncols * 8 * words, cudaMemcpyDeviceToDevice,
+                             c.stream));
+}
 
-ProjResult get_projector(Ctx& c, const MatRef& R1, const MatRef& R2, int chi, const SvdParams& sp,
-                         ProjCache* cache, bool keep_factors) {
-  const int64_t N = R1.rows();
-  IPEPS_CHECK(R1.cols() == R2.rows() && R2.cols() == N, "get_projector: R1*R2 must be square");
-  IPEPS_CHECK(R1.t.dt == DType::F64 && R2.t.dt == DType::F64, "get_projector: real operands expected");
-  const int new_chi = int(std::min<int64_t>(chi, R1.cols()));
-  const int want = int(std::min<int64_t>(N, new_chi + 1));
-  int over = std::max(sp.min_oversample, want * sp.oversample_num / std::max(sp.oversample_den, 1));
-  int kw = int(std::min<int64_t>(N, int64_t(want) + over));
-  // at most 128 columns when the minimum oversampling allows it: the Jacobi
-  // then rotates all of its pairs (64) in one pass of its 64 half-warps
-  if (kw > 128 && want + sp.min_oversample <= 128) kw = 128;
-  const int k = kw;
+template <class Ops>
+ProjResult projector_impl(Ctx& c, Ops& o, int chi, const SvdParams& sp, ProjCache* cache, bool keep_factors) {
+  constexpr DType dt = Ops::dt;
+  constexpr int w = Ops::words;
+  const int64_t N1 = o.N1(), K1 = o.K1(), N2 = o.N2(), Nmin = std::min(N1, N2);
+  const int new_chi = int(std::min<int64_t>(chi, K1));
+  const int want = int(std::min<int64_t>(Nmin, new_chi + 1));
+  const int over = std::max(sp.min_oversample, want * sp.oversample_num / std::max(sp.oversample_den, 1));
+  const int k = o.width(want, int(std::min<int64_t>(Nmin, int64_t(want) + over)), sp);
 
-  // sketch Omega (N x k): resolved right vectors of the previous call first, then Gaussian columns
-  Tensor Om = c.alloc(DType::F64, {N, k});
+  // Sketch Omega (N2 x k): resolved right vectors of an earlier call first,
+  // then Gaussian columns.  No seeds when k = min(N1, N2): a Gaussian Omega
+  // then spans the domain and one pass is exact, which seed vectors (possibly
+  // confined to a few symmetry sectors of M) would not guarantee.  After a
+  // cutoff-limited truncation at least min_oversample columns stay Gaussian,
+  // so that directions absent from the seeds can enter; in the chi-limited
+  // regime the seeds may fill the sketch.
+  Tensor Om = c.alloc(dt, {N2, k});
   randn(c, Om);
   bool warm = false;
-  if (sp.warm_start && cache && !cache->seed(sp.seed_older).empty() && cache->seed(sp.seed_older).dims[0] == N) {
+  const bool room = !cache || cache->cutoff_limited;
+  const int seed_cap = room ? std::max(0, k - std::max(sp.min_oversample, 1)) : k;
+  if (k < Nmin && seed_cap > 0 && sp.warm_start && cache && !cache->seed(sp.seed_older).empty() &&
+      cache->seed(sp.seed_older).dims[0] == N2 && cache->seed(sp.seed_older).dt == dt) {
     const Tensor& Vs = cache->seed(sp.seed_older);
-    int nv = int(std::min<int64_t>(Vs.dims[1], k));
-    IPEPS_CUDA(cudaMemcpyAsync(Om.data(), Vs.data(), size_t(N) * nv * 8, cudaMemcpyDeviceToDevice, c.stream));
+    copy_cols(c, Om, Vs, N2, int(std::min<int64_t>(Vs.dims[1], seed_cap)), w);
     warm = true;
   }
-  int q = (k == N) ? 0 : (warm ? sp.power_iters_warm : sp.power_iters);
+  int q = (k == Nmin) ? 0 : (warm ? sp.power_iters_warm : sp.power_iters);
+  int inter = sp.inter_passes;
+  if (!warm || !cache || cache->cutoff_limited) inter = std::max(inter, 3);
 
   ProjResult r;
   r.k = k;
   Sketch sk;
   std::vector<double> all(k);
-  int n = 0;
+  int n = 0, n_above_last = 0;
   Tensor Ux, Vk;
   int* d_perm = nullptr;
   double* d_res = reinterpret_cast<double*>(c.scal->p) + 48;
   double prev_res = 1e300;
   for (int attempt = 0;; ++attempt) {
-    sk = sketch_pass(c, R1, R2, Om, q, sp);
+    sk = sketch_pass(c, o, Om, q, sp, inter);
     d_perm = static_cast<int*>(sk.perm.data());
     IPEPS_CUDA(cudaMemcpyAsync(all.data(), sk.Ss.data(), size_t(k) * 8, cudaMemcpyDeviceToHost, c.stream));
     c.sync();
@@ -187,32 +302,42 @@ ProjResult get_projector(Ctx& c, const MatRef& R1, const MatRef& R2, int chi, co
     int n_above = 0;
     for (int i = 0; i < k; ++i)
       if (smax > 0 && all[i] / smax > 1e-12) n_above++;
+    n_above_last = n_above;
+    if (n_above < new_chi && inter < 3 && q > 0) {
+      // cutoff-limited after cheap intermediates: small directions may be missing; redo cold with sCholQR3
+      inter = 3;
+      Om = c.alloc(dt, {N2, k});
+      randn(c, Om);
+      q = sp.power_iters;
+      --attempt;
+      continue;
+    }
     n = std::min(new_chi, n_above);
     IPEPS_CHECK(n >= 1, "get_projector: no singular value above the cutoff (zero enlarged corner?)");
-    // the reference's s has length N (full SVD); ours is the top-k part, k > n whenever N > n
-    if (int64_t(N) > n && k > n) {
+    // the reference's s has length min(N1, N2) (full SVD); ours is the top-k part
+    if (Nmin > n && k > n) {
       if (std::fabs(all[n] - all[n - 1]) < 1e-10) n = n + 1;
     }
     IPEPS_CHECK(n <= k, "get_projector: truncation beyond the sketch");
     // Ux[:, j] = W[:, perm[j]] / S_sorted[j] (kept + one), Vk = Q2 J[:, perm]
     const int nc = std::min(n + 1, k);
-    Ux = c.alloc(DType::F64, {k, nc});
-    gather_cols(c, sk.X.f64(), k, k, d_perm, nc, sk.Ss.f64(), 2, Ux.f64(), k);
-    Tensor Js = c.alloc(DType::F64, {k, k});
-    gather_cols(c, sk.J.f64(), k, k, d_perm, k, nullptr, 0, Js.f64(), k);
-    Vk = c.alloc(DType::F64, {N, k});
-    gemm(c, DType::F64, 'N', 'N', N, k, k, cplx(1), sk.Q2.data(), N, Js.data(), k, cplx(0), Vk.data(), N, true);
-    if (q == 0 && k == N) break;  // the sketch spans everything: exact
+    Ux = c.alloc(dt, {k, nc});
+    gather_cols(c, sk.X.f64(), w * k, w * k, d_perm, nc, sk.Ss.f64(), 2, Ux.f64(), w * k);
+    Tensor Js = c.alloc(dt, {k, k});
+    gather_cols(c, sk.J.f64(), w * k, w * k, d_perm, k, nullptr, 0, Js.f64(), w * k);
+    Vk = c.alloc(dt, {N2, k});
+    gemm(c, dt, 'N', 'N', N2, k, k, cplx(1), sk.Q2.data(), N2, Js.data(), k, cplx(0), Vk.data(), N2, true);
+    if (q == 0 && k == Nmin) break;  // the sketch spans a whole side of M: exact
     if (attempt >= sp.max_extra_passes) break;
     // residual of the kept triplets: ||M v_i - s_i u_i|| <= resid_tol * s_1
-    Tensor Vc = c.alloc(DType::F64, {N, nc});
-    IPEPS_CUDA(cudaMemcpyAsync(Vc.data(), Vk.data(), size_t(N) * nc * 8, cudaMemcpyDeviceToDevice, c.stream));
-    Tensor Res = apply(c, R1, 'N', apply(c, R2, 'N', Vc));
-    Tensor Us = c.alloc(DType::F64, {k, nc});
-    gather_cols(c, sk.X.f64(), k, k, d_perm, nc, nullptr, 0, Us.f64(), k);  // W = Ux S
-    gemm(c, DType::F64, 'N', 'N', N, nc, k, cplx(-1), sk.Q.data(), N, Us.data(), k, cplx(1), Res.data(), N, true);
+    Tensor Vc = c.alloc(dt, {N2, nc});
+    copy_cols(c, Vc, Vk, N2, nc, w);
+    Tensor Res = o.M(Vc);
+    Tensor Us = c.alloc(dt, {k, nc});
+    gather_cols(c, sk.X.f64(), w * k, w * k, d_perm, nc, nullptr, 0, Us.f64(), w * k);  // W = Ux S
+    gemm(c, dt, 'N', 'N', N1, nc, k, cplx(-1), sk.Q.data(), N1, Us.data(), k, cplx(1), Res.data(), N1, true);
     IPEPS_CUDA(cudaMemsetAsync(d_res, 0, 8, c.stream));
-    colnorm_max_kernel<<<(nc * 32 + 255) / 256, 256, 0, c.stream>>>(Res.f64(), N, nc,
+    colnorm_max_kernel<<<(nc * 32 + 255) / 256, 256, 0, c.stream>>>(Res.f64(), w * N1, nc,
                                                                     reinterpret_cast<unsigned long long*>(d_res));
     IPEPS_LAUNCH_CHECK();
     double res = 0;
@@ -232,10 +357,10 @@ ProjResult get_projector(Ctx& c, const MatRef& R1, const MatRef& R2, int chi, co
   r.n = n;
   r.s_host.assign(all.begin(), all.begin() + n);
 
-  Tensor U = c.alloc(DType::F64, {N, n});
-  gemm(c, DType::F64, 'N', 'N', N, n, k, cplx(1), sk.Q.data(), N, Ux.data(), k, cplx(0), U.data(), N, true);
-  Tensor V = c.alloc(DType::F64, {N, n});
-  IPEPS_CUDA(cudaMemcpyAsync(V.data(), Vk.data(), size_t(N) * n * 8, cudaMemcpyDeviceToDevice, c.stream));
+  Tensor U = c.alloc(dt, {N1, n});
+  gemm(c, dt, 'N', 'N', N1, n, k, cplx(1), sk.Q.data(), N1, Ux.data(), k, cplx(0), U.data(), N1, true);
+  Tensor V = c.alloc(dt, {N2, n});
+  copy_cols(c, V, Vk, N2, n, w);
   // resolved part of the sketch: s_a > 1e-13 s_1 (W/s is accurate there)
   int rr = 0;
   while (rr < k && all[rr] > 1e-13 * all[0]) ++rr;
@@ -243,32 +368,47 @@ ProjResult get_projector(Ctx& c, const MatRef& R1, const MatRef& R2, int chi, co
   if (cache) {
     // seed for the next call of this direction: the resolved right vectors only
     // (near-null directions of this M say nothing about the next one)
-    Tensor Vc = c.alloc(DType::F64, {N, rr});
-    IPEPS_CUDA(cudaMemcpyAsync(Vc.data(), Vk.data(), size_t(N) * rr * 8, cudaMemcpyDeviceToDevice, c.stream));
+    Tensor Vc = c.alloc(dt, {N2, rr});
+    copy_cols(c, Vc, Vk, N2, rr, w);
     cache->Vold = cache->V;
     cache->V = Vc;
+    cache->cutoff_limited = n_above_last < new_chi;
   }
   if (keep_factors) {
+    IPEPS_CHECK(dt == DType::F64, "get_projector: the projector adjoint is real-only");
     r.r = rr;
     r.sr_host.assign(all.begin(), all.begin() + rr);
-    Tensor Uxr = c.alloc(DType::F64, {k, rr});
+    Tensor Uxr = c.alloc(dt, {k, rr});
     gather_cols(c, sk.X.f64(), k, k, d_perm, rr, sk.Ss.f64(), 2, Uxr.f64(), k);
-    r.Ur = c.alloc(DType::F64, {N, rr});
-    gemm(c, DType::F64, 'N', 'N', N, rr, k, cplx(1), sk.Q.data(), N, Uxr.data(), k, cplx(0), r.Ur.data(), N, true);
-    r.Vr = c.alloc(DType::F64, {N, rr});
-    IPEPS_CUDA(cudaMemcpyAsync(r.Vr.data(), Vk.data(), size_t(N) * rr * 8, cudaMemcpyDeviceToDevice, c.stream));
+    r.Ur = c.alloc(dt, {N1, rr});
+    gemm(c, dt, 'N', 'N', N1, rr, k, cplx(1), sk.Q.data(), N1, Uxr.data(), k, cplx(0), r.Ur.data(), N1, true);
+    r.Vr = c.alloc(dt, {N2, rr});
+    copy_cols(c, r.Vr, Vk, N2, rr, w);
     r.Sr = c.alloc(DType::F64, {rr});
     IPEPS_CUDA(cudaMemcpyAsync(r.Sr.data(), sk.Ss.data(), size_t(rr) * 8, cudaMemcpyDeviceToDevice, c.stream));
   }
 
   r.S = c.alloc(DType::F64, {n});
   IPEPS_CUDA(cudaMemcpyAsync(r.S.data(), sk.Ss.data(), size_t(n) * 8, cudaMemcpyDeviceToDevice, c.stream));
-  // P1 = R2 V S^-1/2 ; P2 = S^-1/2 U^T R1
-  scale_cols(c, V.f64(), N, N, n, r.S.f64(), 1);
-  scale_cols(c, U.f64(), N, N, n, r.S.f64(), 1);
-  r.P1 = apply(c, R2, 'N', V);
-  r.P2 = apply_left_T(c, U, R1, 'N');
+  // P1 = R2 V S^-1/2 ; P2 = S^-1/2 U^H R1
+  scale_cols(c, V.f64(), w * N2, w * N2, n, r.S.f64(), 1);
+  scale_cols(c, U.f64(), w * N1, w * N1, n, r.S.f64(), 1);
+  r.P1 = o.P1(V);
+  r.P2 = o.P2(U);
   return r;
+}
+
+}  // namespace
+
+ProjResult get_projector(Ctx& c, const MatRef& R1, const MatRef& R2, int chi, const SvdParams& sp,
+                         ProjCache* cache, bool keep_factors) {
+  IPEPS_CHECK(R1.cols() == R2.rows(), "get_projector: inner dimensions of R1*R2 differ");
+  if (R1.t.dt == DType::C128 || R2.t.dt == DType::C128) {
+    ComplexOps o(c, R1, R2);
+    return projector_impl(c, o, chi, sp, cache, keep_factors);
+  }
+  RealOps o{c, R1, R2};
+  return projector_impl(c, o, chi, sp, cache, keep_factors);
 }
 
 }  // namespace ipeps

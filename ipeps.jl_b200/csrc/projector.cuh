@@ -18,7 +18,7 @@ struct SvdParams {
   int oversample_den = 1;
   int min_oversample = 16;
   int power_iters = 3;      // cold start
-  int power_iters_warm = 1; // when the previous V of this direction seeds the sketch
+  int power_iters_warm = 2; // when the previous V of this direction seeds the sketch
   int max_extra_passes = 6; // extra power iterations while the residual check fails
   int inter_passes = 1;     // CholeskyQR passes for the intermediate power-iteration sketches
   bool seed_older = true;   // seed from the call before the previous one (period-2 cycles)
@@ -28,7 +28,6 @@ struct SvdParams {
   double jacobi_tol = 0.0;  // <= 0: m * eps (rounding level of the column dot products)
 };
 
-// Cache of the last right singular vectors of one direction (warm start).
 // Resolved right vectors of the last two calls of one direction (warm start).
 // The sketch is seeded from the older one: a CTMRG run that has settled into
 // a period-2 cycle returns to the same environment every second iteration,
@@ -36,6 +35,9 @@ struct SvdParams {
 struct ProjCache {
   Tensor V;      // previous call
   Tensor Vold;   // the call before
+  // the last truncation of this direction was set by the 1e-12 cutoff rather
+  // than by chi: the next sketch keeps its small directions (sCholQR3 throughout)
+  bool cutoff_limited = true;
   const Tensor& seed(bool older) const { return (older && !Vold.empty()) ? Vold : V; }
 };
 

@@ -460,7 +460,7 @@ __global__ void __launch_bounds__(kApplyRows * 32) jacobi_apply_kernel(const dou
     for (int j = lane; j < k; j += 32) J[i + int64_t(j) * ldj] = row[j];
 }
 
-bool g_chol_attr = false, g_trsm_attr[9] = {}, g_jlog_attr[9] = {}, g_apply_attr = false;
+bool g_chol_attr = false, g_trsm_attr[9] = {}, g_jlog_attr[11] = {}, g_apply_attr = false;
 
 template <int NV>
 void launch_jacobi(Ctx& c, double* X, int m, int k, int64_t ldx, double2* rot, int max_sweeps, double tol, double* S,
@@ -527,7 +527,7 @@ void jacobi_svd_auto(Ctx& c, double* X, int m, int k, int64_t ldx, double* J, in
   if (tol <= 0) tol = double(m) * 2.220446049250313e-16;  // rounding level of the column dot products
   const int nv = (m + 15) / 16;
   const size_t smem = (size_t(16) * nv * k + k) * 8;
-  if (k < 2 || nv > 8 || k > 2 * kMaxPairs || smem > kSmemMax || apply_smem_bytes(k) > kSmemMax) {
+  if (k < 2 || nv > 10 || k > 2 * kMaxPairs || smem > kSmemMax || apply_smem_bytes(k) > kSmemMax) {
     jacobi_svd(c, X, m, k, ldx, J, ldj, S, max_sweeps, tol, d_sweeps);
     return;
   }
@@ -544,7 +544,9 @@ void jacobi_svd_auto(Ctx& c, double* X, int m, int k, int64_t ldx, double* J, in
       case 5: launch_jacobi<5>(c, X, m, k, ldx, rp, max_sweeps, tol, S, d_sweeps, smem); break;
       case 6: launch_jacobi<6>(c, X, m, k, ldx, rp, max_sweeps, tol, S, d_sweeps, smem); break;
       case 7: launch_jacobi<7>(c, X, m, k, ldx, rp, max_sweeps, tol, S, d_sweeps, smem); break;
-      default: launch_jacobi<8>(c, X, m, k, ldx, rp, max_sweeps, tol, S, d_sweeps, smem); break;
+      case 8: launch_jacobi<8>(c, X, m, k, ldx, rp, max_sweeps, tol, S, d_sweeps, smem); break;
+      case 9: launch_jacobi<9>(c, X, m, k, ldx, rp, max_sweeps, tol, S, d_sweeps, smem); break;
+      default: launch_jacobi<10>(c, X, m, k, ldx, rp, max_sweeps, tol, S, d_sweeps, smem); break;
     }
     c.count(KFam::Jacobi, 6.0 * double(m) * k * k / 2.0);
   }

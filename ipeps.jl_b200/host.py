@@ -39,7 +39,7 @@ EXPORTED = [
     "ipeps_env_set_params", "ipeps_env_set_svd_params", "ipeps_env_set_A", "ipeps_env_init",
     "ipeps_env_get_CT", "ipeps_env_set_CT", "ipeps_ctm_move", "ipeps_ctm_step", "ipeps_ctm_run",
     "ipeps_ctm_log", "ipeps_energy", "ipeps_gs_norm", "ipeps_nested_set_B", "ipeps_es_energy",
-    "ipeps_all_norm", "ipeps_tcon", "ipeps_projector", "ipeps_ctx_stream", "ipeps_prof_enable",
+    "ipeps_all_norm", "ipeps_tcon", "ipeps_projector", "ipeps_projector_c", "ipeps_ctx_stream", "ipeps_prof_enable",
     "ipeps_prof_query", "ipeps_energy_grad", "ipeps_env_set_mixed", "ipeps_es_energy_grad",
     "ipeps_single_dm_Ad",
 ]
@@ -107,7 +107,8 @@ def load_library(path: str = LIB_PATH) -> ct.CDLL:
         "ipeps_es_energy": [P, dp, dp, I, dp],
         "ipeps_all_norm": [P, dp, dp],
         "ipeps_tcon": [P, I, dp, I, lp, ip, dp, I, lp, ip, dp, ct.c_int64, lp, ip],
-        "ipeps_projector": [P, dp, dp, ct.c_int64, I, dp, dp, dp, ip],
+        "ipeps_projector": [P, dp, dp, ct.c_int64, ct.c_int64, ct.c_int64, I, dp, dp, dp, ip],
+        "ipeps_projector_c": [P, dp, dp, ct.c_int64, ct.c_int64, ct.c_int64, I, dp, dp, dp, ip],
         "ipeps_ctx_stream": [P, ct.POINTER(P)],
         "ipeps_prof_enable": [P, I],
         "ipeps_prof_query": [P, dp, ct.POINTER(ct.c_uint64), dp, dp],
@@ -271,7 +272,7 @@ class CTMTensors:
             self.h, int(p.get("chi", 30)), int(p.get("min_iter", 4)), int(p.get("max_iter", 20)),
             int(p.get("ad_max_iter", 4)), float(p.get("rg_tol", 1e-6))))
         over = p.get("svd_oversample", (1, 1, 16))
-        pit = p.get("svd_power_iters", (3, 1))
+        pit = p.get("svd_power_iters", (3, 2))
         self.engine.check(self.lib.ipeps_env_set_svd_params(
             self.h, int(over[0]), int(over[1]), int(over[2]), int(pit[0]), int(pit[1]),
             int(bool(p.get("svd_warm_start", True))), float(p.get("svd_resid_tol", 1e-11)),
@@ -355,16 +356,22 @@ def tcon(xs, ind_xs, engine: Optional[Engine] = None):
 def get_projector(R1, R2, chi: int, engine: Optional[Engine] = None):
     """get_projector(R1, R2, chi) (ctmrg.jl:254-265) on the device: (P1, P2, S)."""
     eng = engine or default_engine()
-    R1 = _fortran(R1, np.float64)
-    R2 = _fortran(R2, np.float64)
-    N = R1.shape[0]
-    P1 = np.empty(N * (chi + 1))
-    P2 = np.empty(N * (chi + 1))
+    cplx = np.iscomplexobj(R1) or np.iscomplexobj(R2)
+    dt = np.complex128 if cplx else np.float64
+    R1 = _fortran(R1, dt)
+    R2 = _fortran(R2, dt)
+    N1, K1 = R1.shape
+    K1b, N2 = R2.shape
+    if K1b != K1:
+        raise ValueError("get_projector: inner dimensions of R1 * R2 differ")
+    P1 = np.empty(K1 * (chi + 1), dtype=dt)
+    P2 = np.empty(K1 * (chi + 1), dtype=dt)
     s = np.empty(chi + 1)
     n = ct.c_int(0)
-    eng.check(eng.lib.ipeps_projector(eng.h, _dp(R1), _dp(R2), N, int(chi), _dp(P1), _dp(P2), _dp(s), ct.byref(n)))
+    fn = eng.lib.ipeps_projector_c if cplx else eng.lib.ipeps_projector
+    eng.check(fn(eng.h, _dp(R1), _dp(R2), N1, K1, N2, int(chi), _dp(P1), _dp(P2), _dp(s), ct.byref(n)))
     k = n.value
-    return (P1[: N * k].reshape((N, k), order="F"), P2[: N * k].reshape((k, N), order="F"), s[:k].copy())
+    return (P1[: K1 * k].reshape((K1, k), order="F"), P2[: K1 * k].reshape((k, K1), order="F"), s[:k].copy())
 
 
 # ------------------------------------------------------------------ moves

@@ -68,9 +68,31 @@ def bench_workload(path=os.path.join(HERE, "bench_workload.json"), D=4, chi=64, 
     print("bench workload", traj[-2:])
 
 
+def honeycomb_kat(path=os.path.join(HERE, "honeycomb_kat.json")):
+    """The reference's energy known-answer cases (test/test_model.jl:9-16 and
+    :78-83, -0.16349 +- 1e-5 for real(E)/8): complex A with d = 4, default
+    config (chi = 32), converged from init_ctm1 with the energy criterion.
+    Stores the oracle's energy trajectory and converged energy for each."""
+    out = []
+    for name, A, H in [("init_hb_gs_XX", O.init_hb_gs(2, p1=0.24, p2=0, dir="XX"), O.honeycomb(1, 1, dir="XX")),
+                       ("ghz", O.get_Q_ghz(), O.honeycomb(1, 1))]:
+        cfg = O.default_config()
+        log = []
+        E, Na = O.compute_gs_energy(A, H, cfg, log=log)
+        E = complex(E)
+        out.append({"name": name, "chi": cfg["chi"], "min_iter": cfg["min_iter"], "max_iter": cfg["max_iter"],
+                    "rg_tol": cfg["rg_tol"], "E": [E.real, E.imag], "E_over_8": E.real / 8,
+                    "iters": len(log), "trajectory": [complex(l["obj"]).real for l in log]})
+        print(name, E.real / 8, len(log))
+    with open(path, "w") as f:
+        json.dump({"generator": "tests/golden/make_golden.py:honeycomb_kat (CPU oracle)", "cases": out}, f, indent=1)
+
+
 if __name__ == "__main__":
     if "--bench-workload" in sys.argv:
         bench_workload()
+    elif "--honeycomb" in sys.argv:
+        honeycomb_kat()
     elif "--d5" in sys.argv:
         bench_workload(os.path.join(HERE, "d5_chi100.json"), D=5, chi=100, iters=8, seed=1000)
     else:

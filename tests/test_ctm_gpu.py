@@ -172,3 +172,21 @@ def test_bench_workload_trajectory(engine, pkg):
     got = [l["obj"].real for l in info["log"]]
     err = max(abs(a - b) for a, b in zip(got, g["energies"]))
     assert err <= 1e-10, err
+
+
+def test_d5_chi100_trajectory(engine, pkg):
+    """Heisenberg D=5 chi=100 (enlarged corners 2500 x 2500, 160-column
+    sketch): 8 iterations from init_ctm1 against the oracle's energies."""
+    with open(os.path.join(GOLD, "d5_chi100.json")) as f:
+        gold = json.load(f)
+    A = npa(O.random_A(gold["D"], gold["d"], seed=gold["seed"]))
+    cfg = O.default_config()
+    n = len(gold["energies"])
+    cfg.update(chi=gold["chi"], min_iter=n, max_iter=n, rg_tol=0.0)
+    H = [npa(h) for h in O.heisenberg(1.0)]
+    ts = pkg.CTMTensors(A, cfg, engine=engine)
+    ts, info = pkg.run_ctm(ts, conv_fun="energy", H=H)
+    traj = [l["obj"].real for l in info["log"]]
+    err = max(abs(a - b) for a, b in zip(traj, gold["energies"]))
+    assert err <= 1e-10, err
+    ts.close()
