@@ -9,7 +9,9 @@ iterations + the energy.  CTMRG moves/s is measured on the forward part alone
 and reported beside it.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|mixed]
+                    [--workload d4chi64|d5chi100]
     python bench.py --impl reference ...   # CPU arm (see below)
+    python bench.py --forward-only 6       # profiling aid: 6 forward iterations, no timing
 
 Timing: K steps timed with CUDA events recorded on the engine's own stream,
 L2 flushed (512 MB write) between steps, max over ranks; value = E+grad
@@ -78,9 +80,22 @@ def heisenberg(Jz=1.0):
     return [H, H]
 
 
-WORKLOAD = dict(model="heisenberg", D=4, d=2, chi=64, iters=30, ad_iters=4)
-WORKLOAD_NAME = ("heisenberg D=4 d=2 chi=64: E+grad evaluation = init_ctm1 + 30 CTMRG iterations with the energy "
-                 "per iteration + pullback of 4 iterations and the energy")
+WORKLOADS = {
+    # the headline configuration: Heisenberg D=4 chi=64, 30 CTMRG iterations
+    "d4chi64": dict(model="heisenberg", D=4, d=2, chi=64, iters=30, ad_iters=4),
+    # the larger configuration (enlarged corners 2500 x 2500)
+    "d5chi100": dict(model="heisenberg", D=5, d=2, chi=100, iters=30, ad_iters=4),
+}
+WORKLOAD = WORKLOADS["d4chi64"]
+
+
+def workload_name(w):
+    return ("heisenberg D=%d d=%d chi=%d: E+grad evaluation = init_ctm1 + %d CTMRG iterations with the energy "
+            "per iteration + pullback of %d iterations and the energy" % (w["D"], w["d"], w["chi"], w["iters"],
+                                                                          w["ad_iters"]))
+
+
+WORKLOAD_NAME = workload_name(WORKLOAD)
 
 
 def workload_cfg(pkg, chi, iters, ad_iters):
@@ -284,6 +299,16 @@ def run_ours(args):
             return float(tt.item())
         return t
 
+    if args.forward_only > 0:
+        cfg.update(min_iter=args.forward_only, max_iter=args.forward_only)
+        tsf = pkg.CTMTensors(A, cfg, engine=eng)
+        tsf, info = pkg.run_ctm(tsf, conv_fun="energy", H=H)
+        if rank == 0:
+            print(json.dumps({"forward_only": args.forward_only, "workload": WORKLOAD_NAME,
+                              "energy": info["log"][-1]["obj"].real}))
+        tsf.close()
+        return 0
+
     ts = pkg.CTMTensors(A, cfg, engine=eng)
 
     def forward_step():
@@ -403,7 +428,13 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=12.0)
     ap.add_argument("--ref-budget", type=float, default=8.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="d4chi64", choices=sorted(WORKLOADS))
+    ap.add_argument("--forward-only", type=int, default=0, metavar="ITERS",
+                    help="profiling aid: run ITERS forward CTMRG iterations of the workload once, no timing")
     args = ap.parse_args()
+    global WORKLOAD, WORKLOAD_NAME
+    WORKLOAD = WORKLOADS[args.workload]
+    WORKLOAD_NAME = workload_name(WORKLOAD)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

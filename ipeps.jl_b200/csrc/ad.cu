@@ -531,6 +531,12 @@ struct IterCk {
 double energy_grad(Env& e, const Tensor& Hh, const Tensor& Hv, int ad_iters, Tensor* gA) {
   Ctx& c = *e.ctx;
   IPEPS_CHECK(e.dt == DType::F64 && !e.nested, "energy_grad: real single-site A only");
+  // The pullback runs in FP64 in both forms.  Recomputing the enlarged corners
+  // with 3xTF32 contractions inside the backward perturbs them at ~1e-7
+  // relative, and the truncated-SVD adjoint amplifies that through its
+  // 1/(s_i^2 - s_j^2) terms to gradient errors of a few 1e-6; the mixed form
+  // gains its speed in the convergence iterations before this call.
+  Fp64Scope fp64_all(c);
   // forward: ad_iters iterations with checkpoints of C/T and the projector factors
   std::vector<IterCk> ck;
   {
@@ -560,6 +566,7 @@ double energy_grad(Env& e, const Tensor& Hh, const Tensor& Hv, int ad_iters, Ten
   Tensor gAcc, gAdc;
   double Ere = 0;
   {
+    Fp64Scope fp64(c);  // the energy and its seed in FP64 in both forms
     Tape tp(c);
     ADPolicy p{tp};
     AV C[4], E[4];

@@ -288,6 +288,7 @@ std::vector<Traces> dm_traces(Ctx& c, const std::vector<std::pair<Tensor, Tensor
 
 // evaluation.jl:15-29 with get_dms (only_gs) evaluation.jl:124-156
 void gs_energy(Env& e, const Tensor& Hh, const Tensor& Hv, std::complex<double>* E, std::complex<double>* Na) {
+  Fp64Scope fp64(*e.ctx);
   Ctx& c = *e.ctx;
   NTPolicy p{c};
   NT C1(e.Cs[0]), C2(e.Cs[1]), C3(e.Cs[2]), C4(e.Cs[3]);
@@ -303,6 +304,7 @@ void gs_energy(Env& e, const Tensor& Hh, const Tensor& Hv, std::complex<double>*
 
 // evaluation.jl:31-45 (get_dms with only_gs = false)
 double es_energy(Env& e, const Tensor& Hh, const Tensor& Hv) {
+  Fp64Scope fp64(*e.ctx);
   Ctx& c = *e.ctx;
   IPEPS_CHECK(e.nested, "es_energy: no B set");
   NTPolicy p{c};
@@ -341,6 +343,7 @@ static std::complex<double> scalar_of(Ctx& c, const Tensor& t) {
 
 // ndm_Ad of get_tangent_basis (optim_es.jl:247-251): get_single_dm contracted with Ad
 Tensor single_dm_Ad(Env& e) {
+  Fp64Scope fp64(*e.ctx);
   Ctx& c = *e.ctx;
   NTPolicy p{c};
   NT n_dm = get_single_dm(p, NT(e.Cs[0]), NT(e.Cs[1]), NT(e.Cs[2]), NT(e.Cs[3]), NT(e.Es[0]), NT(e.Es[1]),
@@ -350,6 +353,7 @@ Tensor single_dm_Ad(Env& e) {
 
 // evaluation.jl:47-59
 std::complex<double> gs_norm(Env& e) {
+  Fp64Scope fp64(*e.ctx);
   Ctx& c = *e.ctx;
   NTPolicy p{c};
   NT n_dm = get_single_dm(p, NT(e.Cs[0]), NT(e.Cs[1]), NT(e.Cs[2]), NT(e.Cs[3]), NT(e.Es[0]), NT(e.Es[1]),
@@ -361,6 +365,7 @@ std::complex<double> gs_norm(Env& e) {
 
 // evaluation.jl:61-77
 std::complex<double> all_norm(Env& e, Tensor* envB) {
+  Fp64Scope fp64(*e.ctx);
   Ctx& c = *e.ctx;
   IPEPS_CHECK(e.nested, "all_norm: no B set");
   NTPolicy p{c};

@@ -80,6 +80,18 @@ struct Ctx {
 
 // Brackets the launches of one kernel family with CUDA events on the
 // context stream while profiling is enabled.
+// FP64 contractions for the lifetime of the scope, whatever the context's
+// precision: the observables (energies, norms, density matrices) are
+// evaluated in FP64 in both forms.
+struct Fp64Scope {
+  Ctx& c;
+  int prev;
+  explicit Fp64Scope(Ctx& cc) : c(cc), prev(cc.precision) { c.precision = kPrecFP64; }
+  ~Fp64Scope() { c.precision = prev; }
+  Fp64Scope(const Fp64Scope&) = delete;
+  Fp64Scope& operator=(const Fp64Scope&) = delete;
+};
+
 struct ProfScope {
   Ctx& c;
   int fam;

@@ -197,6 +197,7 @@ NAV leaf_nav(Tape& tp, const std::array<Tensor, 4>& comps) {
 
 double es_energy_grad(Env& e, const Tensor& Hh, const Tensor& Hv, int ad_iters, Tensor* gB) {
   Ctx& c = *e.ctx;
+  Fp64Scope fp64_all(c);  // the pullback in FP64 in both forms, as in energy_grad
   IPEPS_CHECK(e.nested && e.dt == DType::F64, "es_energy_grad: nested environment over a real A expected");
   auto slots = [&](std::array<std::array<Tensor, 4>, 4>& C, std::array<std::array<Tensor, 4>, 4>& E) {
     for (int s = 0; s < 4; ++s) {
@@ -237,6 +238,7 @@ double es_energy_grad(Env& e, const Tensor& Hh, const Tensor& Hv, int ad_iters, 
   };
   // get_es_energy on a tape (evaluation.jl:31-45): real part of component 4
   {
+    Fp64Scope fp64(c);  // the energy and its seed in FP64 in both forms
     Tape tp(c);
     NADPolicy p{tp};
     std::array<std::array<Tensor, 4>, 4> Cn, En;
