@@ -21,12 +21,14 @@ void jacobi_svd(Ctx& c, double* X, int m, int k, int64_t ldx, double* J, int64_t
 // diagonal when shift_factor > 0; a pivot at or below 1e-32 trace(G) gives
 // R[j][j] = 1 and a zero row.  Requires chol_fits(k).
 bool chol_fits(int k);
-void chol_blocked(Ctx& c, double* G, int k, int64_t ldg, double shift_factor);
+// Rrow (optional, k(k+1)/2 doubles, 16-byte aligned): R packed row by row, for trsm_right_upper.
+void chol_blocked(Ctx& c, double* G, int k, int64_t ldg, double shift_factor, double* Rrow = nullptr);
 // Q = Y R^-1 (Y: N x k, R: k x k upper triangular), one warp per row of Y.
 // Requires trsm_fits(k).
 bool trsm_fits(int k);
+// Rrow (optional): the same R packed row by row as written by chol_blocked.
 void trsm_right_upper(Ctx& c, const double* Y, int64_t ldy, int64_t N, int k, const double* R, int64_t ldr,
-                      double* Q, int64_t ldq);
+                      double* Q, int64_t ldq, const double* Rrow = nullptr);
 // jacobi_svd with X held in shared memory and J formed from the logged
 // rotations when it fits; tol <= 0 means m * eps
 void jacobi_svd_auto(Ctx& c, double* X, int m, int k, int64_t ldx, double* J, int64_t ldj, double* S,

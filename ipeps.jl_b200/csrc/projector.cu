@@ -57,6 +57,7 @@ Tensor orth(Ctx& c, const Tensor& Y0, int passes, Tensor* Rout) {
   double* d_tr = reinterpret_cast<double*>(c.scal->p) + 8;
   const double u = 1.1102230246251565e-16;
   const bool blocked = chol_fits(k) && trsm_fits(k);
+  Tensor Rrow = blocked ? c.alloc(DType::F64, {int64_t(k) * (k + 1) / 2}) : Tensor();
   for (int pass = 0; pass < passes; ++pass) {
     // G = Y^T Y  (FP64 always: the Gram matrix is where precision is lost)
     gemm(c, DType::F64, 'T', 'N', k, k, N, cplx(1), Y.data(), N, Y.data(), N, cplx(0), G.data(), k, true);
@@ -64,8 +65,8 @@ Tensor orth(Ctx& c, const Tensor& Y0, int passes, Tensor* Rout) {
     const double sf = (pass == 0) ? 11.0 * (double(N) * k + double(k) * (k + 1)) * u : 0.0;
     Tensor Yn = c.alloc(DType::F64, {N, k});
     if (blocked) {
-      chol_blocked(c, G.f64(), k, k, sf);
-      trsm_right_upper(c, Y.f64(), N, N, k, G.f64(), k, Yn.f64(), N);
+      chol_blocked(c, G.f64(), k, k, sf, Rrow.f64());
+      trsm_right_upper(c, Y.f64(), N, N, k, G.f64(), k, Yn.f64(), N, Rrow.f64());
     } else {
       if (pass == 0) {
         trace(c, G.f64(), k, k, d_tr);

@@ -23,6 +23,8 @@ constexpr int kCholThreads = 256;
 constexpr size_t kSmemMax = 226 * 1024;
 
 __device__ __forceinline__ int pku(int i, int j) { return ((j * (j + 1)) >> 1) + i; }  // packed upper, i <= j
+// row-major packed upper triangle: row j (columns j..k-1) starts at rowoff(j)
+__device__ __forceinline__ int rowoff(int j, int k) { return j * k - ((j * (j - 1)) >> 1); }
 
 size_t chol_smem_doubles(int k) {
   const size_t npk = (size_t(k) * (k + 1) / 2 + 1) & ~size_t(1);  // even: W below is 16-byte aligned
@@ -33,9 +35,11 @@ size_t chol_smem_doubles(int k) {
 // symmetric positive semi-definite; shift_factor > 0 first adds
 // shift_factor * trace(G) to the diagonal (shifted CholeskyQR).  A pivot at or
 // below 1e-32 * trace leaves R[j][j] = 1 and row j zero, so R stays
-// invertible.  On exit G holds R (strict lower triangle zeroed).
+// invertible.  On exit G holds R (strict lower triangle zeroed) and, when
+// Rrow is given, Rrow holds R's upper triangle packed row by row (the layout
+// the row-parallel triangular solve stages with contiguous copies).
 __global__ void __launch_bounds__(kCholThreads) chol_blocked_kernel(double* G, int k, int64_t ldg,
-                                                                    double shift_factor) {
+                                                                    double shift_factor, double* Rrow) {
   extern __shared__ __align__(16) double sm[];
   const int npk = ((k * (k + 1)) / 2 + 1) & ~1;
   double* P = sm;                                     // packed upper triangle
@@ -192,10 +196,10 @@ __global__ void __launch_bounds__(kCholThreads) chol_blocked_kernel(double* G, i
   __syncthreads();
   for (int j = warp; j < k; j += nw)
     for (int i = lane; i < k; i += 32) G[i + int64_t(j) * ldg] = (i <= j) ? P[pku(i, j)] : 0.0;
+  if (Rrow)
+    for (int i = warp; i < k; i += nw)
+      for (int jj = lane; jj < k - i; jj += 32) Rrow[rowoff(i, k) + jj] = P[pku(i, i + jj)];
 }
-
-// row-major packed upper triangle: row j (columns j..k-1) starts at rowoff(j)
-__device__ __forceinline__ int rowoff(int j, int k) { return j * k - ((j * (j - 1)) >> 1); }
 
 constexpr int kTrsmRows = 8;  // rows of Y per CTA, one warp each
 
@@ -203,8 +207,8 @@ constexpr int kTrsmRows = 8;  // rows of Y per CTA, one warp each
 // forward substitution, x_j = (y_j - sum_{l<j} x_l R[l][j]) / R[j][j].
 template <int NS>
 __global__ void __launch_bounds__(kTrsmRows * 32) trsm_rows_kernel(const double* Y, int64_t ldy, int64_t N, int k,
-                                                                  const double* R, int64_t ldr, double* Q,
-                                                                  int64_t ldq) {
+                                                                  const double* R, int64_t ldr, const double* Rrow,
+                                                                  double* Q, int64_t ldq) {
   extern __shared__ __align__(16) double sm[];
   const int kp = k | 1;
   double* Rs = sm;                       // k(k+1)/2, row-major packed
@@ -213,9 +217,20 @@ __global__ void __launch_bounds__(kTrsmRows * 32) trsm_rows_kernel(const double*
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   constexpr int nthr = kTrsmRows * 32;
   const int64_t i0 = int64_t(blockIdx.x) * kTrsmRows;
-  for (int l = warp; l < k; l += kTrsmRows)
-    for (int j = lane; j <= l; j += 32) Rs[rowoff(j, k) + (l - j)] = R[j + int64_t(l) * ldr];
-  for (int j = tid; j < k; j += nthr) rinv[j] = 1.0 / R[j + int64_t(j) * ldr];
+  const int npk = (k * (k + 1)) / 2;
+  if (Rrow) {
+    // R already packed row by row: contiguous 16-byte copies (both bases are 16-byte aligned)
+    const double2* src = reinterpret_cast<const double2*>(Rrow);
+    double2* dst = reinterpret_cast<double2*>(Rs);
+    for (int t = tid; t < npk / 2; t += nthr) dst[t] = src[t];
+    if ((npk & 1) && tid == 0) Rs[npk - 1] = Rrow[npk - 1];
+    __syncthreads();
+    for (int j = tid; j < k; j += nthr) rinv[j] = 1.0 / Rs[rowoff(j, k)];
+  } else {
+    for (int l = warp; l < k; l += kTrsmRows)
+      for (int j = lane; j <= l; j += 32) Rs[rowoff(j, k) + (l - j)] = R[j + int64_t(l) * ldr];
+    for (int j = tid; j < k; j += nthr) rinv[j] = 1.0 / R[j + int64_t(j) * ldr];
+  }
   for (int t = tid; t < kTrsmRows * k; t += nthr) {
     const int r = t % kTrsmRows, l = t / kTrsmRows;
     Yt[r * kp + l] = (i0 + r < N) ? Y[(i0 + r) + int64_t(l) * ldy] : 0.0;
@@ -474,15 +489,15 @@ void launch_jacobi(Ctx& c, double* X, int m, int k, int64_t ldx, double2* rot, i
 }
 
 template <int NS>
-void launch_trsm(Ctx& c, const double* Y, int64_t ldy, int64_t N, int k, const double* R, int64_t ldr, double* Q,
-                 int64_t ldq) {
+void launch_trsm(Ctx& c, const double* Y, int64_t ldy, int64_t N, int k, const double* R, int64_t ldr,
+                 const double* Rrow, double* Q, int64_t ldq) {
   const size_t smem = trsm_smem_bytes(k);
   if (!g_trsm_attr[NS]) {
     IPEPS_CUDA(cudaFuncSetAttribute(trsm_rows_kernel<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemMax)));
     g_trsm_attr[NS] = true;
   }
   const unsigned grid = unsigned((N + kTrsmRows - 1) / kTrsmRows);
-  trsm_rows_kernel<NS><<<grid, kTrsmRows * 32, smem, c.stream>>>(Y, ldy, N, k, R, ldr, Q, ldq);
+  trsm_rows_kernel<NS><<<grid, kTrsmRows * 32, smem, c.stream>>>(Y, ldy, N, k, R, ldr, Rrow, Q, ldq);
   IPEPS_LAUNCH_CHECK();
 }
 
@@ -490,14 +505,14 @@ void launch_trsm(Ctx& c, const double* Y, int64_t ldy, int64_t N, int k, const d
 
 bool chol_fits(int k) { return k >= 1 && chol_smem_doubles(k) * 8 <= kSmemMax; }
 
-void chol_blocked(Ctx& c, double* G, int k, int64_t ldg, double shift_factor) {
+void chol_blocked(Ctx& c, double* G, int k, int64_t ldg, double shift_factor, double* Rrow) {
   IPEPS_CHECK(chol_fits(k), "chol_blocked: k too large for shared memory");
   if (!g_chol_attr) {
     IPEPS_CUDA(cudaFuncSetAttribute(chol_blocked_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemMax)));
     g_chol_attr = true;
   }
   ProfScope ps(c, KFam::SmallLinalg);
-  chol_blocked_kernel<<<1, kCholThreads, chol_smem_doubles(k) * 8, c.stream>>>(G, k, ldg, shift_factor);
+  chol_blocked_kernel<<<1, kCholThreads, chol_smem_doubles(k) * 8, c.stream>>>(G, k, ldg, shift_factor, Rrow);
   IPEPS_LAUNCH_CHECK();
   c.count(KFam::SmallLinalg, double(k) * k * k / 3.0);
 }
@@ -505,19 +520,19 @@ void chol_blocked(Ctx& c, double* G, int k, int64_t ldg, double shift_factor) {
 bool trsm_fits(int k) { return k >= 1 && k <= 256 && trsm_smem_bytes(k) <= kSmemMax; }
 
 void trsm_right_upper(Ctx& c, const double* Y, int64_t ldy, int64_t N, int k, const double* R, int64_t ldr, double* Q,
-                      int64_t ldq) {
+                      int64_t ldq, const double* Rrow) {
   IPEPS_CHECK(trsm_fits(k), "trsm_right_upper: k too large for shared memory");
   if (N == 0) return;
   ProfScope ps(c, KFam::SmallLinalg);
   switch ((k + 31) / 32) {
-    case 1: launch_trsm<1>(c, Y, ldy, N, k, R, ldr, Q, ldq); break;
-    case 2: launch_trsm<2>(c, Y, ldy, N, k, R, ldr, Q, ldq); break;
-    case 3: launch_trsm<3>(c, Y, ldy, N, k, R, ldr, Q, ldq); break;
-    case 4: launch_trsm<4>(c, Y, ldy, N, k, R, ldr, Q, ldq); break;
-    case 5: launch_trsm<5>(c, Y, ldy, N, k, R, ldr, Q, ldq); break;
-    case 6: launch_trsm<6>(c, Y, ldy, N, k, R, ldr, Q, ldq); break;
-    case 7: launch_trsm<7>(c, Y, ldy, N, k, R, ldr, Q, ldq); break;
-    default: launch_trsm<8>(c, Y, ldy, N, k, R, ldr, Q, ldq); break;
+    case 1: launch_trsm<1>(c, Y, ldy, N, k, R, ldr, Rrow, Q, ldq); break;
+    case 2: launch_trsm<2>(c, Y, ldy, N, k, R, ldr, Rrow, Q, ldq); break;
+    case 3: launch_trsm<3>(c, Y, ldy, N, k, R, ldr, Rrow, Q, ldq); break;
+    case 4: launch_trsm<4>(c, Y, ldy, N, k, R, ldr, Rrow, Q, ldq); break;
+    case 5: launch_trsm<5>(c, Y, ldy, N, k, R, ldr, Rrow, Q, ldq); break;
+    case 6: launch_trsm<6>(c, Y, ldy, N, k, R, ldr, Rrow, Q, ldq); break;
+    case 7: launch_trsm<7>(c, Y, ldy, N, k, R, ldr, Rrow, Q, ldq); break;
+    default: launch_trsm<8>(c, Y, ldy, N, k, R, ldr, Rrow, Q, ldq); break;
   }
   c.count(KFam::SmallLinalg, double(N) * k * k);
 }

@@ -148,26 +148,77 @@ def evaluate_es(effH: np.ndarray, effN: np.ndarray, nrmB_cut: float = 1e-3):
     return np.sort(w.real)
 
 
+def es_column(px: float, py: float, ts: host.CTMTensors, H, basis: np.ndarray, i: int, C=None):
+    """One basis vector of optim_es (optim_es.jl:127-153): a nested
+    environment started from the ground-state C/T, the pullback w.r.t. B
+    (get_es_grad), projected on the basis: (effH[:, i], effN[:, i])."""
+    C = C if C is not None else [ts.get_CT(k) for k in range(1, 5)]
+    t = host.CTMTensors(ts.A, dict(ts.Params), engine=ts.engine, init=False)
+    try:
+        for k in range(4):
+            t.set_CT(k + 1, *C[k])
+        t.Params["px"], t.Params["py"] = px * math.pi, py * math.pi
+        gH, gN = host.get_es_grad(t, H, basis[:, i])
+    finally:
+        t.close()
+    return basis.conj().T @ gH / 2, basis.conj().T @ gN
+
+
 def optim_es(px: float, py: float, ts: host.CTMTensors, H, basis: np.ndarray,
              indices: Optional[List[int]] = None):
     """optim_es (optim_es.jl:91-165) for one momentum (px, py in units of pi).
 
     ts: normalised ground-state environment (copied per basis vector from its
     C/T), H: Hamiltonian with E0/2 subtracted, basis: (D^4 d, nb) complex.
-    indices: which basis columns to compute (all by default; a rank of a
-    multi-GPU job takes its share).  Returns (effH, effN) columns for those
-    indices (others zero)."""
+    indices: which basis columns to compute (all by default).  Returns (effH,
+    effN) with those columns filled (others zero)."""
     nb = basis.shape[1]
     effH = np.zeros((nb, nb), dtype=np.complex128)
     effN = np.zeros((nb, nb), dtype=np.complex128)
     C = [ts.get_CT(k) for k in range(1, 5)]
     for i in (range(nb) if indices is None else indices):
-        t = host.CTMTensors(ts.A, dict(ts.Params), engine=ts.engine, init=False)
-        for k in range(4):
-            t.set_CT(k + 1, *C[k])
-        t.Params["px"], t.Params["py"] = px * math.pi, py * math.pi
-        gH, gN = host.get_es_grad(t, H, basis[:, i])
-        effH[:, i] = basis.conj().T @ gH / 2
-        effN[:, i] = basis.conj().T @ gN
-        t.close()
+        effH[:, i], effN[:, i] = es_column(px, py, ts, H, basis, i, C)
+    return effH, effN
+
+
+def shard_indices(n: int, rank: int, world: int) -> List[int]:
+    """Basis columns of one rank: i = rank, rank + world, ... (round robin, so
+    that the ranks' shares differ by at most one column)."""
+    return list(range(rank, n, world))
+
+
+def optim_es_sharded(px: float, py: float, ts: Optional[host.CTMTensors], H, basis: np.ndarray, group=None,
+                     column_fn=None):
+    """optim_es over the ranks of a torch.distributed job (one process per GPU).
+
+    The basis vectors of one momentum are independent units (each a nested
+    CTMRG + pullback); rank r computes columns shard_indices(nb, r, world) and
+    one all-reduce (sum; the other ranks' columns are zero) gives every rank
+    the full effH and effN (nb x nb complex, ~0.4 MB each at nb = 161).  The
+    collective runs on the process group's backend (NCCL on GPUs, gloo on CPU).
+    column_fn(i) -> (effH[:, i], effN[:, i]) replaces the GPU computation
+    (es_column) when given.  Without an initialised process group this is
+    optim_es on one process."""
+    import torch
+    import torch.distributed as dist
+
+    nb = basis.shape[1]
+    dist_on = dist.is_available() and dist.is_initialized()
+    rank = dist.get_rank(group) if dist_on else 0
+    world = dist.get_world_size(group) if dist_on else 1
+    if column_fn is None:
+        C = [ts.get_CT(k) for k in range(1, 5)]
+        column_fn = lambda i: es_column(px, py, ts, H, basis, i, C)  # noqa: E731
+    effH = np.zeros((nb, nb), dtype=np.complex128)
+    effN = np.zeros((nb, nb), dtype=np.complex128)
+    for i in shard_indices(nb, rank, world):
+        effH[:, i], effN[:, i] = column_fn(i)
+    if world > 1:
+        backend = dist.get_backend(group)
+        dev = torch.device("cuda", torch.cuda.current_device()) if backend == "nccl" else torch.device("cpu")
+        buf = torch.from_numpy(np.stack([effH.real, effH.imag, effN.real, effN.imag])).to(dev)
+        dist.all_reduce(buf, op=dist.ReduceOp.SUM, group=group)
+        b = buf.cpu().numpy()
+        effH = b[0] + 1j * b[1]
+        effN = b[2] + 1j * b[3]
     return effH, effN
