@@ -48,6 +48,7 @@ extern "C" {
 
 typedef struct ipeps_ctx ipeps_ctx;
 typedef struct ipeps_env ipeps_env;
+typedef struct ipeps_mlp ipeps_mlp;
 
 typedef struct {
   uint64_t launches[8]; /* per kernel family: permute, gemm_f64, gemm_tf32x3, reduce, elementwise, small_linalg, jacobi */
@@ -167,6 +168,28 @@ IPEPS_API int ipeps_all_norm(ipeps_env* env, double* Nb, double* envB);
  * gives gN = envB as in get_es_grad, optim_es.jl:189). */
 IPEPS_API int ipeps_es_energy_grad(ipeps_env* env, const double* Hh, const double* Hv, int d2, int ad_iters,
                                    double* E, double* gB);
+
+/* ---- learned warm start (no counterpart in the reference: its CTMRG always starts
+ * from init_ctm1, ctm_tensor.jl:97-130).  A 3-layer perceptron n_in -> n_hidden ->
+ * n_hidden -> n_out (GELU) whose matrix products run on BF16 tensor-core GEMMs
+ * with FP32 accumulation; FP32 parameters, mean-squared error, Adam.  Host arrays
+ * are float32, column-major with the batch as rows (X: B x n_in, T/Y: B x n_out).
+ * Parameters are one flat vector W1 (n_in x n_hidden), b1, W2, b2, W3 (n_hidden x
+ * n_out), b3.  ipeps_gemm_bf16 exposes the GEMM on host buffers (C = alpha op(A)
+ * op(B) + beta C, operands rounded to BF16) for its parity test. */
+IPEPS_API int ipeps_gemm_bf16(ipeps_ctx* ctx, char opA, char opB, int64_t m, int64_t n, int64_t k, float alpha,
+                    const float* A, int64_t lda, const float* B, int64_t ldb, float beta, float* C, int64_t ldc);
+IPEPS_API int ipeps_mlp_create(ipeps_ctx* ctx, int n_in, int n_hidden, int n_out, int max_batch, uint64_t seed,
+                     ipeps_mlp** out);
+IPEPS_API int ipeps_mlp_destroy(ipeps_mlp* mlp);
+IPEPS_API int ipeps_mlp_num_params(ipeps_mlp* mlp, int64_t* n);
+IPEPS_API int ipeps_mlp_get_params(ipeps_mlp* mlp, float* params);
+IPEPS_API int ipeps_mlp_set_params(ipeps_mlp* mlp, const float* params);
+IPEPS_API int ipeps_mlp_forward(ipeps_mlp* mlp, const float* X, int B, float* Y);
+/* loss and gradient (flat, like the parameters) of the mean-squared error, no update */
+IPEPS_API int ipeps_mlp_grad(ipeps_mlp* mlp, const float* X, const float* T, int B, double* loss, float* grads);
+/* one Adam step (beta1 0.9, beta2 0.999, eps 1e-8) on the batch; *loss = the batch loss before the step */
+IPEPS_API int ipeps_mlp_train_step(ipeps_mlp* mlp, const float* X, const float* T, int B, float lr, double* loss);
 
 /* ---- allocation-free FP64 GEMM (no counterpart in the reference).
  * C = alpha*op(A)*op(B) + beta*C, column-major, op in {'N','T'}; A, B, C are

@@ -1,6 +1,7 @@
 // extern "C" boundary of libipeps_b200 (declared in include/ipeps_b200.h).
 #include "../../include/ipeps_b200.h"
 #include "ctm.cuh"
+#include "mlp.cuh"
 
 #include <cstring>
 
@@ -14,6 +15,11 @@ struct ipeps_ctx {
 struct ipeps_env {
   ipeps_ctx* owner = nullptr;
   ipeps::Env e;
+};
+
+struct ipeps_mlp {
+  ipeps_ctx* owner = nullptr;
+  std::unique_ptr<ipeps::Mlp> m;
 };
 
 namespace {
@@ -532,6 +538,133 @@ extern "C" int ipeps_single_dm_Ad(ipeps_env* env, double* out) {
     IPEPS_CHECK(out, "null output");
     Tensor t = ipeps::single_dm_Ad(env->e);
     download(*env->e.ctx, out, t);
+    return IPEPS_OK;
+  });
+}
+
+// ------------------------------------------------------------ warm-start network
+namespace {
+
+void h2d(ipeps::Ctx& c, void* d, const void* h, size_t bytes) {
+  IPEPS_CUDA(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, c.stream));
+}
+void d2h(ipeps::Ctx& c, void* h, const void* d, size_t bytes) {
+  IPEPS_CUDA(cudaMemcpyAsync(h, d, bytes, cudaMemcpyDeviceToHost, c.stream));
+}
+
+}  // namespace
+
+int ipeps_gemm_bf16(ipeps_ctx* ctx, char opA, char opB, int64_t m, int64_t n, int64_t k, float alpha, const float* A,
+                    int64_t lda, const float* B, int64_t ldb, float beta, float* C, int64_t ldc) {
+  return guarded(ctx, [&] {
+    IPEPS_CHECK(A && B && C && m > 0 && n > 0 && k > 0, "bad gemm_bf16 arguments");
+    auto& c = *ctx->c;
+    const int64_t acols = (opA == 'N') ? k : m, bcols = (opB == 'N') ? n : k;
+    IPEPS_CHECK(lda >= ((opA == 'N') ? m : k) && ldb >= ((opB == 'N') ? k : n) && ldc >= m, "bad leading dimension");
+    ipeps::DBuf dA(size_t(lda * acols) * 4, c.sh), dB(size_t(ldb * bcols) * 4, c.sh), dC(size_t(ldc * n) * 4, c.sh);
+    h2d(c, dA.p, A, dA.bytes);
+    h2d(c, dB.p, B, dB.bytes);
+    h2d(c, dC.p, C, dC.bytes);
+    ipeps::gemm_bf16(c, opA, opB, m, n, k, alpha, static_cast<float*>(dA.p), lda, static_cast<float*>(dB.p), ldb,
+                     beta, static_cast<float*>(dC.p), ldc);
+    d2h(c, C, dC.p, dC.bytes);
+    c.sync();
+    return IPEPS_OK;
+  });
+}
+
+int ipeps_mlp_create(ipeps_ctx* ctx, int n_in, int n_hidden, int n_out, int max_batch, uint64_t seed,
+                     ipeps_mlp** out) {
+  return guarded(ctx, [&] {
+    IPEPS_CHECK(out, "null output handle");
+    auto* h = new ipeps_mlp();
+    h->owner = ctx;
+    try {
+      h->m.reset(new ipeps::Mlp(*ctx->c, n_in, n_hidden, n_out, max_batch, seed));
+    } catch (...) {
+      delete h;
+      throw;
+    }
+    *out = h;
+    return IPEPS_OK;
+  });
+}
+
+int ipeps_mlp_destroy(ipeps_mlp* h) {
+  // touches no context: the network's buffers hold their own reference to the
+  // stream they are freed on (stream-ordered), so this is safe in any order
+  if (!h) return IPEPS_EINVAL;
+  delete h;
+  return IPEPS_OK;
+}
+
+int ipeps_mlp_num_params(ipeps_mlp* h, int64_t* n) {
+  if (!h || !n) return IPEPS_EINVAL;
+  *n = h->m->np;
+  return IPEPS_OK;
+}
+
+int ipeps_mlp_get_params(ipeps_mlp* h, float* p) {
+  if (!h) return IPEPS_EINVAL;
+  return guarded(h->owner, [&] {
+    IPEPS_CHECK(p, "null buffer");
+    d2h(h->m->c, p, h->m->params->p, size_t(h->m->np) * 4);
+    h->m->c.sync();
+    return IPEPS_OK;
+  });
+}
+
+int ipeps_mlp_set_params(ipeps_mlp* h, const float* p) {
+  if (!h) return IPEPS_EINVAL;
+  return guarded(h->owner, [&] {
+    IPEPS_CHECK(p, "null buffer");
+    h2d(h->m->c, h->m->params->p, p, size_t(h->m->np) * 4);
+    return IPEPS_OK;
+  });
+}
+
+int ipeps_mlp_forward(ipeps_mlp* h, const float* X, int B, float* Y) {
+  if (!h) return IPEPS_EINVAL;
+  return guarded(h->owner, [&] {
+    auto& m = *h->m;
+    IPEPS_CHECK(X && Y && B > 0 && B <= m.cap, "bad mlp_forward arguments");
+    h2d(m.c, m.X->p, X, size_t(B) * m.n_in * 4);
+    m.forward(B);
+    d2h(m.c, Y, m.Y->p, size_t(B) * m.n_out * 4);
+    m.c.sync();
+    return IPEPS_OK;
+  });
+}
+
+int ipeps_mlp_grad(ipeps_mlp* h, const float* X, const float* T, int B, double* loss, float* grads) {
+  if (!h) return IPEPS_EINVAL;
+  return guarded(h->owner, [&] {
+    auto& m = *h->m;
+    IPEPS_CHECK(X && T && B > 0 && B <= m.cap, "bad mlp_grad arguments");
+    h2d(m.c, m.X->p, X, size_t(B) * m.n_in * 4);
+    h2d(m.c, m.T->p, T, size_t(B) * m.n_out * 4);
+    m.forward(B);
+    const double l = m.loss_and_grad(B);
+    if (loss) *loss = l;
+    if (grads) {
+      d2h(m.c, grads, m.grads->p, size_t(m.np) * 4);
+      m.c.sync();
+    }
+    return IPEPS_OK;
+  });
+}
+
+int ipeps_mlp_train_step(ipeps_mlp* h, const float* X, const float* T, int B, float lr, double* loss) {
+  if (!h) return IPEPS_EINVAL;
+  return guarded(h->owner, [&] {
+    auto& m = *h->m;
+    IPEPS_CHECK(X && T && B > 0 && B <= m.cap && lr > 0, "bad mlp_train_step arguments");
+    h2d(m.c, m.X->p, X, size_t(B) * m.n_in * 4);
+    h2d(m.c, m.T->p, T, size_t(B) * m.n_out * 4);
+    m.forward(B);
+    const double l = m.loss_and_grad(B);
+    m.adam(lr);
+    if (loss) *loss = l;
     return IPEPS_OK;
   });
 }

@@ -128,6 +128,9 @@ void gemm_f64(Ctx& c, DType dt, char opA, char opB, int64_t m, int64_t n, int64_
               cuDoubleComplex alpha, const void* A, int64_t lda, const void* B, int64_t ldb,
               cuDoubleComplex beta, void* C, int64_t ldc);
 // 3xTF32 tcgen05 GEMM for real operands (FP32-accumulated split products)
+// BF16 operands (rounded from FP32 while staged), FP32 accumulation and result; op in {N, T}
+void gemm_bf16(Ctx& c, char opA, char opB, int64_t m, int64_t n, int64_t k, float alpha, const float* A, int64_t lda,
+               const float* B, int64_t ldb, float beta, float* C, int64_t ldc);
 void gemm_tf32x3(Ctx& c, char opA, char opB, int64_t m, int64_t n, int64_t k, double alpha,
                  const double* A, int64_t lda, const double* B, int64_t ldb, double beta, double* C,
                  int64_t ldc);

@@ -17,7 +17,7 @@
 // fence.proxy.async; the MMA thread commits (tcgen05.commit) to empty[s] and,
 // after the last K-step, to the accumulator barrier.  Every wait is bounded:
 // on timeout the kernel records bit 8 in the status word and drains.
-#include "ctx.cuh"
+#include "umma.cuh"
 
 #include <algorithm>
 
@@ -30,47 +30,11 @@ constexpr int STAGE_BYTES = 4 * TILE_BYTES;        // A_hi, A_lo, B_hi, B_lo
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
 constexpr int NTHREADS = 160;
 constexpr uint32_t TMEM_COLS = 128;
-constexpr long long WAIT_LIMIT = 1LL << 22;
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
-}
-
-// bounded wait for the phase with the given parity; false on timeout
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-  for (long long i = 0; i < WAIT_LIMIT; ++i) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    if (ok) return true;
-  }
-  return false;
-}
 
 __device__ __forceinline__ uint32_t to_tf32(float x) {
   uint32_t r;
   asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
   return r;
-}
-
-// SW128 K-major UMMA shared-memory descriptor (LBO = 16 B, SBO = 1024 B,
-// descriptor version 1, layout type 2 = 128B swizzle)
-__device__ __forceinline__ uint64_t make_desc(uint32_t saddr) {
-  return uint64_t((saddr >> 4) & 0x3FFF) | (uint64_t(1) << 16) | (uint64_t(1024 >> 4) << 32) |
-         (uint64_t(1) << 46) | (uint64_t(2) << 61);
 }
 
 // instruction descriptor: D = F32, A = B = TF32, both K-major, M = 128, N = 128
@@ -83,16 +47,6 @@ __device__ __forceinline__ void mma_tf32(uint32_t tmem, uint64_t da, uint64_t db
       "setp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
       ::"r"(tmem), "l"(da), "l"(db), "r"(IDESC), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
-}
-
-__device__ __forceinline__ void mma_commit(uint32_t bar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
-               : "memory");
-}
-
-// byte offset of element (row r, k) in a 128 x 32 TF32 K-major SW128 tile
-__device__ __forceinline__ uint32_t sw128(int r, int chunk) {
-  return uint32_t((r >> 3) * 1024 + (r & 7) * 128 + ((chunk ^ (r & 7)) << 4));
 }
 
 struct Args {

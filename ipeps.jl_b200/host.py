@@ -41,7 +41,8 @@ EXPORTED = [
     "ipeps_ctm_log", "ipeps_energy", "ipeps_gs_norm", "ipeps_nested_set_B", "ipeps_es_energy",
     "ipeps_all_norm", "ipeps_tcon", "ipeps_projector", "ipeps_projector_c", "ipeps_ctx_stream", "ipeps_prof_enable",
     "ipeps_prof_query", "ipeps_energy_grad", "ipeps_env_set_mixed", "ipeps_es_energy_grad",
-    "ipeps_single_dm_Ad",
+    "ipeps_single_dm_Ad", "ipeps_gemm_bf16", "ipeps_mlp_create", "ipeps_mlp_destroy", "ipeps_mlp_num_params",
+    "ipeps_mlp_get_params", "ipeps_mlp_set_params", "ipeps_mlp_forward", "ipeps_mlp_grad", "ipeps_mlp_train_step",
 ]
 
 
@@ -82,6 +83,7 @@ def load_library(path: str = LIB_PATH) -> ct.CDLL:
     dp = ct.POINTER(ct.c_double)
     ip = ct.POINTER(ct.c_int)
     lp = ct.POINTER(ct.c_int64)
+    fp = ct.POINTER(ct.c_float)
     sig = {
         "ipeps_ctx_create": [I, ct.POINTER(P)],
         "ipeps_ctx_destroy": [P],
@@ -116,6 +118,16 @@ def load_library(path: str = LIB_PATH) -> ct.CDLL:
         "ipeps_env_set_mixed": [P, I, D],
         "ipeps_es_energy_grad": [P, dp, dp, I, I, dp, dp],
         "ipeps_single_dm_Ad": [P, dp],
+        "ipeps_gemm_bf16": [P, ct.c_char, ct.c_char, ct.c_int64, ct.c_int64, ct.c_int64, ct.c_float, fp,
+                            ct.c_int64, fp, ct.c_int64, ct.c_float, fp, ct.c_int64],
+        "ipeps_mlp_create": [P, I, I, I, I, U64, ct.POINTER(P)],
+        "ipeps_mlp_destroy": [P],
+        "ipeps_mlp_num_params": [P, lp],
+        "ipeps_mlp_get_params": [P, fp],
+        "ipeps_mlp_set_params": [P, fp],
+        "ipeps_mlp_forward": [P, fp, I, fp],
+        "ipeps_mlp_grad": [P, fp, fp, I, dp, fp],
+        "ipeps_mlp_train_step": [P, fp, fp, I, ct.c_float, dp],
     }
     for name, args in sig.items():
         f = getattr(lib, name)
@@ -544,3 +556,87 @@ def compute_gs_energy(A, H, cfg, engine: Optional[Engine] = None):
     ts, info = run_ctm(ts, conv_fun="energy", H=H)
     E, Na = get_gs_energy(ts, H)
     return (E, Na), ts, info
+
+
+# ------------------------------------------------------------ warm-start network
+def _fp(a: np.ndarray):
+    return a.ctypes.data_as(ct.POINTER(ct.c_float))
+
+
+def _f32(a) -> np.ndarray:
+    return np.asfortranarray(np.asarray(a, dtype=np.float32))
+
+
+def gemm_bf16(opA: str, opB: str, A, B, alpha: float = 1.0, beta: float = 0.0, C=None,
+              engine: Optional[Engine] = None) -> np.ndarray:
+    """C = alpha op(A) op(B) + beta C on the BF16 tensor-core GEMM (host buffers, float32)."""
+    eng = engine or default_engine()
+    A, B = _f32(A), _f32(B)
+    m = A.shape[0] if opA == "N" else A.shape[1]
+    k = A.shape[1] if opA == "N" else A.shape[0]
+    n = B.shape[1] if opB == "N" else B.shape[0]
+    C = np.zeros((m, n), dtype=np.float32, order="F") if C is None else _f32(C).copy(order="F")
+    eng.check(eng.lib.ipeps_gemm_bf16(eng.h, opA.encode(), opB.encode(), m, n, k, float(alpha), _fp(A), A.shape[0],
+                                      _fp(B), B.shape[0], float(beta), _fp(C), m))
+    return C
+
+
+class Mlp:
+    """The warm-start network on the device (ipeps_mlp_*): n_in -> n_hidden ->
+    n_hidden -> n_out with GELU, BF16 tensor-core GEMMs, FP32 parameters, Adam."""
+
+    def __init__(self, n_in: int, n_hidden: int, n_out: int, max_batch: int = 256, seed: int = 0,
+                 engine: Optional[Engine] = None):
+        self.engine = engine or default_engine()
+        self.lib = self.engine.lib
+        self.n_in, self.n_hidden, self.n_out, self.max_batch = n_in, n_hidden, n_out, max_batch
+        h = ct.c_void_p()
+        self.engine.check(self.lib.ipeps_mlp_create(self.engine.h, n_in, n_hidden, n_out, max_batch, seed,
+                                                    ct.byref(h)))
+        self.h = h
+        n = ct.c_int64(0)
+        self.lib.ipeps_mlp_num_params(self.h, ct.byref(n))
+        self.num_params = n.value
+
+    def params(self) -> np.ndarray:
+        p = np.empty(self.num_params, dtype=np.float32)
+        self.engine.check(self.lib.ipeps_mlp_get_params(self.h, _fp(p)))
+        return p
+
+    def set_params(self, p) -> None:
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        assert p.size == self.num_params
+        self.engine.check(self.lib.ipeps_mlp_set_params(self.h, _fp(p)))
+
+    def forward(self, X) -> np.ndarray:
+        X = _f32(X)
+        Y = np.empty((X.shape[0], self.n_out), dtype=np.float32, order="F")
+        self.engine.check(self.lib.ipeps_mlp_forward(self.h, _fp(X), X.shape[0], _fp(Y)))
+        return Y
+
+    def grad(self, X, T):
+        X, T = _f32(X), _f32(T)
+        g = np.empty(self.num_params, dtype=np.float32)
+        loss = ct.c_double(0)
+        self.engine.check(self.lib.ipeps_mlp_grad(self.h, _fp(X), _fp(T), X.shape[0], ct.byref(loss), _fp(g)))
+        return loss.value, g
+
+    def train_step(self, X, T, lr: float) -> float:
+        X, T = _f32(X), _f32(T)
+        loss = ct.c_double(0)
+        self.engine.check(self.lib.ipeps_mlp_train_step(self.h, _fp(X), _fp(T), X.shape[0], float(lr),
+                                                        ct.byref(loss)))
+        return loss.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            if getattr(self.engine, "h", None):  # a closed engine took the device state with it
+                self.lib.ipeps_mlp_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
