@@ -1,0 +1,228 @@
+"""Learned warm start for CTMRG (no counterpart in the reference, whose run_ctm
+always starts from init_ctm1, ctm_tensor.jl:97-130).
+
+A small network (host.Mlp: BF16 tensor-core GEMMs, FP32 parameters) maps the
+flattened iPEPS tensor A to a rank-r environment in a canonical gauge; CTMRG
+then iterates from that environment to rg_tol.  Plain CTMRG stays the judge
+and the fallback: a warm start that has not converged by max_iter is dropped
+and the run restarts from init_ctm1, so the converged energy is always the one
+plain CTMRG reaches.
+
+Canonical gauge.  With a one-site unit cell an environment has four bond
+gauges, one per boundary (top, right, bottom, left): both legs of the
+boundary's edge and one leg of each of its two corners carry it (an edge's two
+legs meet each other between neighbouring sites).  For converged (real)
+environments the orthogonal part is fixed here: C1 = U S V^T fixes the left
+(U) and top (V) gauges; the sign of singular pair a >= 1 is chosen so that the
+entry of largest modulus of E1[0, a, :, :] in that gauge is positive (flipping
+every pair at once is a trivial gauge, so pair 0 needs no rule); the right
+gauge makes V^T C2 Q_right lower triangular with a positive diagonal (an LQ
+factorisation), the bottom gauge does the same for U^T C4; C3 and the edges
+follow.  Truncating every bond to its leading r directions gives the
+network's target: r + 3 r^2 corner entries and 4 r^2 D^2 edge entries.
+
+The boundaries (which edge and corner legs share a gauge) are those of the
+reference's contractions (ctmrg.jl:122-252, evaluation.jl:124-248): top = E1
+with C1's second and C2's first leg, right = E2 with C2's second and C3's
+first, bottom = E3 with C3's second and C4's second, left = E4 with C1's first
+and C4's first.
+"""
+from __future__ import annotations
+
+import time
+from typing import Any, Dict, List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from . import host
+
+# boundary j (0 top, 1 right, 2 bottom, 3 left): edge j (both legs) and two corner legs (corner, leg), 0-based
+BOUNDARIES = [((0, 1), (1, 0)), ((1, 1), (2, 0)), ((2, 1), (3, 1)), ((0, 0), (3, 0))]
+
+
+def _apply_leg(E: np.ndarray, leg: int, Q: np.ndarray) -> np.ndarray:
+    """E with leg `leg` (0 or 1) contracted against Q (new index = column of Q)."""
+    if leg == 0:
+        return np.einsum("iabc,ij->jabc", E, Q)
+    return np.einsum("aibc,ij->ajbc", E, Q)
+
+
+def gauge_transform(Cs: Sequence[np.ndarray], Es: Sequence[np.ndarray], Qb: Sequence[np.ndarray]):
+    """Apply the orthogonal boundary gauges Qb[j] (new index = column of Q) to
+    every leg on boundary j."""
+    Cn = [np.array(C) for C in Cs]
+    En = [np.array(E) for E in Es]
+    for j, legs in enumerate(BOUNDARIES):
+        for k, l in legs:
+            Cn[k] = Qb[j].T @ Cn[k] if l == 0 else Cn[k] @ Qb[j]
+        En[j] = _apply_leg(_apply_leg(En[j], 0, Qb[j]), 1, Qb[j])
+    return Cn, En
+
+
+def _lq_gauge(M: np.ndarray) -> np.ndarray:
+    """Orthogonal Q with M Q lower triangular with a non-negative diagonal."""
+    Q, R = np.linalg.qr(M.T)
+    sgn = np.sign(np.diag(R))
+    sgn[sgn == 0] = 1.0
+    return Q * sgn
+
+
+def canonical(Cs: Sequence[np.ndarray], Es: Sequence[np.ndarray]):
+    """The environment in the canonical gauge (full rank)."""
+    Cs = [np.asarray(C, dtype=np.float64) for C in Cs]
+    Es = [np.asarray(E, dtype=np.float64) for E in Es]
+    U, s, Vt = np.linalg.svd(Cs[0])
+    V = Vt.T.copy()
+    E1 = _apply_leg(_apply_leg(Es[0], 0, V), 1, V)
+    for a in range(1, len(s)):
+        blk = E1[0, a]
+        if blk.flat[np.argmax(np.abs(blk))] < 0:
+            U[:, a] *= -1
+            V[:, a] *= -1
+    Qr = _lq_gauge(V.T @ Cs[1])
+    Qbot = _lq_gauge(U.T @ Cs[3])
+    return gauge_transform(Cs, Es, [V, Qr, Qbot, U])
+
+
+def gauge_fix(Cs: Sequence[np.ndarray], Es: Sequence[np.ndarray], r: Optional[int] = None) -> np.ndarray:
+    """Canonical-gauge vector of a real environment truncated to rank r:
+    [diag C1[:r], C2, C3, C4 (r x r, column-major), E1 .. E4 (r, r, D, D)]."""
+    Cn, En = canonical(Cs, Es)
+    r = r or min(C.shape[0] for C in Cn)
+    parts = [np.diag(Cn[0])[:r]] + [C[:r, :r].ravel(order="F") for C in Cn[1:]] + \
+        [E[:r, :r].ravel(order="F") for E in En]
+    return np.concatenate(parts)
+
+
+def unpack(vec: np.ndarray, r: int, D: int):
+    """(Cs, Es) of a rank-r environment in the canonical gauge from its vector."""
+    vec = np.asarray(vec, dtype=np.float64)
+    Cs = [np.diag(vec[:r])]
+    o = r
+    for _ in range(3):
+        Cs.append(np.asfortranarray(vec[o:o + r * r].reshape((r, r), order="F")))
+        o += r * r
+    n = r * r * D * D
+    Es = [np.asfortranarray(vec[o + j * n:o + (j + 1) * n].reshape((r, r, D, D), order="F")) for j in range(4)]
+    return Cs, Es
+
+
+def read_env(ts: host.CTMTensors):
+    Cs, Es = [], []
+    for k in range(1, 5):
+        C, E = ts.get_CT(k)
+        Cs.append(np.asarray(C))
+        Es.append(np.asarray(E))
+    return Cs, Es
+
+
+def converge_default(A, H, cfg: Dict[str, Any], engine=None):
+    """Plain CTMRG from init_ctm1 with the energy criterion (the judge)."""
+    ts = host.CTMTensors(A, cfg, engine=engine)
+    ts, info = host.run_ctm(ts, conv_fun="energy", H=H)
+    return ts, info
+
+
+class WarmStart:
+    """Network + standardisation of inputs and targets for one (D, d, r)."""
+
+    def __init__(self, D: int, d: int, r: int = 8, hidden: int = 512, max_batch: int = 256, seed: int = 0,
+                 engine=None):
+        self.D, self.d, self.r = D, d, r
+        self.n_in = D ** 4 * d
+        self.n_out = r + 3 * r * r + 4 * r * r * D * D
+        self.engine = engine or host.default_engine()
+        self.net = host.Mlp(self.n_in, hidden, self.n_out, max_batch=max_batch, seed=seed, engine=self.engine)
+        self.max_batch = max_batch
+        self.xm = self.xs = self.ym = self.ys = None
+
+    def _x(self, As) -> np.ndarray:
+        return np.stack([np.asarray(A, dtype=np.float64).ravel(order="F") for A in As])
+
+    def fit(self, As, targets: np.ndarray, epochs: int = 400, lr: float = 1e-3, seed: int = 0) -> List[float]:
+        X = self._x(As)
+        Y = np.asarray(targets, dtype=np.float64)
+        self.xm, self.xs = X.mean(0), X.std(0) + 1e-8
+        self.ym, self.ys = Y.mean(0), Y.std(0) + 1e-8
+        Xn = ((X - self.xm) / self.xs).astype(np.float32)
+        Yn = ((Y - self.ym) / self.ys).astype(np.float32)
+        rng = np.random.default_rng(seed)
+        losses = []
+        n = len(X)
+        for _ in range(epochs):
+            perm = rng.permutation(n)
+            ep = []
+            for b0 in range(0, n, self.max_batch):
+                idx = perm[b0:b0 + self.max_batch]
+                ep.append(self.net.train_step(Xn[idx], Yn[idx], lr))
+            losses.append(float(np.mean(ep)))
+        return losses
+
+    def predict(self, As) -> np.ndarray:
+        Xn = ((self._x(As) - self.xm) / self.xs).astype(np.float32)
+        out = []
+        for b0 in range(0, len(Xn), self.max_batch):
+            out.append(self.net.forward(Xn[b0:b0 + self.max_batch]))
+        return np.concatenate(out).astype(np.float64) * self.ys + self.ym
+
+    def converge(self, A, H, cfg: Dict[str, Any], warm_max_iter: Optional[int] = None):
+        """CTMRG from the predicted environment; falls back to init_ctm1 when it
+        has not converged within warm_max_iter iterations (default max_iter).
+        Returns (ts, info, used_warm_start, iterations in total)."""
+        Cs, Es = unpack(self.predict([A])[0], self.r, self.D)
+        wcfg = dict(cfg)
+        if warm_max_iter is not None:
+            wcfg["max_iter"] = int(warm_max_iter)
+        ts = host.CTMTensors(A, wcfg, engine=self.engine, init=False)
+        for k in range(4):
+            ts.set_CT(k + 1, Cs[k], Es[k])
+        ts, info = host.run_ctm(ts, conv_fun="energy", H=H)
+        if info["converged"]:
+            return ts, info, True, len(info["log"])
+        spent = len(info["log"])
+        ts.close()
+        ts, info = converge_default(A, H, cfg, engine=self.engine)
+        return ts, info, False, spent + len(info["log"])
+
+    def close(self):
+        self.net.close()
+
+
+def path_family(D: int, d: int, seeds: Sequence[int], n_points: int, scale: float = 0.3):
+    """A family of iPEPS tensors on straight paths A(t) = A0 + t (A1 - A0),
+    t in [0, 1], around near-product states (a product state plus `scale`
+    times a random tensor, so that CTMRG converges): one path per seed."""
+    out = []
+    for sd in seeds:
+        rng = np.random.default_rng(sd)
+        prod = np.zeros((D, D, D, D, d))
+        prod[0, 0, 0, 0, :] = rng.standard_normal(d)
+        A0 = prod + scale * rng.standard_normal(prod.shape)
+        A1 = prod + scale * rng.standard_normal(prod.shape)
+        for t in np.linspace(0.0, 1.0, n_points):
+            A = A0 + t * (A1 - A0)
+            out.append((sd, float(t), np.asfortranarray(A / np.abs(A).max())))
+    return out
+
+
+def evaluate(As, H, cfg: Dict[str, Any], ws: WarmStart, engine=None) -> Dict[str, Any]:
+    """Iterations and time to rg_tol from init_ctm1 and from the warm start, and
+    the converged energies of both (they must agree)."""
+    rows = []
+    for A in As:
+        t0 = time.time()
+        ts0, info0 = converge_default(A, H, cfg, engine=engine)
+        t1 = time.time()
+        E0 = host.get_gs_energy(ts0, H)[0].real
+        ts0.close()
+        t2 = time.time()
+        ts1, info1, used, iters = ws.converge(A, H, cfg)
+        t3 = time.time()
+        E1 = host.get_gs_energy(ts1, H)[0].real
+        ts1.close()
+        rows.append(dict(iters_default=len(info0["log"]), iters_warm=iters, used_warm=used, E_default=E0, E_warm=E1,
+                         s_default=t1 - t0, s_warm=t3 - t2, converged_default=info0.get("converged", True)))
+    return dict(rows=rows, mean_iters_default=float(np.mean([r["iters_default"] for r in rows])),
+                mean_iters_warm=float(np.mean([r["iters_warm"] for r in rows])),
+                max_dE=float(max(abs(r["E_default"] - r["E_warm"]) for r in rows)),
+                warm_used=sum(r["used_warm"] for r in rows), n=len(rows))
