@@ -72,14 +72,15 @@ __global__ void renorm_back_kernel(const double* dy, const double* x, int64_t n,
   }
 }
 
-// X[:, j] *= f(s[j]); mode 0: s, 1: 1/sqrt(s), 2: sqrt(s), 3: 1/s
+// X[:, j] *= f(s[j]); mode 0: s, 1: 1/sqrt(s), 2: sqrt(s), 3: 1/s.  The inverse
+// of a kept s of exactly 0 is taken as 0 (its projector column is zero).
 __global__ void colscale_kernel(double* X, int64_t ld, int64_t m, int ncols, const double* s, int mode) {
   const int64_t tot = m * ncols;
   for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < tot; t += int64_t(gridDim.x) * blockDim.x) {
     const int64_t i = t % m;
     const int j = int(t / m);
     const double v = s[j];
-    const double f = mode == 0 ? v : mode == 1 ? 1.0 / sqrt(v) : mode == 2 ? sqrt(v) : 1.0 / v;
+    const double f = mode == 0 ? v : mode == 2 ? sqrt(v) : v > 0.0 ? (mode == 1 ? 1.0 / sqrt(v) : 1.0 / v) : 0.0;
     X[i + j * ld] *= f;
   }
 }
@@ -90,7 +91,7 @@ __global__ void transpose_scale_kernel(const double* in, int n, int64_t N, const
   for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < tot; t += int64_t(gridDim.x) * blockDim.x) {
     const int64_t a = t % N;
     const int i = int(t / N);
-    out[a + i * N] = in[i + a * n] / sqrt(s[i]);
+    out[a + i * N] = s[i] > 0.0 ? in[i + a * n] / sqrt(s[i]) : 0.0;
   }
 }
 
@@ -106,7 +107,7 @@ __global__ void dS_kernel(int n, int64_t N, const double* dP1, const double* P1,
   if (dP2)
     for (int64_t j = lane; j < N; j += 32) acc = fma(dP2[i + j * n], P2[i + j * n], acc);
   acc = wsum(acc);
-  if (lane == 0) dS[i] = -0.5 * acc / s[i];
+  if (lane == 0) dS[i] = s[i] > 0.0 ? -0.5 * acc / s[i] : 0.0;
 }
 
 __device__ __forceinline__ double Fb(double x, double eta) { return x / (x * x + eta); }

@@ -196,7 +196,9 @@ __global__ void scale_cols_kernel(double* X, int64_t ldx, int64_t m, int ncols, 
   for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < tot; t += int64_t(gridDim.x) * blockDim.x) {
     int64_t i = t % m;
     int j = int(t / m);
-    double f = (mode == 1) ? 1.0 / sqrt(s[j]) : s[j];
+    // a kept s of exactly 0 (the degenerate-pair rule of the cutoff can keep one
+    // past the 1e-12 cutoff) gets a zero column instead of an infinite one
+    double f = (mode == 1) ? (s[j] > 0.0 ? 1.0 / sqrt(s[j]) : 0.0) : s[j];
     X[i + j * ldx] *= f;
   }
 }
@@ -205,7 +207,7 @@ __global__ void scale_rows_kernel(double* X, int64_t ldx, int64_t m, int64_t nco
   int64_t tot = m * ncols;
   for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < tot; t += int64_t(gridDim.x) * blockDim.x) {
     int64_t i = t % m, j = t / m;
-    double f = (mode == 1) ? 1.0 / sqrt(s[i]) : s[i];
+    double f = (mode == 1) ? (s[i] > 0.0 ? 1.0 / sqrt(s[i]) : 0.0) : s[i];
     X[i + j * ldx] *= f;
   }
 }

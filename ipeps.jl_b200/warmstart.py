@@ -9,23 +9,32 @@ and the run restarts from init_ctm1, so the converged energy is always the one
 plain CTMRG reaches.
 
 Canonical gauge.  With a one-site unit cell an environment has four bond
-gauges, one per boundary (top, right, bottom, left): both legs of the
-boundary's edge and one leg of each of its two corners carry it (an edge's two
-legs meet each other between neighbouring sites).  For converged (real)
-environments the orthogonal part is fixed here: C1 = U S V^T fixes the left
-(U) and top (V) gauges; the sign of singular pair a >= 1 is chosen so that the
-entry of largest modulus of E1[0, a, :, :] in that gauge is positive (flipping
-every pair at once is a trivial gauge, so pair 0 needs no rule); the right
-gauge makes V^T C2 Q_right lower triangular with a positive diagonal (an LQ
-factorisation), the bottom gauge does the same for U^T C4; C3 and the edges
-follow.  Truncating every bond to its leading r directions gives the
-network's target: r + 3 r^2 corner entries and 4 r^2 D^2 edge entries.
+gauges, one per boundary (top, right, bottom, left), each an invertible
+chi x chi matrix X: the boundary's edge E becomes X^-1 E X (its two legs meet
+each other between neighbouring sites) and the two corner legs on the
+boundary absorb X or X^-T, so every contraction is unchanged.  CTMRG's
+truncation (an SVD of the half-system matrix) is invariant only under the
+orthogonal part of that freedom: from an environment in another GL(chi) gauge
+it keeps a slightly different subspace and has to relax back (a fixed point
+re-gauged by a well-conditioned X needs about as many iterations as a cold
+start to get back to 1e-10 in the energy).  So the network's target keeps
+CTMRG's own gauge and fixes only the orthogonal part: C1 = U S V^T fixes the
+left (U) and top (V) gauges; the sign of singular pair a >= 1 makes the
+leading entry of E1[b, a, :, :] positive in that gauge, b < a the pair coupled
+most strongly to a (flipping every pair at once is a trivial gauge); the
+right gauge makes V^T C2 Q_right lower triangular with a positive diagonal
+(an LQ factorisation), the bottom gauge does the same for U^T C4; C3 and the
+edges follow.  "Leading" is the first entry in storage order whose modulus is
+within 1e-6 of the largest, so that exact ties of symmetric tensors break the
+same way.  Truncating every bond to its leading r directions gives the
+network's target: 4 r^2 corner entries and 4 r^2 D^2 edge entries.
 
-The boundaries (which edge and corner legs share a gauge) are those of the
-reference's contractions (ctmrg.jl:122-252, evaluation.jl:124-248): top = E1
-with C1's second and C2's first leg, right = E2 with C2's second and C3's
-first, bottom = E3 with C3's second and C4's second, left = E4 with C1's first
-and C4's first.
+Which corner legs face which edge legs follows the reference's contractions
+(ctmrg.jl:122-252, evaluation.jl:124-248): E1 (top) leg 0 faces C1 leg 1 and
+leg 1 faces C2 leg 0; E2 (right) leg 0 faces C2 leg 1, leg 1 faces C3 leg 0;
+E3 (bottom) leg 0 faces C4 leg 1, leg 1 faces C3 leg 1; E4 (left) leg 0 faces
+C1 leg 0, leg 1 faces C4 leg 0.  A corner leg facing an edge's leg 0 absorbs
+X, one facing leg 1 absorbs X^-T.
 """
 from __future__ import annotations
 
@@ -36,8 +45,9 @@ import numpy as np
 
 from . import host
 
-# boundary j (0 top, 1 right, 2 bottom, 3 left): edge j (both legs) and two corner legs (corner, leg), 0-based
-BOUNDARIES = [((0, 1), (1, 0)), ((1, 1), (2, 0)), ((2, 1), (3, 1)), ((0, 0), (3, 0))]
+# boundary j (0 top, 1 right, 2 bottom, 3 left), 0-based: (corner, leg) facing
+# edge j's leg 0, and (corner, leg) facing its leg 1
+FACING = [((0, 1), (1, 0)), ((1, 1), (2, 0)), ((3, 1), (2, 1)), ((0, 0), (3, 0))]
 
 
 def _apply_leg(E: np.ndarray, leg: int, Q: np.ndarray) -> np.ndarray:
@@ -47,16 +57,29 @@ def _apply_leg(E: np.ndarray, leg: int, Q: np.ndarray) -> np.ndarray:
     return np.einsum("aibc,ij->ajbc", E, Q)
 
 
-def gauge_transform(Cs: Sequence[np.ndarray], Es: Sequence[np.ndarray], Qb: Sequence[np.ndarray]):
-    """Apply the orthogonal boundary gauges Qb[j] (new index = column of Q) to
-    every leg on boundary j."""
+def _corner_leg(C: np.ndarray, leg: int, Q: np.ndarray) -> np.ndarray:
+    return Q.T @ C if leg == 0 else C @ Q
+
+
+def gauge_transform(Cs: Sequence[np.ndarray], Es: Sequence[np.ndarray], Xs: Sequence[np.ndarray]):
+    """Apply the boundary gauges Xs[j] (invertible): E_j -> X^-1 E_j X, the
+    corner leg facing E_j's leg 0 absorbs X, the one facing leg 1 absorbs X^-T."""
     Cn = [np.array(C) for C in Cs]
     En = [np.array(E) for E in Es]
-    for j, legs in enumerate(BOUNDARIES):
-        for k, l in legs:
-            Cn[k] = Qb[j].T @ Cn[k] if l == 0 else Cn[k] @ Qb[j]
-        En[j] = _apply_leg(_apply_leg(En[j], 0, Qb[j]), 1, Qb[j])
+    for j, ((k0, l0), (k1, l1)) in enumerate(FACING):
+        X = np.asarray(Xs[j])
+        XiT = np.linalg.inv(X).T
+        Cn[k0] = _corner_leg(Cn[k0], l0, X)
+        Cn[k1] = _corner_leg(Cn[k1], l1, XiT)
+        En[j] = _apply_leg(_apply_leg(En[j], 0, XiT), 1, X)
     return Cn, En
+
+
+def _lead(x: np.ndarray, rel: float = 1e-6) -> int:
+    """Flat index of the first entry whose modulus is within rel of the largest
+    (a tie-proof "entry of largest modulus": symmetric tensors have exact ties)."""
+    a = np.abs(np.ravel(x))
+    return int(np.argmax(a >= (1.0 - rel) * a.max()))
 
 
 def _lq_gauge(M: np.ndarray) -> np.ndarray:
@@ -68,17 +91,20 @@ def _lq_gauge(M: np.ndarray) -> np.ndarray:
 
 
 def canonical(Cs: Sequence[np.ndarray], Es: Sequence[np.ndarray]):
-    """The environment in the canonical gauge (full rank)."""
+    """The environment with its orthogonal boundary gauges fixed (full rank)."""
     Cs = [np.asarray(C, dtype=np.float64) for C in Cs]
     Es = [np.asarray(E, dtype=np.float64) for E in Es]
     U, s, Vt = np.linalg.svd(Cs[0])
     V = Vt.T.copy()
     E1 = _apply_leg(_apply_leg(Es[0], 0, V), 1, V)
+    sgn = np.ones(len(s))
     for a in range(1, len(s)):
-        blk = E1[0, a]
-        if blk.flat[np.argmax(np.abs(blk))] < 0:
-            U[:, a] *= -1
-            V[:, a] *= -1
+        blk = E1[:a, a] * sgn[:a, None, None]
+        b = _lead(np.abs(blk).reshape(a, -1).max(1))
+        row = blk[b]
+        if row.flat[_lead(row)] < 0:
+            sgn[a] = -1.0
+    U, V = U * sgn, V * sgn
     Qr = _lq_gauge(V.T @ Cs[1])
     Qbot = _lq_gauge(U.T @ Cs[3])
     return gauge_transform(Cs, Es, [V, Qr, Qbot, U])
@@ -86,22 +112,20 @@ def canonical(Cs: Sequence[np.ndarray], Es: Sequence[np.ndarray]):
 
 def gauge_fix(Cs: Sequence[np.ndarray], Es: Sequence[np.ndarray], r: Optional[int] = None) -> np.ndarray:
     """Canonical-gauge vector of a real environment truncated to rank r:
-    [diag C1[:r], C2, C3, C4 (r x r, column-major), E1 .. E4 (r, r, D, D)]."""
+    [C1 .. C4 (r x r), E1 .. E4 (r, r, D, D)], each column-major."""
     Cn, En = canonical(Cs, Es)
     r = r or min(C.shape[0] for C in Cn)
-    parts = [np.diag(Cn[0])[:r]] + [C[:r, :r].ravel(order="F") for C in Cn[1:]] + \
-        [E[:r, :r].ravel(order="F") for E in En]
+    Cn = [C / np.abs(C).max() for C in Cn]
+    En = [E / np.abs(E).max() for E in En]
+    parts = [C[:r, :r].ravel(order="F") for C in Cn] + [E[:r, :r].ravel(order="F") for E in En]
     return np.concatenate(parts)
 
 
 def unpack(vec: np.ndarray, r: int, D: int):
     """(Cs, Es) of a rank-r environment in the canonical gauge from its vector."""
     vec = np.asarray(vec, dtype=np.float64)
-    Cs = [np.diag(vec[:r])]
-    o = r
-    for _ in range(3):
-        Cs.append(np.asfortranarray(vec[o:o + r * r].reshape((r, r), order="F")))
-        o += r * r
+    Cs = [np.asfortranarray(vec[j * r * r:(j + 1) * r * r].reshape((r, r), order="F")) for j in range(4)]
+    o = 4 * r * r
     n = r * r * D * D
     Es = [np.asfortranarray(vec[o + j * n:o + (j + 1) * n].reshape((r, r, D, D), order="F")) for j in range(4)]
     return Cs, Es
@@ -130,7 +154,7 @@ class WarmStart:
                  engine=None):
         self.D, self.d, self.r = D, d, r
         self.n_in = D ** 4 * d
-        self.n_out = r + 3 * r * r + 4 * r * r * D * D
+        self.n_out = 4 * r * r + 4 * r * r * D * D
         self.engine = engine or host.default_engine()
         self.net = host.Mlp(self.n_in, hidden, self.n_out, max_batch=max_batch, seed=seed, engine=self.engine)
         self.max_batch = max_batch

@@ -1,11 +1,13 @@
 """CPU checks of the warm start's canonical gauge (ipeps.jl_b200/warmstart.py)
 on an environment converged by the oracle.
 
-* the boundaries: a random orthogonal matrix on each of the 4 boundary gauges,
-  applied to both legs of the edge and to the two corner legs of the boundary,
-  leaves the energy unchanged (a wrong pairing of legs would not);
-* the canonical gauge: gauge_fix of the environment and of any such
-  re-gauged copy give the same vector;
+* the boundaries: a random invertible matrix X on each of the 4 boundary
+  gauges (E -> X^-1 E X, the facing corner legs absorbing X or X^-T) leaves the
+  energy unchanged (a wrong pairing of corner and edge legs would not);
+* the canonical gauge: gauge_fix of the environment and of a copy re-gauged by
+  random orthogonal matrices give the same vector, and so do the environments
+  after one and two more CTMRG iterations (CTMRG moves its fixed point only
+  through orthogonal gauges, which gauge_fix removes);
 * the canonical form at full rank is an exact gauge transform (same energy),
   and unpack inverts the vector layout."""
 import numpy as np
@@ -18,7 +20,7 @@ from conftest import load_package
 def _converged(D=2, chi=6, seed=3):
     A = O.random_A(D, 2, seed=seed)
     cfg = O.default_config()
-    cfg.update(chi=chi, min_iter=4, max_iter=40, rg_tol=1e-12)
+    cfg.update(chi=chi, min_iter=4, max_iter=60, rg_tol=1e-13)
     H = O.ising(2.0)
     ts = O.make_ctm_tensors(A, cfg)
     ts, _ = O.run_ctm(ts, conv_fun=lambda x: O.get_gs_energy(x, H)[0])
@@ -30,18 +32,22 @@ def _energy(ts, Cs, Es, H):
     return complex(O.get_gs_energy(t, H)[0]).real
 
 
-def test_bond_map_and_canonical_gauge():
+def _env(ts):
+    return [c.numpy() for c in ts.Cs], [e.numpy() for e in ts.Es]
+
+
+def test_boundaries_and_canonical_gauge():
     ws = load_package().warmstart
     ts, H = _converged()
-    Cs = [c.numpy() for c in ts.Cs]
-    Es = [e.numpy() for e in ts.Es]
+    Cs, Es = _env(ts)
     E0 = _energy(ts, Cs, Es, H)
     rng = np.random.default_rng(0)
-    Qb = []
-    for j in range(4):
-        n = Es[j].shape[0]
-        Qb.append(np.linalg.qr(rng.standard_normal((n, n)))[0])
-    Cg, Eg = ws.gauge_transform(Cs, Es, Qb)
+    n = [E.shape[0] for E in Es]
+    Xs = [np.eye(m) + 0.3 * rng.standard_normal((m, m)) for m in n]
+    Cx, Ex = ws.gauge_transform(Cs, Es, Xs)
+    assert abs(_energy(ts, Cx, Ex, H) - E0) <= 1e-12
+    Qs = [np.linalg.qr(rng.standard_normal((m, m)))[0] for m in n]
+    Cg, Eg = ws.gauge_transform(Cs, Es, Qs)
     assert abs(_energy(ts, Cg, Eg, H) - E0) <= 1e-12
     v = ws.gauge_fix(Cs, Es)
     vg = ws.gauge_fix(Cg, Eg)
@@ -50,3 +56,13 @@ def test_bond_map_and_canonical_gauge():
     Cc, Ec = ws.unpack(v, r, Es[0].shape[2])
     assert abs(_energy(ts, Cc, Ec, H) - E0) <= 1e-12
     assert np.allclose(ws.gauge_fix(Cc, Ec), v, atol=1e-12)
+
+
+def test_canonical_gauge_stable_under_ctmrg_iterations():
+    ws = load_package().warmstart
+    ts, H = _converged()
+    v0 = ws.gauge_fix(*_env(ts))
+    for _ in range(2):
+        ts, _ = O.rg_step(ts, 6)
+        v = ws.gauge_fix(*_env(ts))
+        assert np.abs(v - v0).max() <= 1e-7, np.abs(v - v0).max()
