@@ -191,6 +191,16 @@ IPEPS_API int ipeps_mlp_grad(ipeps_mlp* mlp, const float* X, const float* T, int
 /* one Adam step (beta1 0.9, beta2 0.999, eps 1e-8) on the batch; *loss = the batch loss before the step */
 IPEPS_API int ipeps_mlp_train_step(ipeps_mlp* mlp, const float* X, const float* T, int B, float lr, double* loss);
 
+/* ---- FP64 GEMM of the engine (the DMMA kernel every real FP64 contraction of
+ * tcon, the projector and the adjoint runs on; no counterpart in the reference,
+ * where these products are BLAS calls inside TensorOperations).  Host buffers:
+ * C = alpha*op(A)*op(B) + beta*C, column-major, op in {'N','T'}; the product is
+ * computed `reps` times from the same input C (for timing; the result is that
+ * of one product). */
+IPEPS_API int ipeps_gemm_f64(ipeps_ctx* ctx, char opA, char opB, int64_t m, int64_t n, int64_t k, double alpha,
+                             const double* A, int64_t lda, const double* B, int64_t ldb, double beta, double* C,
+                             int64_t ldc, int reps);
+
 /* ---- allocation-free FP64 GEMM (no counterpart in the reference).
  * C = alpha*op(A)*op(B) + beta*C, column-major, op in {'N','T'}; A, B, C are
  * DEVICE pointers and the work is enqueued on `stream` (a cudaStream_t; NULL =

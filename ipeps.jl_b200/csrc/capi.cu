@@ -573,6 +573,31 @@ int ipeps_gemm_bf16(ipeps_ctx* ctx, char opA, char opB, int64_t m, int64_t n, in
   });
 }
 
+int ipeps_gemm_f64(ipeps_ctx* ctx, char opA, char opB, int64_t m, int64_t n, int64_t k, double alpha,
+                   const double* A, int64_t lda, const double* B, int64_t ldb, double beta, double* C, int64_t ldc,
+                   int reps) {
+  return guarded(ctx, [&] {
+    IPEPS_CHECK(A && B && C && m > 0 && n > 0 && k > 0 && reps >= 1, "bad gemm_f64 arguments");
+    IPEPS_CHECK((opA == 'N' || opA == 'T') && (opB == 'N' || opB == 'T'), "gemm_f64: op must be 'N' or 'T'");
+    auto& c = *ctx->c;
+    const int64_t acols = (opA == 'N') ? k : m, bcols = (opB == 'N') ? n : k;
+    IPEPS_CHECK(lda >= ((opA == 'N') ? m : k) && ldb >= ((opB == 'N') ? k : n) && ldc >= m, "bad leading dimension");
+    ipeps::DBuf dA(size_t(lda * acols) * 8, c.sh), dB(size_t(ldb * bcols) * 8, c.sh), dC(size_t(ldc * n) * 8, c.sh),
+        dC0(size_t(ldc * n) * 8, c.sh);
+    h2d(c, dA.p, A, dA.bytes);
+    h2d(c, dB.p, B, dB.bytes);
+    h2d(c, dC0.p, C, dC0.bytes);
+    for (int r = 0; r < reps; ++r) {
+      IPEPS_CUDA(cudaMemcpyAsync(dC.p, dC0.p, dC.bytes, cudaMemcpyDeviceToDevice, c.stream));
+      ipeps::gemm_f64_dmma(c, opA, opB, m, n, k, alpha, static_cast<double*>(dA.p), lda, static_cast<double*>(dB.p),
+                           ldb, beta, static_cast<double*>(dC.p), ldc);
+    }
+    d2h(c, C, dC.p, dC.bytes);
+    c.sync();
+    return IPEPS_OK;
+  });
+}
+
 int ipeps_mlp_create(ipeps_ctx* ctx, int n_in, int n_hidden, int n_out, int max_batch, uint64_t seed,
                      ipeps_mlp** out) {
   return guarded(ctx, [&] {

@@ -119,14 +119,17 @@ Tensor permute(Ctx& c, const Tensor& in, const std::vector<int>& perm);
 Tensor clone(Ctx& c, const Tensor& in);
 
 // C = alpha*op(A)*op(B) + beta*C, column-major, op in {'N','T','C'}.
-// Dispatches on c.precision for real operands (FP64 SIMT or 3xTF32 tcgen05).
+// Dispatches on c.precision for real operands (FP64 DMMA or 3xTF32 tcgen05).
 void gemm(Ctx& c, DType dt, char opA, char opB, int64_t m, int64_t n, int64_t k,
           cuDoubleComplex alpha, const void* A, int64_t lda, const void* B, int64_t ldb,
           cuDoubleComplex beta, void* C, int64_t ldc, bool force_fp64 = false);
-// FP64 SIMT GEMM (always available)
+// FP64 GEMM: DMMA for real operands, register-tiled SIMT for complex128
 void gemm_f64(Ctx& c, DType dt, char opA, char opB, int64_t m, int64_t n, int64_t k,
               cuDoubleComplex alpha, const void* A, int64_t lda, const void* B, int64_t ldb,
               cuDoubleComplex beta, void* C, int64_t ldc);
+// real FP64 GEMM on the DMMA (FP64 tensor-core) path, op in {N, T}
+void gemm_f64_dmma(Ctx& c, char opA, char opB, int64_t m, int64_t n, int64_t k, double alpha, const double* A,
+                   int64_t lda, const double* B, int64_t ldb, double beta, double* C, int64_t ldc);
 // 3xTF32 tcgen05 GEMM for real operands (FP32-accumulated split products)
 // BF16 operands (rounded from FP32 while staged), FP32 accumulation and result; op in {N, T}
 void gemm_bf16(Ctx& c, char opA, char opB, int64_t m, int64_t n, int64_t k, float alpha, const float* A, int64_t lda,

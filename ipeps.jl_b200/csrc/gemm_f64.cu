@@ -1,9 +1,7 @@
-// FP64 / complex128 GEMM for sm_100a: register-tiled SIMT FMA kernel.
-//
-// On B200 the FP64 tensor-core rate equals the FP64 FMA rate, so a
-// register-tiled DFMA kernel is the plain-FP64 baseline of the engine.  Tiles:
-//   real    128x128x8, 8x8 outputs per thread, 256 threads
-//   real     64x64x16, 4x4 outputs per thread (skinny problems)
+// Complex128 GEMM for sm_100a (and the real FP64 kernel of the allocation-free
+// entry point): register-tiled SIMT FMA kernel.  Real FP64 products of the
+// engine go to the DMMA kernel (gemm_dmma.cu).  Tiles:
+//   real     64x64x16, 4x4 outputs per thread (allocation-free entry point)
 //   complex  64x64x8,  4x4 outputs per thread
 // Operands are staged through shared memory with one register prefetch stage.
 // Skinny problems (few output tiles, long K) use a deterministic split-K:
@@ -243,11 +241,8 @@ void gemm_f64(Ctx& c, DType dt, char opA, char opB, int64_t m, int64_t n, int64_
   IPEPS_CHECK(k > 0, "gemm: k == 0 is not supported");
   if (dt == DType::F64) {
     IPEPS_CHECK(oa != 2 && ob != 2, "gemm: conjugate op on real data");
-    int64_t big_tiles = ((m + 127) / 128) * ((n + 127) / 128);
-    if (big_tiles >= c.sm_count)
-      launch<double, 128, 128, 8, 8, 8>(c, oa, ob, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
-    else
-      launch<double, 64, 64, 16, 4, 4>(c, oa, ob, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+    gemm_f64_dmma(c, opA, opB, m, n, k, alpha.x, static_cast<const double*>(A), lda, static_cast<const double*>(B),
+                  ldb, beta.x, static_cast<double*>(C), ldc);
   } else {
     launch<cuDoubleComplex, 64, 64, 8, 4, 4>(c, oa, ob, m, n, k, alpha, A, lda, B, ldb, beta, C,
                                              ldc);

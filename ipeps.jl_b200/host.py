@@ -41,7 +41,7 @@ EXPORTED = [
     "ipeps_ctm_log", "ipeps_energy", "ipeps_gs_norm", "ipeps_nested_set_B", "ipeps_es_energy",
     "ipeps_all_norm", "ipeps_tcon", "ipeps_projector", "ipeps_projector_c", "ipeps_ctx_stream", "ipeps_prof_enable",
     "ipeps_prof_query", "ipeps_energy_grad", "ipeps_env_set_mixed", "ipeps_es_energy_grad",
-    "ipeps_single_dm_Ad", "ipeps_gemm_bf16", "ipeps_mlp_create", "ipeps_mlp_destroy", "ipeps_mlp_num_params",
+    "ipeps_single_dm_Ad", "ipeps_gemm_f64", "ipeps_gemm_bf16", "ipeps_mlp_create", "ipeps_mlp_destroy", "ipeps_mlp_num_params",
     "ipeps_mlp_get_params", "ipeps_mlp_set_params", "ipeps_mlp_forward", "ipeps_mlp_grad", "ipeps_mlp_train_step",
 ]
 
@@ -118,6 +118,8 @@ def load_library(path: str = LIB_PATH) -> ct.CDLL:
         "ipeps_env_set_mixed": [P, I, D],
         "ipeps_es_energy_grad": [P, dp, dp, I, I, dp, dp],
         "ipeps_single_dm_Ad": [P, dp],
+        "ipeps_gemm_f64": [P, ct.c_char, ct.c_char, ct.c_int64, ct.c_int64, ct.c_int64, D, dp, ct.c_int64, dp,
+                           ct.c_int64, D, dp, ct.c_int64, I],
         "ipeps_gemm_bf16": [P, ct.c_char, ct.c_char, ct.c_int64, ct.c_int64, ct.c_int64, ct.c_float, fp,
                             ct.c_int64, fp, ct.c_int64, ct.c_float, fp, ct.c_int64],
         "ipeps_mlp_create": [P, I, I, I, I, U64, ct.POINTER(P)],
@@ -565,6 +567,21 @@ def _fp(a: np.ndarray):
 
 def _f32(a) -> np.ndarray:
     return np.asfortranarray(np.asarray(a, dtype=np.float32))
+
+
+def gemm_f64(opA: str, opB: str, A, B, alpha: float = 1.0, beta: float = 0.0, C=None,
+             engine: Optional[Engine] = None, reps: int = 1) -> np.ndarray:
+    """C = alpha op(A) op(B) + beta C on the engine's FP64 (DMMA) GEMM; host arrays."""
+    eng = engine or default_engine()
+    A = _fortran(A, np.float64)
+    B = _fortran(B, np.float64)
+    m = A.shape[0] if opA == "N" else A.shape[1]
+    k = A.shape[1] if opA == "N" else A.shape[0]
+    n = B.shape[1] if opB == "N" else B.shape[0]
+    C = np.zeros((m, n), order="F") if C is None else _fortran(C, np.float64).copy(order="F")
+    eng.check(eng.lib.ipeps_gemm_f64(eng.h, opA.encode(), opB.encode(), m, n, k, float(alpha), _dp(A), A.shape[0],
+                                     _dp(B), B.shape[0], float(beta), _dp(C), C.shape[0], int(reps)))
+    return C
 
 
 def gemm_bf16(opA: str, opB: str, A, B, alpha: float = 1.0, beta: float = 0.0, C=None,

@@ -26,8 +26,12 @@ right gauge makes V^T C2 Q_right lower triangular with a positive diagonal
 (an LQ factorisation), the bottom gauge does the same for U^T C4; C3 and the
 edges follow.  "Leading" is the first entry in storage order whose modulus is
 within 1e-6 of the largest, so that exact ties of symmetric tensors break the
-same way.  Truncating every bond to its leading r directions gives the
-network's target: 4 r^2 corner entries and 4 r^2 D^2 edge entries.
+same way.  Rectangular corners (bonds of different dimensions after a
+cutoff-limited truncation) leave basis vectors past a corner's rank; they are
+ordered by the next corner on their boundary and signed by its edge in the
+same way.  Truncating every bond to its leading r directions (zero-padding
+narrower ones) gives the network's target: 4 r^2 corner entries and 4 r^2 D^2
+edge entries.
 
 Which corner legs face which edge legs follows the reference's contractions
 (ctmrg.jl:122-252, evaluation.jl:124-248): E1 (top) leg 0 faces C1 leg 1 and
@@ -83,11 +87,34 @@ def _lead(x: np.ndarray, rel: float = 1e-6) -> int:
 
 
 def _lq_gauge(M: np.ndarray) -> np.ndarray:
-    """Orthogonal Q with M Q lower triangular with a non-negative diagonal."""
-    Q, R = np.linalg.qr(M.T)
-    sgn = np.sign(np.diag(R))
-    sgn[sgn == 0] = 1.0
-    return Q * sgn
+    """Square orthogonal Q with M Q lower triangular with a non-negative
+    diagonal (M may be rectangular; columns past its rank stay as QR gives them)."""
+    Q, R = np.linalg.qr(M.T, mode="complete")
+    d = np.sign(np.diag(R))
+    d[d == 0] = 1.0
+    Q[:, :len(d)] *= d
+    return Q
+
+
+def _null_basis(B: np.ndarray, C: np.ndarray) -> np.ndarray:
+    """Basis of span(B) (orthonormal columns) ordered by the corner C whose
+    first leg it indexes: the left singular vectors of B^T C, which do not
+    depend on the gauge of C's other leg (signs are fixed separately)."""
+    if B.shape[1] == 0:
+        return B
+    P, _, _ = np.linalg.svd(B.T @ C)
+    return B @ P
+
+
+def _signs(E: np.ndarray, start: int, sgn: np.ndarray) -> None:
+    """Signs sgn[c], c >= start, of the basis vectors of a boundary whose edge,
+    in that basis, is E: the leading entry of E[b, c, :, :] * sgn[b] is made
+    positive, b < c the vector coupled most strongly to c."""
+    for c in range(max(start, 1), E.shape[0]):
+        blk = E[:c, c] * sgn[:c, None, None]
+        b = _lead(np.abs(blk).reshape(c, -1).max(1))
+        row = blk[b]
+        sgn[c] = -1.0 if row.flat[_lead(row)] < 0 else 1.0
 
 
 def canonical(Cs: Sequence[np.ndarray], Es: Sequence[np.ndarray]):
@@ -96,28 +123,48 @@ def canonical(Cs: Sequence[np.ndarray], Es: Sequence[np.ndarray]):
     Es = [np.asarray(E, dtype=np.float64) for E in Es]
     U, s, Vt = np.linalg.svd(Cs[0])
     V = Vt.T.copy()
-    E1 = _apply_leg(_apply_leg(Es[0], 0, V), 1, V)
-    sgn = np.ones(len(s))
-    for a in range(1, len(s)):
-        blk = E1[:a, a] * sgn[:a, None, None]
-        b = _lead(np.abs(blk).reshape(a, -1).max(1))
-        row = blk[b]
-        if row.flat[_lead(row)] < 0:
-            sgn[a] = -1.0
-    U, V = U * sgn, V * sgn
-    Qr = _lq_gauge(V.T @ Cs[1])
-    Qbot = _lq_gauge(U.T @ Cs[3])
-    return gauge_transform(Cs, Es, [V, Qr, Qbot, U])
+    ns = len(s)
+    # corners may be rectangular (the boundaries' bond dimensions differ after a
+    # cutoff-limited truncation): basis vectors past C1's rank are ordered by the
+    # next corner on their boundary (C4 for the left one, C2 for the top one)
+    U[:, ns:] = _null_basis(U[:, ns:], Cs[3])
+    V[:, ns:] = _null_basis(V[:, ns:], Cs[1])
+    # signs: singular pairs and the top boundary's extra vectors from E1 (pair 0
+    # is free: flipping every pair at once is a trivial gauge), then the left
+    # boundary's extra vectors from E4
+    st = np.ones(V.shape[1])
+    _signs(_apply_leg(_apply_leg(Es[0], 0, V), 1, V), 1, st)
+    V = V * st
+    U[:, :ns] *= st[:ns]
+    sl = np.ones(U.shape[1])
+    _signs(_apply_leg(_apply_leg(Es[3], 0, U), 1, U), ns, sl)
+    U = U * sl
+    # right and bottom gauges: LQ of C2 and C4 in the fixed top and left gauges;
+    # vectors past the corner's rank are ordered by C3 and signed by the edge
+    Qs = []
+    for M, C3leg, E in ((V.T @ Cs[1], Cs[2], Es[1]), (U.T @ Cs[3], Cs[2].T, Es[2])):
+        Q = _lq_gauge(M)
+        rk = min(M.shape)
+        Q[:, rk:] = _null_basis(Q[:, rk:], C3leg)
+        sq = np.ones(Q.shape[1])
+        _signs(_apply_leg(_apply_leg(E, 0, Q), 1, Q), max(rk, 1), sq)
+        Qs.append(Q * sq)
+    return gauge_transform(Cs, Es, [V, Qs[0], Qs[1], U])
 
 
 def gauge_fix(Cs: Sequence[np.ndarray], Es: Sequence[np.ndarray], r: Optional[int] = None) -> np.ndarray:
-    """Canonical-gauge vector of a real environment truncated to rank r:
-    [C1 .. C4 (r x r), E1 .. E4 (r, r, D, D)], each column-major."""
+    """Canonical-gauge vector of a real environment truncated (or zero-padded)
+    to rank r on every bond: [C1 .. C4 (r x r), E1 .. E4 (r, r, D, D)], each
+    column-major and scaled to max-abs 1."""
     Cn, En = canonical(Cs, Es)
-    r = r or min(C.shape[0] for C in Cn)
-    Cn = [C / np.abs(C).max() for C in Cn]
-    En = [E / np.abs(E).max() for E in En]
-    parts = [C[:r, :r].ravel(order="F") for C in Cn] + [E[:r, :r].ravel(order="F") for E in En]
+    r = r or max(max(C.shape) for C in Cn)
+    parts = []
+    for X in list(Cn) + list(En):
+        # bonds narrower than r are padded with zeros
+        P = np.zeros((r, r) + X.shape[2:])
+        a, b = min(r, X.shape[0]), min(r, X.shape[1])
+        P[:a, :b] = X[:a, :b] / np.abs(X).max()
+        parts.append(P.ravel(order="F"))
     return np.concatenate(parts)
 
 

@@ -66,3 +66,23 @@ def test_canonical_gauge_stable_under_ctmrg_iterations():
         ts, _ = O.rg_step(ts, 6)
         v = ws.gauge_fix(*_env(ts))
         assert np.abs(v - v0).max() <= 1e-7, np.abs(v - v0).max()
+
+
+def test_canonical_gauge_rectangular_corners():
+    """A top boundary narrower than the others (as after a cutoff-limited
+    truncation): corners C1, C2 are rectangular; the vector is zero-padded to
+    rank r and still gauge invariant."""
+    ws = load_package().warmstart
+    ts, H = _converged()
+    Cs, Es = _env(ts)
+    rng = np.random.default_rng(5)
+    W = np.linalg.qr(rng.standard_normal((Es[0].shape[0], 4)))[0]
+    Cs[0], Cs[1] = Cs[0] @ W, W.T @ Cs[1]
+    Es[0] = ws._apply_leg(ws._apply_leg(Es[0], 0, W), 1, W)
+    n = [E.shape[0] for E in Es]
+    assert n[0] == 4 and n[1] == 6
+    v = ws.gauge_fix(Cs, Es, r=6)
+    assert v.size == 4 * 36 + 4 * 36 * 4
+    Qs = [np.linalg.qr(rng.standard_normal((m, m)))[0] for m in n]
+    vg = ws.gauge_fix(*ws.gauge_transform(Cs, Es, Qs), r=6)
+    assert np.allclose(v, vg, atol=1e-10), np.abs(v - vg).max()
