@@ -250,7 +250,8 @@ def run_reference(args):
             moves.append(mv)
             ts.append(t_eval)
     value = len(ts) / sum(ts)
-    line = {"impl": "reference", "metric": "E+grad evals/s (Heisenberg D=4 chi=64, FP64)", "value": value,
+    line = {"impl": "reference", "metric": "E+grad evals/s (Heisenberg D=%d chi=%d); CTMRG moves/s in moves_per_s"
+            % (D, chi), "value": value,
             "unit": "evals/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * sum(ts) / max(len(ts), 1), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -387,7 +388,7 @@ def run_ours(args):
                                                          threads=os.cpu_count())
             cpu = {"value": v, "unit": "evals/s", "cores": nth, "kind": "port", "sample": sample, "moves_per_s": mv}
         out = {
-            "metric": "E+grad evals/s (Heisenberg D=4 chi=64); CTMRG moves/s in moves_per_s",
+            "metric": "E+grad evals/s (Heisenberg D=%d chi=%d); CTMRG moves/s in moves_per_s" % (D, chi),
             "value": value, "unit": "evals/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f64 (3xTF32 contractions)",
@@ -399,7 +400,7 @@ def run_ours(args):
                     "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": int(launches),
             "roofline": {"bound": "fp64" if args.precision == "fp64" else "tensor",
-                         "kernel": "gemm_f64 (register-tiled DFMA)" if args.precision == "fp64" else "gemm_tf32x3",
+                         "kernel": "gemm_f64 (DMMA m8n8k4 FP64 tensor cores)" if args.precision == "fp64" else "gemm_tf32x3",
                          "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak if peak else None, "traffic": None, "peak_source": peak_note,
                          "kernel_share_of_device_time": g["ms"] / total_ms if total_ms else None,

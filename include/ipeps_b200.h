@@ -98,6 +98,12 @@ IPEPS_API int ipeps_env_create(ipeps_ctx* ctx, int D, int d, int chi, int is_com
 IPEPS_API int ipeps_env_destroy(ipeps_env* env);
 /* Params Dict keys chi/min_iter/max_iter/ad_max_iter/rg_tol (default_config.toml:9-17) */
 IPEPS_API int ipeps_env_set_params(ipeps_env* env, int chi, int min_iter, int max_iter, int ad_max_iter, double rg_tol);
+/* rg_step runs the left and right moves concurrently, then the top and bottom
+ * moves (each pair reads and writes disjoint slots, ctmrg.jl:122-252), on two
+ * streams from two host threads; on = 0 runs the four moves one after another
+ * on one stream (same results up to the projectors' random sketches).
+ * Default on.  No counterpart in the reference (sequential moves). */
+IPEPS_API int ipeps_env_set_parallel(ipeps_env* env, int on);
 /* projector sketch: k = n+1 + max(min_over, (n+1)*num/den); power iterations cold/warm;
  * a posteriori check ||M v_i - s_i u_i|| <= resid_tol * s_1 with up to max_extra
  * further power iterations; inter_passes CholeskyQR passes for intermediate sketches;

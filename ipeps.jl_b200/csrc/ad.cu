@@ -546,7 +546,7 @@ double energy_grad(Env& e, const Tensor& Hh, const Tensor& Hv, int ad_iters, Ten
       IterCk k;
       k.Cs = e.Cs;
       k.Es = e.Es;
-      for (int d = 0; d < 4; ++d) ctm_move(e, d, &k.proj[d]);
+      ctm_moves4(e, k.proj.data());
       ck.push_back(std::move(k));
       // run_ctm's early exit (ctmrg.jl:44) can only trigger once i >= min_iter
       if (i >= e.prm.min_iter && i < ad_iters) {

@@ -270,6 +270,14 @@ int ipeps_env_set_params(ipeps_env* env, int chi, int min_iter, int max_iter, in
   });
 }
 
+int ipeps_env_set_parallel(ipeps_env* env, int on) {
+  if (!env) return IPEPS_EINVAL;
+  return guarded(env->owner, [&] {
+    env->e.parallel_moves = on != 0;
+    return IPEPS_OK;
+  });
+}
+
 int ipeps_env_set_svd_params(ipeps_env* env, int over_num, int over_den, int min_over, int power_iters,
                              int power_iters_warm, int warm_start, double resid_tol, int max_extra,
                              int inter_passes, int seed_older) {

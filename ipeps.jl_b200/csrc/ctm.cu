@@ -8,6 +8,8 @@
 #include "moves.cuh"
 
 #include <chrono>
+#include <exception>
+#include <thread>
 #include <cmath>
 
 namespace ipeps {
@@ -222,12 +224,129 @@ std::vector<double> ctm_move(Env& e, int dir, ProjResult* keep) {
   return s;
 }
 
+namespace {
+
+void rehome(Tensor& t, const std::shared_ptr<StreamHolder>& sh) {
+  if (t.buf && t.buf->sh != sh) t.buf->sh = sh;
+}
+
+// Moves `da` (on e's context) and `db` (on the auxiliary context) at the same
+// time.  The pairs (left, right) and (top, bottom) touch disjoint slots: left
+// reads C1 C4 E1 E3 E4 and writes C1 E4 C4, right reads C2 C3 E1 E2 E3 and
+// writes C2 E2 C3 (ctmrg.jl:122-186); top reads C1 C2 E1 E2 E4 and writes
+// C1 E1 C2, bottom reads C3 C4 E2 E3 E4 and writes C3 E3 C4 (ctmrg.jl:188-252).
+// Each move runs from its own host thread (the projector reads singular values
+// back, so one thread could not keep both streams busy) on a shallow copy of
+// the environment; afterwards the streams are joined both ways, the second
+// move's slots and projector cache are copied back, and every long-lived
+// tensor is re-homed to the main stream, so later frees are ordered after all
+// work of both streams.  Until then `keep` holds every tensor either move may
+// drop, so no buffer is freed while the other stream may still read it.
+std::vector<double> move_pair(Env& e, int da, int db, ProjResult* ka, ProjResult* kb) {
+  Ctx& c1 = *e.ctx;
+  if (!e.aux) {
+    e.aux = std::make_shared<Ctx>(c1.device);
+    e.aux->rng_seed = c1.rng_seed ^ 0x9e3779b97f4a7c15ULL;
+  }
+  Ctx& c2 = *e.aux;
+  c2.precision = c1.precision;
+  c2.prof = c1.prof;
+  const Env keep = e;
+  Env eb = e;
+  eb.ctx = &c2;
+  eb.aux.reset();
+  cudaEvent_t ev0 = c1.take_event(), ev1 = c1.take_event(), ev2 = c1.take_event();
+  IPEPS_CUDA(cudaEventRecord(ev0, c1.stream));
+  IPEPS_CUDA(cudaStreamWaitEvent(c2.stream, ev0, 0));
+  std::exception_ptr err_a, err_b;
+  std::vector<double> s;
+  std::thread tb([&] {
+    try {
+      IPEPS_CUDA(cudaSetDevice(c2.device));
+      ctm_move(eb, db, kb);
+    } catch (...) {
+      err_b = std::current_exception();
+    }
+  });
+  try {
+    s = ctm_move(e, da, ka);
+  } catch (...) {
+    err_a = std::current_exception();
+  }
+  tb.join();
+  IPEPS_CUDA(cudaEventRecord(ev1, c2.stream));
+  IPEPS_CUDA(cudaStreamWaitEvent(c1.stream, ev1, 0));
+  IPEPS_CUDA(cudaEventRecord(ev2, c1.stream));
+  IPEPS_CUDA(cudaStreamWaitEvent(c2.stream, ev2, 0));
+  c1.ev_pool.push_back(ev0);
+  c1.ev_pool.push_back(ev1);
+  c1.ev_pool.push_back(ev2);
+  // counters and timing records of the auxiliary context go to the main one
+  for (int f = 0; f < int(KFam::Count); ++f) {
+    c1.stats[f].launches += c2.stats[f].launches;
+    c1.stats[f].flops += c2.stats[f].flops;
+    c1.stats[f].bytes += c2.stats[f].bytes;
+    c1.prof_stats[f].launches += c2.prof_stats[f].launches;
+    c1.prof_stats[f].flops += c2.prof_stats[f].flops;
+    c1.prof_stats[f].bytes += c2.prof_stats[f].bytes;
+  }
+  c2.stats = {};
+  c2.prof_stats = {};
+  c1.jacobi_sweeps += c2.jacobi_sweeps;
+  c1.projector_calls += c2.projector_calls;
+  c1.projector_extra_passes += c2.projector_extra_passes;
+  c2.jacobi_sweeps = c2.projector_calls = c2.projector_extra_passes = 0;
+  for (auto& r : c2.prof_rec) c1.prof_rec.push_back(r);
+  c2.prof_rec.clear();
+  if (err_a) std::rethrow_exception(err_a);
+  if (err_b) std::rethrow_exception(err_b);
+  int ia, ib, ie;
+  move_slots(db, &ia, &ib, &ie);
+  e.Cs[ia] = eb.Cs[ia];
+  e.Cs[ib] = eb.Cs[ib];
+  e.Es[ie] = eb.Es[ie];
+  using Slots = std::array<Tensor, 4> Env::*;
+  if (e.nested) {
+    for (Slots a : {&Env::B_Cs, &Env::Bd_Cs, &Env::BB_Cs}) {
+      (e.*a)[ia] = (eb.*a)[ia];
+      (e.*a)[ib] = (eb.*a)[ib];
+    }
+    for (Slots a : {&Env::B_Es, &Env::Bd_Es, &Env::BB_Es}) (e.*a)[ie] = (eb.*a)[ie];
+  }
+  e.cache[db] = eb.cache[db];
+  e.moves += eb.moves - keep.moves;
+  e.move_seconds += eb.move_seconds - keep.move_seconds;
+  for (int i = 0; i < 4; ++i) {
+    for (Slots a : {&Env::Cs, &Env::Es, &Env::B_Cs, &Env::Bd_Cs, &Env::BB_Cs, &Env::B_Es, &Env::Bd_Es, &Env::BB_Es})
+      rehome((e.*a)[i], c1.sh);
+    rehome(e.cache[i].V, c1.sh);
+    rehome(e.cache[i].Vold, c1.sh);
+  }
+  if (kb)
+    for (Tensor* t : {&kb->P1, &kb->P2, &kb->S, &kb->Ur, &kb->Vr, &kb->Sr}) rehome(*t, c1.sh);
+  return s;
+}
+
+}  // namespace
+
+std::vector<double> ctm_moves4(Env& e, ProjResult* keep) {
+  ProjResult* k[4] = {nullptr, nullptr, nullptr, nullptr};
+  if (keep)
+    for (int d = 0; d < 4; ++d) k[d] = keep + d;
+  std::vector<double> s;
+  if (e.parallel_moves) {
+    s = move_pair(e, 0, 1, k[0], k[1]);
+    move_pair(e, 2, 3, k[2], k[3]);
+  } else {
+    s = ctm_move(e, 0, k[0]);
+    for (int d = 1; d < 4; ++d) ctm_move(e, d, k[d]);
+  }
+  return s;
+}
+
 // ctmrg.jl:57-64
 std::vector<double> rg_step(Env& e) {
-  std::vector<double> s = ctm_move(e, 0);
-  ctm_move(e, 1);
-  ctm_move(e, 2);
-  ctm_move(e, 3);
+  std::vector<double> s = ctm_moves4(e, nullptr);
   e.last_s = s;
   return s;
 }

@@ -62,6 +62,11 @@ struct Env {
   // statistics
   uint64_t moves = 0;
   double move_seconds = 0;
+  // rg_step runs left || right, then top || bottom: each pair reads and writes
+  // disjoint environment slots.  The second move of a pair runs on `aux`, a
+  // context with its own stream (created on first use).
+  bool parallel_moves = true;
+  std::shared_ptr<Ctx> aux;
 
   NT all_A() const;
   NT all_Ad() const;
@@ -80,6 +85,10 @@ struct Traces {
 // tr(H rho) and tr(rho) of several (rho, H) pairs (FP64, one host round trip)
 std::vector<Traces> dm_traces(Ctx& c, const std::vector<std::pair<Tensor, Tensor>>& items);
 std::vector<double> rg_step(Env& e);
+// the four moves of rg_step (left || right, then top || bottom when
+// e.parallel_moves); keep (optional, 4 entries, by direction) receives the
+// projectors with their resolved triplets.  Returns the left-move spectrum.
+std::vector<double> ctm_moves4(Env& e, ProjResult* keep);
 // energy (evaluation.jl:15-29): E (complex) and Na (complex)
 void gs_energy(Env& e, const Tensor& Hh, const Tensor& Hv, std::complex<double>* E, std::complex<double>* Na);
 // nested energy (evaluation.jl:31-45): real(E[4])

@@ -12,6 +12,8 @@
 // kernel records bit 8 in the status word and drains.
 #include "umma.cuh"
 
+#include <atomic>
+
 #include <algorithm>
 
 namespace ipeps {
@@ -203,7 +205,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) gemm_bf16_kernel(ArgsB a) {
   }
 }
 
-bool g_bf16_attr = false;
+std::atomic<bool> g_bf16_attr{false};
 
 }  // namespace
 

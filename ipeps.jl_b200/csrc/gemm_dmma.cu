@@ -20,6 +20,8 @@
 // K chunk go to a workspace and are summed in a fixed order.
 #include "ctx.cuh"
 
+#include <atomic>
+
 #include <algorithm>
 
 namespace ipeps {
@@ -201,7 +203,7 @@ void launch_cfg(Ctx& c, int64_t m, int64_t n, int64_t k, double alpha, const dou
   constexpr size_t smem = size_t(kStages) * (Tile<BM, AK>::size + Tile<BN, BK_>::size) * sizeof(double);
   auto kern = dmma_gemm_kernel<BM, BN, WGM, WGN, AK, BK_, VEC>;
   // the dynamic shared-memory limit is a per-function, per-device attribute
-  static bool attr_set[64] = {};
+  static std::atomic<bool> attr_set[64];
   int dev = 0;
   IPEPS_CUDA(cudaGetDevice(&dev));
   if (dev >= 64 || !attr_set[dev]) {

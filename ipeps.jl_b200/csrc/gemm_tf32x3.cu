@@ -19,6 +19,8 @@
 // on timeout the kernel records bit 8 in the status word and drains.
 #include "umma.cuh"
 
+#include <atomic>
+
 #include <algorithm>
 
 namespace ipeps {
@@ -245,7 +247,7 @@ __global__ void splitk_reduce_f64(int64_t M, int64_t N, int S, const double* __r
   *cp = (beta != 0.0) ? fma(alpha, s, beta * *cp) : alpha * s;
 }
 
-bool g_attr_set = false;
+std::atomic<bool> g_attr_set{false};
 
 }  // namespace
 

@@ -212,11 +212,11 @@ double es_energy_grad(Env& e, const Tensor& Hh, const Tensor& Hv, int ad_iters, 
     for (int i = 1; i <= ad_iters; ++i) {
       EsCk k;
       slots(k.C, k.E);
+      std::array<ProjResult, 4> pr;
+      ctm_moves4(e, pr.data());
       for (int d = 0; d < 4; ++d) {
-        ProjResult pr;
-        ctm_move(e, d, &pr);
-        k.P1[d] = pr.P1;
-        k.P2[d] = pr.P2;
+        k.P1[d] = pr[d].P1;
+        k.P2[d] = pr[d].P2;
       }
       ck.push_back(std::move(k));
       // run_ctm's early exit with conv_fun = get_es_energy / get_all_norm (optim_es.jl:200)

@@ -116,6 +116,34 @@ __global__ void permute_simple(PermArgs a, int64_t total, const T* __restrict__ 
   }
 }
 
+// perm[0] == 0 with a long first dimension: every output "row" (n0
+// consecutive elements) is a contiguous run of the input too.  One warp per
+// row; the mixed-radix decomposition of the row index (integer divisions) is
+// done once per row instead of once per element.
+struct RowArgs {
+  int nd;                     // output dims after the first
+  int64_t n0;                 // row length (extent of the shared first dim)
+  int64_t odims[kMaxDims];    // output dims 1.. (innermost first)
+  int64_t istride[kMaxDims];  // their input strides
+};
+
+template <typename T>
+__global__ void permute_rows(RowArgs a, int64_t rows, const T* __restrict__ in, T* __restrict__ out) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t r = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; r < rows; r += nwarps) {
+    int64_t q = r, off = 0;
+    for (int i = 0; i < a.nd; ++i) {
+      const int64_t t = q / a.odims[i];
+      off += (q - t * a.odims[i]) * a.istride[i];
+      q = t;
+    }
+    const T* src = in + off;
+    T* dst = out + r * a.n0;
+    for (int64_t i = lane; i < a.n0; i += 32) dst[i] = src[i];
+  }
+}
+
 struct TileArgs {
   int64_t n0, nq;        // extent of input dim 0 and of input dim q (= output dim 0)
   int64_t in_q_stride;   // input stride of dim q
@@ -167,7 +195,18 @@ void permute_impl(Ctx& c, const Tensor& in, const std::vector<int>& perm, Tensor
   const int64_t total = in.numel();
   const T* ip = static_cast<const T*>(in.data());
   T* op = static_cast<T*>(out.data());
-  if (perm[0] == 0 || in.dims[0] == 1 || out.dims[0] == 1) {
+  if (perm[0] == 0 && in.dims[0] >= 16 && nd > 1) {
+    RowArgs a{};
+    a.nd = nd - 1;
+    a.n0 = in.dims[0];
+    for (int i = 1; i < nd; ++i) {
+      a.odims[i - 1] = out.dims[i];
+      a.istride[i - 1] = istr[perm[i]];
+    }
+    const int64_t rows = total / a.n0;
+    const int64_t blocks = std::min<int64_t>((rows + 7) / 8, int64_t(c.sm_count) * 16);
+    permute_rows<T><<<unsigned(std::max<int64_t>(blocks, 1)), 256, 0, c.stream>>>(a, rows, ip, op);
+  } else if (perm[0] == 0 || in.dims[0] == 1 || out.dims[0] == 1) {
     PermArgs a{};
     a.nd = nd;
     for (int i = 0; i < nd; ++i) {
@@ -239,8 +278,29 @@ Tensor permute(Ctx& c, const Tensor& in, const std::vector<int>& perm) {
   std::vector<int> p2;
   for (int i = 0; i < in.nd; ++i)
     if (in.dims[perm[i]] != 1) p2.push_back(rank[perm[i]]);
-  in2.nd = int(keep.size());
-  for (size_t r = 0; r < keep.size(); ++r) in2.dims[r] = in.dims[keep[r]];
+  // merge runs of input dims that stay adjacent (and in order) in the output:
+  // fewer dims, longer contiguous runs, shorter index arithmetic
+  std::vector<int64_t> kd(keep.size());
+  for (size_t r = 0; r < keep.size(); ++r) kd[r] = in.dims[keep[r]];
+  std::vector<int> gstart;  // output-ordered groups: first input dim of each
+  std::vector<int64_t> gsize;
+  for (size_t t = 0; t < p2.size(); ++t) {
+    if (t > 0 && p2[t] == p2[t - 1] + 1) {
+      gsize.back() *= kd[p2[t]];
+    } else {
+      gstart.push_back(p2[t]);
+      gsize.push_back(kd[p2[t]]);
+    }
+  }
+  std::vector<int> order(gstart.size());  // groups sorted by input position
+  for (size_t g = 0; g < order.size(); ++g) order[g] = int(g);
+  std::sort(order.begin(), order.end(), [&](int x, int y) { return gstart[x] < gstart[y]; });
+  std::vector<int> gpos(gstart.size());
+  for (size_t r = 0; r < order.size(); ++r) gpos[order[r]] = int(r);
+  in2.nd = int(order.size());
+  for (size_t r = 0; r < order.size(); ++r) in2.dims[r] = gsize[order[r]];
+  p2.assign(gstart.size(), 0);
+  for (size_t g = 0; g < gstart.size(); ++g) p2[g] = gpos[g];
   out2.nd = int(p2.size());
   for (size_t r = 0; r < p2.size(); ++r) out2.dims[r] = in2.dims[p2[r]];
   ProfScope ps(c, KFam::Permute);

@@ -13,6 +13,8 @@
 // svd(R1*R2) (src/utility/wrapper.jl:25-35) in the randomized projector.
 #include "linalg.cuh"
 
+#include <atomic>
+
 namespace ipeps {
 namespace {
 
@@ -475,7 +477,8 @@ __global__ void __launch_bounds__(kApplyRows * 32) jacobi_apply_kernel(const dou
     for (int j = lane; j < k; j += 32) J[i + int64_t(j) * ldj] = row[j];
 }
 
-bool g_chol_attr = false, g_trsm_attr[9] = {}, g_jlog_attr[11] = {}, g_apply_attr = false;
+// shared-memory opt-in done once per kernel (concurrent moves may race to it: atomics)
+std::atomic<bool> g_chol_attr{false}, g_trsm_attr[9], g_jlog_attr[11], g_apply_attr{false};
 
 template <int NV>
 void launch_jacobi(Ctx& c, double* X, int m, int k, int64_t ldx, double2* rot, int max_sweeps, double tol, double* S,

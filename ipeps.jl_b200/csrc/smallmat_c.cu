@@ -12,6 +12,8 @@
 //                    (unitary); the rotations are logged and applied to J row-parallel.
 #include "linalg.cuh"
 
+#include <atomic>
+
 namespace ipeps {
 namespace {
 
@@ -279,7 +281,7 @@ __global__ void __launch_bounds__(kApplyCRows * 32) jacobi_c_apply_kernel(const 
   for (int j = lane; j < k; j += 32) J[i + int64_t(j) * ldj] = row[j];
 }
 
-bool g_cholc_attr = false, g_trsmc_attr = false, g_jacc_attr = false, g_appc_attr = false;
+std::atomic<bool> g_cholc_attr{false}, g_trsmc_attr{false}, g_jacc_attr{false}, g_appc_attr{false};
 
 size_t cholc_smem(int k) { return (size_t(k) * (k + 1) / 2 + size_t(k)) * 16; }
 size_t trsmc_smem(int k) { return (size_t(k) * (k + 1) / 2 + size_t(kTrsmCRows) * k) * 16 + size_t(k) * 8; }

@@ -36,7 +36,7 @@ CONV_ENERGY, CONV_SPECTRUM, CONV_ES = 0, 1, 2
 EXPORTED = [
     "ipeps_ctx_create", "ipeps_ctx_destroy", "ipeps_last_error", "ipeps_ctx_set_precision",
     "ipeps_ctx_set_seed", "ipeps_stats", "ipeps_stats_reset", "ipeps_env_create", "ipeps_env_destroy",
-    "ipeps_env_set_params", "ipeps_env_set_svd_params", "ipeps_env_set_A", "ipeps_env_init",
+    "ipeps_env_set_params", "ipeps_env_set_svd_params", "ipeps_env_set_parallel", "ipeps_env_set_A", "ipeps_env_init",
     "ipeps_env_get_CT", "ipeps_env_set_CT", "ipeps_ctm_move", "ipeps_ctm_step", "ipeps_ctm_run",
     "ipeps_ctm_log", "ipeps_energy", "ipeps_gs_norm", "ipeps_nested_set_B", "ipeps_es_energy",
     "ipeps_all_norm", "ipeps_tcon", "ipeps_projector", "ipeps_projector_c", "ipeps_ctx_stream", "ipeps_prof_enable",
@@ -95,6 +95,7 @@ def load_library(path: str = LIB_PATH) -> ct.CDLL:
         "ipeps_env_destroy": [P],
         "ipeps_env_set_params": [P, I, I, I, I, D],
         "ipeps_env_set_svd_params": [P, I, I, I, I, I, I, D, I, I, I],
+        "ipeps_env_set_parallel": [P, I],
         "ipeps_env_set_A": [P, dp, dp],
         "ipeps_env_init": [P],
         "ipeps_env_get_CT": [P, I, dp, lp, dp, lp],
@@ -244,7 +245,8 @@ class CTMTensors:
     reference constructor.  The Params dict is ``self.Params``; keys chi,
     min_iter, max_iter, ad_max_iter, rg_tol are pushed to the device before
     every run/step.  Extra keys (not read by the reference): ``svd_oversample``
-    (num, den, min), ``svd_power_iters`` (cold, warm), ``svd_warm_start``.
+    (num, den, min), ``svd_power_iters`` (cold, warm), ``svd_warm_start``,
+    ``parallel_moves`` (left || right and top || bottom on two streams).
     """
 
     def __init__(self, A, cfg: Optional[Dict[str, Any]] = None, Ad=None, engine: Optional[Engine] = None,
@@ -289,9 +291,10 @@ class CTMTensors:
         pit = p.get("svd_power_iters", (3, 2))
         self.engine.check(self.lib.ipeps_env_set_svd_params(
             self.h, int(over[0]), int(over[1]), int(over[2]), int(pit[0]), int(pit[1]),
-            int(bool(p.get("svd_warm_start", True))), float(p.get("svd_resid_tol", 1e-11)),
+            int(bool(p.get("svd_warm_start", True))), float(p.get("svd_resid_tol", 1e-10)),
             int(p.get("svd_max_extra", 6)), int(p.get("svd_inter_passes", 1)),
             int(bool(p.get("svd_seed_older", True)))))
+        self.engine.check(self.lib.ipeps_env_set_parallel(self.h, int(bool(p.get("parallel_moves", True)))))
         self.engine.check(self.lib.ipeps_env_set_mixed(
             self.h, int(p.get("mixed_polish_iters", 4)), float(p.get("mixed_polish_tol", 1e-6))))
 
