@@ -379,22 +379,25 @@ namespace {
 void projector_backward(Ctx& c, const Tensor& R1t, bool t1, const Tensor& R2t, bool t2, const ProjResult& pr,
                         const Tensor& P1, const Tensor& P2, const Tensor& dP1in, const Tensor& dP2in, Tensor* dR1t,
                         Tensor* dR2t) {
+  // R1: N1 x K1, R2: K1 x N2 (rectangular when the boundaries' bond
+  // dimensions differ); U: N1 x n, V: N2 x n, P1: K1 x n, P2: n x K1
   const int n = pr.n, r = pr.r;
-  const int64_t N = pr.Ur.dims[0];
+  const int64_t N1 = pr.Ur.dims[0], N2 = pr.Vr.dims[0], K1 = P1.dims[0];
+  IPEPS_CHECK(P2.dims[1] == K1, "projector_backward: P1/P2 shapes differ");
   Tensor Ut = cols(pr.Ur, 0, n), Vt = cols(pr.Vr, 0, n);
   Tensor s = vec_view(pr.Sr, 0, n);
-  Tensor dP1 = dP1in.empty() ? c.zeros(DType::F64, {N, n}) : dP1in.reshape({N, n});
-  Tensor dP2 = dP2in.empty() ? c.zeros(DType::F64, {n, N}) : dP2in.reshape({n, N});
+  Tensor dP1 = dP1in.empty() ? c.zeros(DType::F64, {K1, n}) : dP1in.reshape({K1, n});
+  Tensor dP2 = dP2in.empty() ? c.zeros(DType::F64, {n, K1}) : dP2in.reshape({n, K1});
   // dU_t = R1 dP2^T S^-1/2,  dV_t = R2^T dP1 S^-1/2
-  Tensor dUt = c.alloc(DType::F64, {N, n});
-  gemm(c, DType::F64, t1 ? 'T' : 'N', 'T', N, n, N, cplx(1), R1t.data(), R1t.dims[0], dP2.data(), n, cplx(0),
-       dUt.data(), N);
+  Tensor dUt = c.alloc(DType::F64, {N1, n});
+  gemm(c, DType::F64, t1 ? 'T' : 'N', 'T', N1, n, K1, cplx(1), R1t.data(), R1t.dims[0], dP2.data(), n, cplx(0),
+       dUt.data(), N1);
   colscale(c, dUt, s.f64(), n, 1);
   Tensor dVt = Rapply(c, R2t, t2, 'T', dP1);
   colscale(c, dVt, s.f64(), n, 1);
   // dS
   Tensor dS = c.alloc(DType::F64, {n});
-  dS_kernel<<<(n * 32 + 255) / 256, 256, 0, c.stream>>>(n, N, dP1.f64(), P1.f64(), dP2.f64(), P2.f64(), s.f64(),
+  dS_kernel<<<(n * 32 + 255) / 256, 256, 0, c.stream>>>(n, K1, dP1.f64(), P1.f64(), dP2.f64(), P2.f64(), s.f64(),
                                                          dS.f64());
   IPEPS_LAUNCH_CHECK();
   // kept x kept block
@@ -405,9 +408,9 @@ void projector_backward(Ctx& c, const Tensor& R1t, bool t1, const Tensor& R2t, b
   IPEPS_LAUNCH_CHECK();
   // W1 = V_t A_tt^T ; Acol, Bcol accumulate the discarded couplings
   Tensor W1 = mm(c, Vt, 'N', Att, 'T', true);
-  Tensor Bcol = c.zeros(DType::F64, {N, n});
-  Tensor VinGv_plus_Xv = c.zeros(DType::F64, {N, n});  // (V_in G_v + X_v), later scaled by s_t
-  Tensor UinGu_plus_Xu = c.zeros(DType::F64, {N, n});  // (U_in G_u + X_u), later scaled by s_t
+  Tensor Bcol = c.zeros(DType::F64, {N1, n});
+  Tensor VinGv_plus_Xv = c.zeros(DType::F64, {N2, n});  // (V_in G_v + X_v), later scaled by s_t
+  Tensor UinGu_plus_Xu = c.zeros(DType::F64, {N1, n});  // (U_in G_u + X_u), later scaled by s_t
   if (r > n) {
     const int nin = r - n;
     Tensor Uin = cols(pr.Ur, n, nin), Vin = cols(pr.Vr, n, nin);
@@ -423,22 +426,22 @@ void projector_backward(Ctx& c, const Tensor& R1t, bool t1, const Tensor& R2t, b
     Tensor sGu = clone(c, Gu), sGv = clone(c, Gv);
     scale_rows(c, sGu.f64(), nin, nin, n, sin.f64(), 0);
     scale_rows(c, sGv.f64(), nin, nin, n, sin.f64(), 0);
-    gemm(c, DType::F64, 'N', 'N', N, n, nin, cplx(1), Vin.data(), N, sGu.data(), nin, cplx(1), W1.data(), N, true);
-    gemm(c, DType::F64, 'N', 'N', N, n, nin, cplx(1), Uin.data(), N, sGv.data(), nin, cplx(1), Bcol.data(), N, true);
-    gemm(c, DType::F64, 'N', 'N', N, n, nin, cplx(1), Vin.data(), N, Gv.data(), nin, cplx(0), VinGv_plus_Xv.data(), N,
-         true);
-    gemm(c, DType::F64, 'N', 'N', N, n, nin, cplx(1), Uin.data(), N, Gu.data(), nin, cplx(0), UinGu_plus_Xu.data(), N,
-         true);
+    gemm(c, DType::F64, 'N', 'N', N2, n, nin, cplx(1), Vin.data(), N2, sGu.data(), nin, cplx(1), W1.data(), N2, true);
+    gemm(c, DType::F64, 'N', 'N', N1, n, nin, cplx(1), Uin.data(), N1, sGv.data(), nin, cplx(1), Bcol.data(), N1, true);
+    gemm(c, DType::F64, 'N', 'N', N2, n, nin, cplx(1), Vin.data(), N2, Gv.data(), nin, cplx(0), VinGv_plus_Xv.data(),
+         N2, true);
+    gemm(c, DType::F64, 'N', 'N', N1, n, nin, cplx(1), Uin.data(), N1, Gu.data(), nin, cplx(0), UinGu_plus_Xu.data(),
+         N1, true);
   }
   // complement of the resolved vectors: Taylor series of the broadened resolvent
   {
     Tensor Ur = pr.Ur, Vr = pr.Vr;
     Tensor Yu = project_out(c, Ur, dUt), Yv = project_out(c, Vr, dVt);
-    Tensor Xu = c.zeros(DType::F64, {N, n}), Xv = c.zeros(DType::F64, {N, n});
+    Tensor Xu = c.zeros(DType::F64, {N1, n}), Xv = c.zeros(DType::F64, {N2, n});
     double* d_cmax = reinterpret_cast<double*>(c.scal->p) + 40;
     for (int m = 0; m < 16; ++m) {
-      series_acc_kernel<<<gridn(c, N * n), 256, 0, c.stream>>>(Xu.f64(), Yu.f64(), N, n, s.f64(), kSvdEta, m);
-      series_acc_kernel<<<gridn(c, N * n), 256, 0, c.stream>>>(Xv.f64(), Yv.f64(), N, n, s.f64(), kSvdEta, m);
+      series_acc_kernel<<<gridn(c, N1 * n), 256, 0, c.stream>>>(Xu.f64(), Yu.f64(), N1, n, s.f64(), kSvdEta, m);
+      series_acc_kernel<<<gridn(c, N2 * n), 256, 0, c.stream>>>(Xv.f64(), Yv.f64(), N2, n, s.f64(), kSvdEta, m);
       series_coef_max_kernel<<<1, 32, 0, c.stream>>>(s.f64(), n, kSvdEta, m, d_cmax);
       IPEPS_LAUNCH_CHECK();
       double cmax = 0;
@@ -472,8 +475,8 @@ void projector_backward(Ctx& c, const Tensor& R1t, bool t1, const Tensor& R2t, b
   axpy(c, cplx(1), UinGu_plus_Xu, Bcol);  // Bcol complete
   // dR1 = U_t [ (R2 W1)^T + S^-1/2 dP2 ] + Bcol (R2 V_t)^T,   R2 V_t = P1 S^1/2
   Tensor Z = Rapply(c, R2t, t2, 'N', W1);
-  Tensor dP2T = c.alloc(DType::F64, {N, n});
-  transpose_scale_kernel<<<gridn(c, N * n), 256, 0, c.stream>>>(dP2.f64(), n, N, s.f64(), dP2T.f64());
+  Tensor dP2T = c.alloc(DType::F64, {K1, n});
+  transpose_scale_kernel<<<gridn(c, K1 * n), 256, 0, c.stream>>>(dP2.f64(), n, K1, s.f64(), dP2T.f64());
   IPEPS_LAUNCH_CHECK();
   axpy(c, cplx(1), dP2T, Z);
   Tensor BcolS = clone(c, Bcol);

@@ -30,10 +30,13 @@ def _sphere_project(x, g):
 
 def optim_gs(H, A0, cfg: Dict[str, Any], m: int = 10, g_tol: float = 1e-6, f_tol: float = 1e-7,
              iterations: int = 200, engine: Optional[host.Engine] = None,
-             callback: Optional[Callable[[int, float, float], None]] = None):
+             callback: Optional[Callable[[int, float, float], None]] = None,
+             fg_fn: Optional[Callable] = None):
     """L-BFGS over A on the unit sphere with the device E+grad unit (fg!).
 
-    Returns dict(A, energies, gradnorms, evals)."""
+    ``fg_fn(A, H, cfg, engine=...) -> (E, g, info)`` replaces host.fg (e.g. the
+    warm-started unit of warmstart.WarmStart.fg).  Returns dict(A, energies,
+    gradnorms, evals)."""
     x = np.asarray(A0, dtype=np.float64).ravel(order="F")
     shape = np.asarray(A0).shape
     x = x / np.linalg.norm(x)
@@ -46,7 +49,7 @@ def optim_gs(H, A0, cfg: Dict[str, Any], m: int = 10, g_tol: float = 1e-6, f_tol
         # fg! renormalises x by max|x| before the energy (optim_gs.jl:55); the
         # energy is scale invariant, the gradient scales by max|x|
         s = np.abs(A).max()
-        E, g, _ = host.fg(A, H, cfg, engine=engine)
+        E, g, _ = (fg_fn or host.fg)(A, H, cfg, engine=engine)
         return E, g.ravel(order="F") / s
 
     f, g = fg(x)

@@ -187,6 +187,13 @@ def read_env(ts: host.CTMTensors):
     return Cs, Es
 
 
+def energy_bound(H) -> float:
+    """|E| per site can not exceed ||Hh||_2 + ||Hv||_2 (one horizontal and one
+    vertical bond per site); a converged run outside it is a spurious fixed
+    point (from a bad starting environment) and is rejected."""
+    return float(sum(np.linalg.norm(np.asarray(h).reshape(int(np.sqrt(np.asarray(h).size)), -1), 2) for h in H)) * (1 + 1e-9)
+
+
 def converge_default(A, H, cfg: Dict[str, Any], engine=None):
     """Plain CTMRG from init_ctm1 with the energy criterion (the judge)."""
     ts = host.CTMTensors(A, cfg, engine=engine)
@@ -238,8 +245,9 @@ class WarmStart:
 
     def converge(self, A, H, cfg: Dict[str, Any], warm_max_iter: Optional[int] = None):
         """CTMRG from the predicted environment; falls back to init_ctm1 when it
-        has not converged within warm_max_iter iterations (default max_iter).
-        Returns (ts, info, used_warm_start, iterations in total)."""
+        has not converged within warm_max_iter iterations (default max_iter)
+        or converged outside the energy bound of H.  Returns (ts, info,
+        used_warm_start, iterations in total)."""
         Cs, Es = unpack(self.predict([A])[0], self.r, self.D)
         wcfg = dict(cfg)
         if warm_max_iter is not None:
@@ -248,12 +256,25 @@ class WarmStart:
         for k in range(4):
             ts.set_CT(k + 1, Cs[k], Es[k])
         ts, info = host.run_ctm(ts, conv_fun="energy", H=H)
-        if info["converged"]:
+        if info["converged"] and abs(info["log"][-1]["obj"]) <= energy_bound(H):
             return ts, info, True, len(info["log"])
         spent = len(info["log"])
         ts.close()
         ts, info = converge_default(A, H, cfg, engine=self.engine)
         return ts, info, False, spent + len(info["log"])
+
+    def fg(self, A, H, cfg: Dict[str, Any], engine=None, warm_max_iter: Optional[int] = None):
+        """The E+grad unit of optim_gs (host.fg) started from the predicted
+        environment; same return value (E, g, info), info["warm_start"] telling
+        whether the prediction was used and info["iterations"] the CTMRG
+        iterations spent (fallback included)."""
+        A = np.asarray(A, dtype=np.float64)
+        A = A / np.abs(A).max()
+        ts, info, used, iters = self.converge(A, H, cfg, warm_max_iter=warm_max_iter)
+        E, g = host.energy_grad(ts, H)
+        ts.close()
+        info = dict(info, warm_start=used, iterations=iters)
+        return E, g, info
 
     def close(self):
         self.net.close()

@@ -26,6 +26,31 @@ def test_energy_grad_matches_oracle(engine, pkg, D, chi, model, seed):
     assert rel <= 1e-6, rel
 
 
+def test_energy_grad_rectangular_environment(engine, pkg):
+    """A near-product state (a product state plus 0.3 times Gaussian tensors,
+    halfway along a straight path) whose cutoff-limited truncations leave
+    boundaries of different bond dimensions (oracle: C1 16 x 14, C2 14 x 15,
+    C3 15 x 16): the enlarged-corner matrices of the projector adjoint are
+    rectangular (R1 N1 x K1, R2 K1 x N2 with N1, K1, N2 all different)."""
+    rng = np.random.default_rng(3)
+    prod = np.zeros((2, 2, 2, 2, 2))
+    prod[0, 0, 0, 0, :] = rng.standard_normal(2)
+    A0 = prod + 0.3 * rng.standard_normal(prod.shape)
+    A1 = prod + 0.3 * rng.standard_normal(prod.shape)
+    A = 0.5 * (A0 + A1)
+    A = np.asfortranarray(A / np.abs(A).max())
+    H = O.heisenberg(1.0)
+    cfg = O.default_config()
+    cfg.update(chi=16, max_iter=80, min_iter=4, rg_tol=1e-11, ad_max_iter=4)
+    Eo, go, tso = O.energy_and_grad(torch.tensor(A), H, cfg)
+    assert len({tuple(c.shape) for c in tso.Cs}) > 1
+    E, g, info = pkg.fg(A, [h.numpy() for h in H], cfg, engine=engine)
+    go = go.numpy()
+    assert abs(E - Eo) <= 1e-10, (E, Eo)
+    rel = np.linalg.norm(g - go) / np.linalg.norm(go)
+    assert rel <= 1e-6, rel
+
+
 def test_energy_grad_finite_difference(engine, pkg):
     """Directional derivatives of the GPU E+grad unit against central
     differences of the GPU energy of the same unit (step 1e-6)."""

@@ -86,3 +86,14 @@ def test_canonical_gauge_rectangular_corners():
     Qs = [np.linalg.qr(rng.standard_normal((m, m)))[0] for m in n]
     vg = ws.gauge_fix(*ws.gauge_transform(Cs, Es, Qs), r=6)
     assert np.allclose(v, vg, atol=1e-10), np.abs(v - vg).max()
+
+
+def test_energy_bound():
+    """The sanity bound a warm-started result must satisfy: |E| <= ||Hh|| + ||Hv||
+    (Heisenberg S.S: 3/4 per bond); the oracle's converged energy lies inside."""
+    ws = load_package().warmstart
+    Hh = [h.numpy() for h in O.heisenberg(1.0)]
+    assert abs(ws.energy_bound(Hh) - 1.5) < 1e-8
+    ts, H = _converged()
+    E = _energy(ts, *_env(ts), H)
+    assert abs(E) <= ws.energy_bound([h.numpy() for h in H]) and 34.0 > ws.energy_bound([h.numpy() for h in H])
