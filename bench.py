@@ -12,6 +12,7 @@ and reported beside it.
                     [--workload d4chi64|d5chi100]
     python bench.py --impl reference ...   # CPU arm (see below)
     python bench.py --forward-only 6       # profiling aid: 6 forward iterations, no timing
+    python bench.py --gemm-shapes          # FP64 DMMA GEMM vs cuBLAS on the engine's shapes
 
 Timing: K steps timed with CUDA events recorded on the engine's own stream,
 L2 flushed (512 MB write) between steps, max over ranks; value = E+grad
@@ -419,6 +420,46 @@ def run_ours(args):
     return 0
 
 
+def run_gemm_shapes():
+    """ipeps_gemm_f64 (10 products from one input upload, timed as the difference
+    of 11 and 1 products) against torch.matmul (cuBLAS DGEMM, CUDA events)."""
+    import numpy as np
+    import torch
+    pkg = load_pkg()
+    eng = pkg.Engine(0)
+    shapes = [("N", "N", 2500, 160, 2500), ("T", "N", 2500, 160, 2500), ("T", "N", 160, 160, 2500),
+              ("N", "N", 2500, 2500, 100), ("N", "N", 250000, 50, 25), ("N", "T", 4096, 4096, 4096)]
+    rng = np.random.default_rng(0)
+    for oa, ob, m, n, k in shapes:
+        A = rng.standard_normal((m, k) if oa == "N" else (k, m))
+        B = rng.standard_normal((k, n) if ob == "N" else (n, k))
+        for _ in range(2):  # the second round is the timed one
+            ts = []
+            for reps in (1, 11):
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                pkg.host.gemm_f64(oa, ob, A, B, engine=eng, reps=reps)
+                ts.append(time.perf_counter() - t0)
+        dt = (ts[1] - ts[0]) / 10
+        a, b = torch.tensor(A, device="cuda"), torch.tensor(B, device="cuda")
+        fa = (lambda x: x) if oa == "N" else (lambda x: x.T)
+        fb = (lambda x: x) if ob == "N" else (lambda x: x.T)
+        for _ in range(3):
+            fa(a) @ fb(b)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(10):
+            fa(a) @ fb(b)
+        e1.record()
+        torch.cuda.synchronize()
+        dc = e0.elapsed_time(e1) / 10 / 1e3
+        fl = 2.0 * m * n * k
+        print(json.dumps({"op": oa + ob, "m": m, "n": n, "k": k, "dmma_us": round(dt * 1e6, 1),
+                          "dmma_tflops": round(fl / dt / 1e12, 2), "cublas_us": round(dc * 1e6, 1),
+                          "cublas_tflops": round(fl / dc / 1e12, 2)}), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -432,7 +473,12 @@ def main():
     ap.add_argument("--workload", default="d4chi64", choices=sorted(WORKLOADS))
     ap.add_argument("--forward-only", type=int, default=0, metavar="ITERS",
                     help="profiling aid: run ITERS forward CTMRG iterations of the workload once, no timing")
+    ap.add_argument("--gemm-shapes", action="store_true",
+                    help="kernel aid: FP64 GEMM throughput of the engine's DMMA kernel and of cuBLAS on the "
+                         "projector's and the contractions' shapes, one JSON line per shape")
     args = ap.parse_args()
+    if args.gemm_shapes:
+        return run_gemm_shapes()
     global WORKLOAD, WORKLOAD_NAME
     WORKLOAD = WORKLOADS[args.workload]
     WORKLOAD_NAME = workload_name(WORKLOAD)
