@@ -265,7 +265,19 @@ void gemm_f64_dmma(Ctx& c, char opA, char opB, int64_t m, int64_t n, int64_t k, 
   const bool vec = (reinterpret_cast<uintptr_t>(A) % 16 == 0) && (reinterpret_cast<uintptr_t>(B) % 16 == 0) &&
                    lda % 2 == 0 && ldb % 2 == 0;
   const int64_t big_tiles = ((m + 127) / 128) * ((n + 127) / 128);
-  if (big_tiles >= c.sm_count) {
+  // one narrow side (<= 64, e.g. a leg of D^2 d = 50 in the contractions with
+  // A): 128x64 / 64x128 tiles, so that half of a 128x128 tile is not wasted
+  if (n <= 64 && ((m + 127) / 128) >= c.sm_count) {
+    if (vec)
+      launch_ops<128, 64, 4, 2, 2>(c, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+    else
+      launch_ops<128, 64, 4, 2, 1>(c, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+  } else if (m <= 64 && ((n + 127) / 128) >= c.sm_count) {
+    if (vec)
+      launch_ops<64, 128, 2, 4, 2>(c, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+    else
+      launch_ops<64, 128, 2, 4, 1>(c, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+  } else if (big_tiles >= c.sm_count) {
     if (vec)
       launch_ops<128, 128, 2, 4, 2>(c, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
     else

@@ -23,6 +23,9 @@ CASES = [
     (160, 160, 2500, 0),    # Gram matrix shape
     (1000, 1200, 100, 0),   # many output tiles (128x128 kernel)
     (1001, 1203, 101, 1),   # the same with odd sizes (odd leading dimensions)
+    (40000, 50, 25, 0),     # tall and narrow (128x64 tiles): the contractions with A
+    (40001, 49, 25, 1),     # the same, odd
+    (50, 40000, 25, 0),     # short and wide (64x128 tiles)
 ]
 
 
