@@ -502,6 +502,122 @@ std::complex<double> all_norm(Env& e, Tensor* envB) {
   return scalar_of(c, Nb) / n1;
 }
 
+namespace {
+
+// Moves the counters and timing records of `from` into `to`.
+void merge_stats(Ctx& to, Ctx& from) {
+  for (int f = 0; f < int(KFam::Count); ++f) {
+    to.stats[f].launches += from.stats[f].launches;
+    to.stats[f].flops += from.stats[f].flops;
+    to.stats[f].bytes += from.stats[f].bytes;
+    to.prof_stats[f].launches += from.prof_stats[f].launches;
+    to.prof_stats[f].flops += from.prof_stats[f].flops;
+    to.prof_stats[f].bytes += from.prof_stats[f].bytes;
+  }
+  from.stats = {};
+  from.prof_stats = {};
+  to.jacobi_sweeps += from.jacobi_sweeps;
+  to.projector_calls += from.projector_calls;
+  to.projector_extra_passes += from.projector_extra_passes;
+  from.jacobi_sweeps = from.projector_calls = from.projector_extra_passes = 0;
+  for (auto& r : from.prof_rec) to.prof_rec.push_back(r);
+  from.prof_rec.clear();
+}
+
+// The convergence value of run_ctm: get_gs_energy (mode 0) or
+// get_es_energy / get_all_norm (mode 2).
+std::complex<double> conv_value(Env& e, int conv_mode, const Tensor& Hh, const Tensor& Hv) {
+  if (conv_mode == 0) {
+    std::complex<double> E, Na;
+    gs_energy(e, Hh, Hv, &E, &Na);
+    return E;
+  }
+  return es_energy(e, Hh, Hv) / all_norm(e, nullptr);
+}
+
+// One convergence evaluation in flight on the evaluation context, from its own
+// host thread, on a snapshot of the environment after iteration `iter`.  The
+// snapshot also keeps every tensor the evaluation reads alive until finish().
+struct PendingConv {
+  Env& e;
+  int conv_mode;
+  const Tensor& Hh;
+  const Tensor& Hv;
+  bool active = false;
+  std::thread th;
+  std::complex<double> val;
+  std::exception_ptr err;
+  Env snap;
+  std::vector<double> s;
+  uint64_t rng1 = 0, rng2 = 0;
+  int iter = 0;
+
+  PendingConv(Env& env, int mode, const Tensor& hh, const Tensor& hv) : e(env), conv_mode(mode), Hh(hh), Hv(hv) {}
+  ~PendingConv() {
+    if (th.joinable()) th.join();
+  }
+  void launch(int it, const std::vector<double>& sp) {
+    Ctx& c1 = *e.ctx;
+    if (!e.aux_eval) e.aux_eval = std::make_shared<Ctx>(c1.device);
+    Ctx& c3 = *e.aux_eval;
+    c3.prof = c1.prof;
+    snap = e;
+    s = sp;
+    iter = it;
+    err = nullptr;
+    rng1 = c1.rng_counter;
+    rng2 = e.aux ? e.aux->rng_counter : 0;
+    Env ev = e;
+    ev.ctx = &c3;
+    ev.aux.reset();
+    ev.aux_eval.reset();
+    cudaEvent_t ev0 = c1.take_event();
+    IPEPS_CUDA(cudaEventRecord(ev0, c1.stream));
+    IPEPS_CUDA(cudaStreamWaitEvent(c3.stream, ev0, 0));
+    c1.ev_pool.push_back(ev0);
+    active = true;
+    th = std::thread([this, &c3, ev]() mutable {
+      try {
+        IPEPS_CUDA(cudaSetDevice(c3.device));
+        val = conv_value(ev, conv_mode, Hh, Hv);
+      } catch (...) {
+        err = std::current_exception();
+      }
+    });
+  }
+  std::complex<double> finish() {
+    Ctx& c1 = *e.ctx;
+    Ctx& c3 = *e.aux_eval;
+    th.join();
+    active = false;
+    // later frees of the snapshot's buffers (main stream) follow the evaluation's reads
+    cudaEvent_t ev1 = c1.take_event();
+    IPEPS_CUDA(cudaEventRecord(ev1, c3.stream));
+    IPEPS_CUDA(cudaStreamWaitEvent(c1.stream, ev1, 0));
+    c1.ev_pool.push_back(ev1);
+    merge_stats(c1, c3);
+    if (err) std::rethrow_exception(err);
+    return val;
+  }
+  // back to the environment the evaluation saw (drops a speculative iteration)
+  void roll_back() {
+    e.Cs = snap.Cs;
+    e.Es = snap.Es;
+    e.B_Cs = snap.B_Cs;
+    e.Bd_Cs = snap.Bd_Cs;
+    e.BB_Cs = snap.BB_Cs;
+    e.B_Es = snap.B_Es;
+    e.Bd_Es = snap.Bd_Es;
+    e.BB_Es = snap.BB_Es;
+    for (int d = 0; d < 4; ++d) e.cache[d] = snap.cache[d];
+    e.last_s = snap.last_s;
+    e.ctx->rng_counter = rng1;
+    if (e.aux) e.aux->rng_counter = rng2;
+  }
+};
+
+}  // namespace
+
 // ctmrg.jl:1-55
 int run_ctm(Env& e, int conv_mode, const Tensor* Hh, const Tensor* Hv, double* last_diff, bool* converged) {
   std::vector<double> diffs{1.0};
@@ -525,6 +641,38 @@ int run_ctm(Env& e, int conv_mode, const Tensor* Hh, const Tensor* Hv, double* l
     int p;
     ~Restore() { c.precision = p; }
   } restore{c, prec0};
+  if ((conv_mode == 0 || conv_mode == 2) && !polish && e.parallel_moves) {
+    // Pipelined: the energy of iteration i is evaluated while iteration i+1
+    // runs.  When iteration i turns out converged, iteration i+1 is rolled
+    // back, so the returned environment and log are those of the sequential loop.
+    PendingConv pc(e, conv_mode, *Hh, *Hv);
+    auto record = [&](std::complex<double> v) {
+      const std::complex<double> old = conv;
+      conv = v;
+      diffs.push_back(std::abs(conv - old));
+      CtmLogEntry le{pc.iter, diffs.back(), conv.real(), conv.imag(), int(pc.s.size())};
+      e.log.push_back(le);
+      return pc.iter >= e.prm.min_iter && diffs.back() < e.prm.rg_tol;
+    };
+    int last = 0;
+    for (; i <= e.prm.max_iter; ++i) {
+      std::vector<double> s = rg_step(e);
+      if (pc.active && record(pc.finish())) {
+        pc.roll_back();
+        done = true;
+        last = pc.iter;
+        break;
+      }
+      pc.launch(i, s);
+    }
+    if (!done && pc.active) {
+      done = record(pc.finish());
+      last = pc.iter;
+    }
+    if (last_diff) *last_diff = diffs.back();
+    if (converged) *converged = done;
+    return done ? last : e.prm.max_iter;
+  }
   for (; i <= e.prm.max_iter; ++i) {
     if (polish && c.precision != kPrecFP64 && (i >= polish_start || diffs.back() < e.prm.polish_tol))
       c.precision = kPrecFP64;

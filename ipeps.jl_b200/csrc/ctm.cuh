@@ -67,6 +67,11 @@ struct Env {
   // context with its own stream (created on first use).
   bool parallel_moves = true;
   std::shared_ptr<Ctx> aux;
+  // run_ctm evaluates the convergence criterion of iteration i on `aux_eval`
+  // (a third stream, its own host thread) while iteration i+1 runs; a
+  // speculative iteration after convergence is rolled back (FP64 form,
+  // energy criteria; on with parallel_moves)
+  std::shared_ptr<Ctx> aux_eval;
 
   NT all_A() const;
   NT all_Ad() const;
