@@ -4,6 +4,7 @@
 #include "ctx.cuh"
 
 #include <algorithm>
+#include <atomic>
 #include <numeric>
 
 namespace ipeps {
@@ -21,14 +22,30 @@ Ctx::Ctx(int dev) : device(dev) {
   sh->device = dev;
   IPEPS_CUDA(cudaStreamCreateWithFlags(&sh->s, cudaStreamNonBlocking));
   stream = sh->s;
-  cudaDeviceProp prop;
-  IPEPS_CUDA(cudaGetDeviceProperties(&prop, dev));
-  sm_count = prop.multiProcessorCount;
+  IPEPS_CUDA(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, dev));
   // keep freed blocks in the pool (no release back to the driver)
   cudaMemPool_t pool;
   IPEPS_CUDA(cudaDeviceGetDefaultMemPool(&pool, dev));
   uint64_t thr = UINT64_MAX;
   IPEPS_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+  // Once per device: grow the pool by a block of min(8 GiB, a quarter of the
+  // free memory) and hand it back, so that steady-state allocations (up to a
+  // few GB at D=5 chi=100, from up to three streams) are served from reserved
+  // memory instead of mapping new memory in the middle of a CTMRG step.
+  static std::atomic<bool> reserved[64];
+  if (dev >= 0 && dev < 64 && !reserved[dev].exchange(true)) {
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
+      const size_t want = std::min<size_t>(size_t(8) << 30, free_b / 4);
+      void* p = nullptr;
+      if (want > 0 && cudaMallocAsync(&p, want, stream) == cudaSuccess) {
+        IPEPS_CUDA(cudaFreeAsync(p, stream));
+        IPEPS_CUDA(cudaStreamSynchronize(stream));
+      } else {
+        (void)cudaGetLastError();  // not fatal: the pool then grows on demand
+      }
+    }
+  }
   scal = std::make_shared<DBuf>(4096, sh);
   IPEPS_CUDA(cudaMemsetAsync(scal->p, 0, 4096, stream));
   d_status = reinterpret_cast<int*>(static_cast<char*>(scal->p) + 4000);
