@@ -277,6 +277,14 @@ void gemm_f64_dmma(Ctx& c, char opA, char opB, int64_t m, int64_t n, int64_t k, 
       launch_ops<64, 128, 2, 4, 2>(c, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
     else
       launch_ops<64, 128, 2, 4, 1>(c, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+  } else if (k <= 256 && ((m + 127) / 128) * ((n + 63) / 64) >= 2 * c.sm_count) {
+    // short K (e.g. a bond of chi = 100): the 128x64 tiles hold two CTAs per SM
+    // (<= 128 registers, 92 KB of shared memory), which hides the load latency
+    // of the few K steps better than one 128x128 CTA
+    if (vec)
+      launch_ops<128, 64, 4, 2, 2>(c, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+    else
+      launch_ops<128, 64, 4, 2, 1>(c, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
   } else if (big_tiles >= c.sm_count) {
     if (vec)
       launch_ops<128, 128, 2, 4, 2>(c, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
