@@ -282,6 +282,14 @@ ProjResult projector_impl(Ctx& c, Ops& o, int chi, const SvdParams& sp, ProjCach
   int q = (k == Nmin) ? 0 : (warm ? sp.power_iters_warm : sp.power_iters);
   int inter = sp.inter_passes;
   if (!warm || !cache || cache->cutoff_limited) inter = std::max(inter, 3);
+  // power iterations this direction's recent calls needed beyond q (each
+  // extra pass below costs a Rayleigh-Ritz step, two sCholQR3 and a Jacobi SVD
+  // on top of its power iteration; doing the iterations up front is cheaper).
+  // Only with sCholQR3 intermediates: a single shifted pass drops directions
+  // below ~sqrt(shift) s_1 at every iteration, so more iterations would lose them.
+  const bool adapt = q > 0 && cache && inter >= 3;
+  if (adapt) q += cache->qbonus;
+  int extra = 0;
 
   ProjResult r;
   r.k = k;
@@ -352,6 +360,7 @@ ProjResult projector_impl(Ctx& c, Ops& o, int chi, const SvdParams& sp, ProjCach
     Om = Vk;
     q = 1;
     c.projector_extra_passes++;
+    ++extra;
   }
   r.sweeps = sk.sweeps;
   c.projector_calls++;
@@ -374,6 +383,8 @@ ProjResult projector_impl(Ctx& c, Ops& o, int chi, const SvdParams& sp, ProjCach
     cache->Vold = cache->V;
     cache->V = Vc;
     cache->cutoff_limited = n_above_last < new_chi;
+    if (adapt)
+      cache->qbonus = extra > 0 ? std::min(cache->qbonus + extra, sp.max_extra_passes) : std::max(cache->qbonus - 1, 0);
   }
   if (keep_factors) {
     IPEPS_CHECK(dt == DType::F64, "get_projector: the projector adjoint is real-only");

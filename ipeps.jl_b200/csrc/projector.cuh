@@ -43,6 +43,9 @@ struct ProjCache {
   // the last truncation of this direction was set by the 1e-12 cutoff rather
   // than by chi: the next sketch keeps its small directions (sCholQR3 throughout)
   bool cutoff_limited = true;
+  // power iterations added to the next call's sketch: raised by the extra
+  // passes a call needed, lowered by one after a call that needed none
+  int qbonus = 0;
   const Tensor& seed(bool older) const { return (older && !Vold.empty()) ? Vold : V; }
 };
 
