@@ -641,22 +641,30 @@ int run_ctm(Env& e, int conv_mode, const Tensor* Hh, const Tensor* Hv, double* l
     int p;
     ~Restore() { c.precision = p; }
   } restore{c, prec0};
-  if ((conv_mode == 0 || conv_mode == 2) && !polish && e.parallel_moves) {
+  if ((conv_mode == 0 || conv_mode == 2) && e.parallel_moves) {
     // Pipelined: the energy of iteration i is evaluated while iteration i+1
     // runs.  When iteration i turns out converged, iteration i+1 is rolled
-    // back, so the returned environment and log are those of the sequential loop.
+    // back, so the returned environment and log are those of the sequential
+    // loop.  In the mixed form the switch to FP64 sees the change per
+    // iteration one iteration later than the sequential loop does.
     PendingConv pc(e, conv_mode, *Hh, *Hv);
+    std::vector<int> fp64_upto(size_t(std::max(e.prm.max_iter, 0)) + 2, 0);
     auto record = [&](std::complex<double> v) {
       const std::complex<double> old = conv;
       conv = v;
       diffs.push_back(std::abs(conv - old));
       CtmLogEntry le{pc.iter, diffs.back(), conv.real(), conv.imag(), int(pc.s.size())};
       e.log.push_back(le);
-      return pc.iter >= e.prm.min_iter && diffs.back() < e.prm.rg_tol;
+      return pc.iter >= e.prm.min_iter && diffs.back() < e.prm.rg_tol &&
+             (!polish || fp64_upto[pc.iter] >= e.prm.polish_iters);
     };
     int last = 0;
     for (; i <= e.prm.max_iter; ++i) {
+      if (polish && c.precision != kPrecFP64 && (i >= polish_start || diffs.back() < e.prm.polish_tol))
+        c.precision = kPrecFP64;
       std::vector<double> s = rg_step(e);
+      if (polish && c.precision == kPrecFP64) fp64_done++;
+      fp64_upto[i] = fp64_done;
       if (pc.active && record(pc.finish())) {
         pc.roll_back();
         done = true;
