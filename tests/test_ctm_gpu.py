@@ -155,9 +155,12 @@ def test_nested_energy_and_norm(engine, pkg):
     assert np.allclose(envB, npa(envBo), rtol=1e-8, atol=1e-10 * np.abs(npa(envBo)).max())
 
 
-def test_bench_workload_trajectory(engine, pkg):
+@pytest.mark.parametrize("parallel", [True, False])
+def test_bench_workload_trajectory(engine, pkg, parallel):
     """The bench workload (Heisenberg D=4 chi=64, 30 iterations): every
-    per-iteration energy against the oracle's, |dE| <= 1e-10."""
+    per-iteration energy against the oracle's, |dE| <= 1e-10, with the moves
+    in concurrent pairs and the energies overlapped (default) and with the
+    four moves and the energies in order."""
     with open(os.path.join(GOLD, "bench_workload.json")) as f:
         g = json.load(f)
     rng = np.random.default_rng(g["seed"])
@@ -166,7 +169,7 @@ def test_bench_workload_trajectory(engine, pkg):
     A = np.asfortranarray(A / np.abs(A).max())
     H = [npa(h) for h in O.heisenberg(1.0)]
     cfg = pkg.default_config()
-    cfg.update(chi=chi, min_iter=30, max_iter=30, rg_tol=0.0)
+    cfg.update(chi=chi, min_iter=30, max_iter=30, rg_tol=0.0, parallel_moves=parallel)
     ts = pkg.CTMTensors(A, cfg, engine=engine)
     ts, info = pkg.run_ctm(ts, conv_fun="energy", H=H)
     got = [l["obj"].real for l in info["log"]]
@@ -190,6 +193,35 @@ def test_d5_chi100_trajectory(engine, pkg):
     err = max(abs(a - b) for a, b in zip(traj, gold["energies"]))
     assert err <= 1e-10, err
     ts.close()
+
+
+@pytest.mark.parametrize("idx", [0, 3])
+def test_early_exit_matches_sequential_loop(engine, pkg, idx):
+    """run_ctm with the convergence test overlapped (the energy of iteration i
+    evaluated while iteration i+1 runs, the speculative iteration rolled back on
+    convergence) stops at the same iteration with the same log and environment
+    shapes as the loop that evaluates every energy in order."""
+    with open(os.path.join(GOLD, "ctm_energies.json")) as f:
+        case = json.load(f)["cases"][idx]
+    A = npa(O.random_A(case["D"], case["d"], seed=case["seed"]))
+    H = O.ising(case["h"]) if case["model"] == "ising" else O.heisenberg(case["Jz"])
+    H = [npa(h) for h in H]
+    runs = []
+    for parallel in (True, False):
+        cfg = O.default_config()
+        cfg.update(chi=case["chi"], min_iter=case["min_iter"], max_iter=case["max_iter"], rg_tol=case["rg_tol"],
+                   parallel_moves=parallel)
+        ts = pkg.CTMTensors(A, cfg, engine=engine)
+        ts, info = pkg.run_ctm(ts, conv_fun="energy", H=H)
+        E = pkg.get_gs_energy(ts, H)[0].real
+        runs.append((info, E, [c.shape for c in ts.Cs]))
+        ts.close()
+    (i1, E1, s1), (i2, E2, s2) = runs
+    assert i1["converged"] and i2["converged"]
+    assert i1["iters"] == i2["iters"] == len(i1["log"]), (i1["iters"], i2["iters"], len(i1["log"]))
+    assert s1 == s2
+    assert abs(E1 - E2) <= 1e-10 and abs(E1 - case["E"]) <= 1e-10, (E1, E2, case["E"])
+    assert abs(i1["log"][-1]["obj"].real - E1) <= 1e-12
 
 
 def test_degenerate_rule_keeps_zero_singular_value(engine, pkg):
