@@ -61,6 +61,9 @@ function push_params!(ts::CTMTensorsB200)
     check(ts.eng.h, ccall((:ipeps_env_set_params, lib), Cint, (Ptr{Cvoid}, Cint, Cint, Cint, Cint, Float64),
                           ts.h, get(p, "chi", 30), get(p, "min_iter", 4), get(p, "max_iter", 20),
                           get(p, "ad_max_iter", 4), get(p, "rg_tol", 1e-6)))
+    # left/right and top/bottom moves on two streams (key absent: on)
+    check(ts.eng.h, ccall((:ipeps_env_set_parallel, lib), Cint, (Ptr{Cvoid}, Cint),
+                          ts.h, get(p, "parallel_moves", true) ? 1 : 0))
 end
 
 """`CTMTensors(A, cfg)` (ctm_tensor.jl:63-69): Ad = conj(A), init_ctm1 on the device."""
