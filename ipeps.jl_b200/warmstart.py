@@ -3,10 +3,11 @@ always starts from init_ctm1, ctm_tensor.jl:97-130).
 
 A small network (host.Mlp: BF16 tensor-core GEMMs, FP32 parameters) maps the
 flattened iPEPS tensor A to a rank-r environment in a canonical gauge; CTMRG
-then iterates from that environment to rg_tol.  Plain CTMRG stays the judge
-and the fallback: a warm start that has not converged by max_iter is dropped
-and the run restarts from init_ctm1, so the converged energy is always the one
-plain CTMRG reaches.
+then iterates from that environment to rg_tol.  Plain CTMRG stays the arbiter
+and the fallback: a warm start that has not converged within its iteration
+budget, or that converged outside the energy bound of H (a spurious fixed
+point), is dropped and the run restarts from init_ctm1.  The tests compare the
+warm-started energies with plain CTMRG's.
 
 Canonical gauge.  With a one-site unit cell an environment has four bond
 gauges, one per boundary (top, right, bottom, left), each an invertible
@@ -195,7 +196,7 @@ def energy_bound(H) -> float:
 
 
 def converge_default(A, H, cfg: Dict[str, Any], engine=None):
-    """Plain CTMRG from init_ctm1 with the energy criterion (the judge)."""
+    """Plain CTMRG from init_ctm1 with the energy criterion (the arbiter)."""
     ts = host.CTMTensors(A, cfg, engine=engine)
     ts, info = host.run_ctm(ts, conv_fun="energy", H=H)
     return ts, info
