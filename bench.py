@@ -1,18 +1,26 @@
 """Benchmark of the CTMRG hot path on B200.
 
 Workload (default): spin-1/2 Heisenberg (sublattice-rotated), single-site
-iPEPS A of shape (4,4,4,4,2), i.i.d. N(0,1) seeded, max|A| = 1, chi = 64.
-One step = one energy+gradient evaluation (fg! of optim_gs): init_ctm1, 30
-CTMRG iterations (4 directional moves each) with the energy every iteration
-(the reference's conv_fun), then the pullback of ad_max_iter = 4 further
-iterations + the energy.  CTMRG moves/s is measured on the forward part alone
-and reported beside it.
+iPEPS A of shape (5,5,5,5,2), i.i.d. N(0,1) seeded, max|A| = 1, chi = 100
+(enlarged-corner matrices 2500 x 2500).  One step = one energy+gradient
+evaluation (fg! of optim_gs): init_ctm1, 30 CTMRG iterations (4 directional
+moves each) with the energy every iteration (the reference's conv_fun), then
+the pullback of ad_max_iter = 4 further iterations + the energy.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|mixed]
-                    [--workload d4chi64|d5chi100]
+By default both forms run on the same input: the mixed form (3xTF32
+contractions on the tensor cores, FP64 projector / normalisation / final
+energy) gives ``value``; the plain FP64 form is timed beside it
+(``fp64``), with the ratio and the mixed form's energy and gradient errors
+against the FP64 form and the 30-iteration energy against the oracle's
+(tests/golden/d5_chi100_30.json).  CTMRG moves/s is measured on the forward
+part alone and reported beside it.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision both|fp64|mixed]
+                    [--workload d5chi100|d4chi64]
     python bench.py --impl reference ...   # CPU arm (see below)
     python bench.py --forward-only 6       # profiling aid: 6 forward iterations, no timing
     python bench.py --gemm-shapes          # FP64 DMMA GEMM vs cuBLAS on the engine's shapes
+    python bench.py --tf32-shapes          # 3xTF32 tcgen05 GEMM on the engine's shapes
 
 Timing: K steps timed with CUDA events recorded on the engine's own stream,
 L2 flushed (512 MB write) between steps, max over ranks; value = E+grad
@@ -24,8 +32,12 @@ with no data-parallel split, so N GPUs run N independent evaluations.
 
 Reference arm: the reference is Julia, which is not installed, so
 ``--impl reference`` times the CPU FP64 oracle (a restatement of the
-reference's algorithm) on the host cores, on a bounded sample of the same
-workload.  It is the CPU baseline, not a target.
+reference's algorithm) on the host cores.  Each of its steps is one forward
+CTMRG iteration (with the energy) of the same workload, timed as it runs;
+one pullback iteration is timed after them, and the evaluations/s value is
+derived from those two times (30 forward + 4 pullback iterations per
+evaluation), as the line's ``value_derivation`` states.  It is the CPU
+baseline, not a target.
 """
 from __future__ import annotations
 
@@ -82,12 +94,13 @@ def heisenberg(Jz=1.0):
 
 
 WORKLOADS = {
-    # the headline configuration: Heisenberg D=4 chi=64, 30 CTMRG iterations
-    "d4chi64": dict(model="heisenberg", D=4, d=2, chi=64, iters=30, ad_iters=4),
-    # the larger configuration (enlarged corners 2500 x 2500)
-    "d5chi100": dict(model="heisenberg", D=5, d=2, chi=100, iters=30, ad_iters=4),
+    # the headline configuration: Heisenberg D=5 chi=100 (enlarged corners 2500 x 2500), 30 CTMRG iterations
+    "d5chi100": dict(model="heisenberg", D=5, d=2, chi=100, iters=30, ad_iters=4,
+                     golden="d5_chi100_30.json"),
+    # the smaller configuration (enlarged corners 1024 x 1024)
+    "d4chi64": dict(model="heisenberg", D=4, d=2, chi=64, iters=30, ad_iters=4, golden="config2.json"),
 }
-WORKLOAD = WORKLOADS["d4chi64"]
+WORKLOAD = WORKLOADS["d5chi100"]
 
 
 def workload_name(w):
@@ -194,39 +207,57 @@ def measure_fp64_peak(torch):
     return 2.0 * n ** 3 / best / 1e12
 
 
-def cpu_oracle_eg_sample(D, d, chi, seed, budget_s=12.0, threads=None):
-    """CPU oracle on a bounded sample of the workload.  Times (a) forward CTMRG
-    iterations with the energy (~budget_s) and (b) the pullback of one CTMRG
-    iteration + the energy (torch autograd with the reference's svd_back), and
-    extrapolates one E+grad evaluation = iters forward + ad_iters pullback
-    iterations.  Returns (evals/s, moves/s, sample description, threads)."""
+def _oracle(threads):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import torch
     import ipeps_oracle as O
     if threads:
         torch.set_num_threads(threads)
+    return torch, O
+
+
+def _oracle_workload(O, torch, seed):
+    D, d, chi = WORKLOAD["D"], WORKLOAD["d"], WORKLOAD["chi"]
     A = torch.tensor(random_A(D, d, seed))
     H = O.heisenberg(1.0)
     cfg = O.default_config()
     cfg.update(chi=chi, min_iter=1, max_iter=1, rg_tol=0.0, ad_max_iter=1)
-    ts = O.make_ctm_tensors(A, cfg)
-    for _ in range(2):  # first iterations have small chi
-        ts, _ = O.rg_step(ts, chi)
-    t0 = time.perf_counter()
-    it = 0
-    while True:
-        ts, _ = O.rg_step(ts, chi)
-        O.get_gs_energy(ts, H)
-        it += 1
-        if time.perf_counter() - t0 > budget_s:
-            break
-    t_iter = (time.perf_counter() - t0) / it
+    return A, H, cfg
+
+
+def _oracle_pullback_iter(O, torch, ts, A, H):
+    """One pullback iteration of run_gs (ad_max_iter = 1) + the energy, timed."""
     ts1 = O._detach_ts(ts)
     xv = A.clone().requires_grad_(True)
     t0 = time.perf_counter()
     y = O.run_gs(ts1, H, xv)
     torch.autograd.grad(y.real, xv)
-    t_ad = time.perf_counter() - t0
+    return time.perf_counter() - t0
+
+
+def cpu_oracle_eg_sample(seed, budget_s=12.0, threads=None):
+    """CPU oracle on a bounded sample of the workload.  Times (a) forward CTMRG
+    iterations with the energy (~budget_s) and (b) the pullback of one CTMRG
+    iteration + the energy (torch autograd with the reference's svd_back), and
+    scales to one E+grad evaluation = iters forward + ad_iters pullback
+    iterations.  Returns (evals/s, moves/s, sample description, threads)."""
+    torch, O = _oracle(threads)
+    A, H, cfg = _oracle_workload(O, torch, seed)
+    ts = O.make_ctm_tensors(A, cfg)
+    chi = WORKLOAD["chi"]
+    with torch.no_grad():
+        for _ in range(2):  # first iterations have small chi
+            ts, _ = O.rg_step(ts, chi)
+        t0 = time.perf_counter()
+        it = 0
+        while True:
+            ts, _ = O.rg_step(ts, chi)
+            O.get_gs_energy(ts, H)
+            it += 1
+            if time.perf_counter() - t0 > budget_s:
+                break
+    t_iter = (time.perf_counter() - t0) / it
+    t_ad = _oracle_pullback_iter(O, torch, ts, A, H)
     t_eval = WORKLOAD["iters"] * t_iter + WORKLOAD["ad_iters"] * t_ad
     sample = (f"CPU oracle (torch float64, {torch.get_num_threads()} threads): {it} forward iterations "
               f"({t_iter:.2f} s each) and one pullback iteration ({t_ad:.1f} s) timed; one E+grad evaluation = "
@@ -236,34 +267,69 @@ def cpu_oracle_eg_sample(D, d, chi, seed, budget_s=12.0, threads=None):
 
 # ---------------------------------------------------------------- arms
 def run_reference(args):
+    """CPU arm: the oracle restatement of the reference on the host cores.
+
+    Warm-up steps are forward iterations from init_ctm1 (the environment grows
+    to chi); each timed step is one forward CTMRG iteration + energy of the
+    same workload, and ms_per_step is their measured mean.  One pullback
+    iteration is timed after the steps.  The evaluations/s value is derived
+    from the two measured times (value_derivation)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     D, d, chi = WORKLOAD["D"], WORKLOAD["d"], WORKLOAD["chi"]
     threads = os.cpu_count() or 1
-    vals, moves, ts = [], [], []
-    sample = ""
-    for i in range(args.warmup + args.steps):
-        v, mv, sample, nth, t_eval = cpu_oracle_eg_sample(D, d, chi, seed=1000, budget_s=args.ref_budget,
-                                                          threads=threads)
-        if i >= args.warmup:
-            vals.append(v)
-            moves.append(mv)
-            ts.append(t_eval)
-    value = len(ts) / sum(ts)
-    line = {"impl": "reference", "metric": "E+grad evals/s (Heisenberg D=%d chi=%d); CTMRG moves/s in moves_per_s"
-            % (D, chi), "value": value,
+    t_start = time.perf_counter()
+    torch, O = _oracle(threads)
+    A, H, cfg = _oracle_workload(O, torch, seed=1000)
+    ts = O.make_ctm_tensors(A, cfg)
+    step_s = []
+    with torch.no_grad():
+        for i in range(max(args.warmup, 2) + args.steps):
+            t0 = time.perf_counter()
+            ts, _ = O.rg_step(ts, chi)
+            O.get_gs_energy(ts, H)
+            if i >= max(args.warmup, 2):
+                step_s.append(time.perf_counter() - t0)
+    t_iter = statistics.mean(step_s)
+    t_ad = _oracle_pullback_iter(O, torch, ts, A, H)
+    t_eval = WORKLOAD["iters"] * t_iter + WORKLOAD["ad_iters"] * t_ad
+    value = 1.0 / t_eval
+    sample = (f"CPU oracle (torch float64, {torch.get_num_threads()} threads): {len(step_s)} forward iterations "
+              f"timed as the steps ({t_iter:.2f} s each) and one pullback iteration ({t_ad:.1f} s)")
+    line = {"impl": "reference", "metric": metric_name(), "value": value,
             "unit": "evals/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 1e3 * sum(ts) / max(len(ts), 1), "higher_is_better": True, "scaling": "weak",
+            "ms_per_step": 1e3 * t_iter, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD_NAME, "D": D, "chi": chi, "sample": "bounded CPU sample, see cpu_baseline"},
-            "moves_per_s": statistics.mean(moves),
-            "cpu_baseline": {"value": value, "unit": "evals/s", "cores": nth, "kind": "port", "sample": sample},
+            "config": {"workload": WORKLOAD_NAME, "D": D, "chi": chi,
+                       "step": "one forward CTMRG iteration + energy of the workload (bounded CPU sample)"},
+            "value_derivation": {"formula": "1 / (%d x forward iteration + %d x pullback iteration)"
+                                 % (WORKLOAD["iters"], WORKLOAD["ad_iters"]),
+                                 "forward_iteration_s": t_iter, "pullback_iteration_s": t_ad,
+                                 "one_evaluation_s": t_eval, "extrapolated": True},
+            "moves_per_s": 4.0 / t_iter,
+            "cpu_baseline": {"value": value, "unit": "evals/s", "cores": torch.get_num_threads(), "kind": "port",
+                             "sample": sample},
             "e2e": {"value": value, "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "wall_s": time.perf_counter() - t_start,
             "reference_note": "iPEPS.jl is Julia; no Julia toolchain on this machine, so the CPU arm is the "
                               "oracle restatement of its algorithm"}
     print(json.dumps(line))
     return 0
+
+
+def metric_name():
+    return ("E+grad evals/s, mixed form (3xTF32 contractions) with the plain FP64 form beside it "
+            "(Heisenberg D=%d chi=%d); CTMRG moves/s in moves_per_s" % (WORKLOAD["D"], WORKLOAD["chi"]))
+
+
+def golden_energies():
+    p = os.path.join(ROOT, "tests", "golden", WORKLOAD["golden"])
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        g = json.load(f)
+    return g.get("energies")
 
 
 def run_ours(args):
@@ -279,15 +345,50 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
 
     pkg = load_pkg()
-    eng = pkg.Engine(local, precision=args.precision)
+    forms = ["mixed", "fp64"] if args.precision == "both" else [args.precision]
     D, d, chi, iters, ad_iters = (WORKLOAD[k] for k in ("D", "d", "chi", "iters", "ad_iters"))
     cfg = workload_cfg(pkg, chi, iters, ad_iters)
     H = heisenberg(1.0)
     A = random_A(D, d, seed=1000 + rank)
     moves_per_fwd = 4 * iters
-
-    ext = torch.cuda.ExternalStream(eng.stream_ptr())
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    class Form:
+        """one precision form: its engine (own CUDA stream) and environment"""
+
+        def __init__(self, name):
+            self.name = name
+            self.eng = pkg.Engine(local, precision=name)
+            self.ext = torch.cuda.ExternalStream(self.eng.stream_ptr())
+            self.ts = pkg.CTMTensors(A, cfg, engine=self.eng)
+            self.last = None
+
+        def forward(self):
+            # inputs resident: A already on the device; re-initialise and iterate
+            self.eng.check(self.eng.lib.ipeps_env_init(self.ts.h))
+            _, info = pkg.run_ctm(self.ts, conv_fun="energy", H=H)
+            return info
+
+        def step(self):
+            info = self.forward()
+            E, g = pkg.energy_grad(self.ts, H, ad_iters)
+            self.last = (info["log"][-1]["obj"].real, E, g)
+
+        def e2e(self):
+            pkg.fg(A, H, cfg, engine=self.eng)
+
+        def timed(self, fn, k):
+            times = []
+            for _ in range(k):
+                flush.zero_()
+                torch.cuda.synchronize()
+                s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                s.record(self.ext)
+                fn()
+                e.record(self.ext)
+                e.synchronize()
+                times.append(s.elapsed_time(e) / 1e3)
+            return times
 
     def barrier():
         if world > 1:
@@ -303,117 +404,133 @@ def run_ours(args):
 
     if args.forward_only > 0:
         cfg.update(min_iter=args.forward_only, max_iter=args.forward_only)
-        tsf = pkg.CTMTensors(A, cfg, engine=eng)
-        tsf, info = pkg.run_ctm(tsf, conv_fun="energy", H=H)
+        f = Form(forms[0])
+        info = f.forward()
         if rank == 0:
-            print(json.dumps({"forward_only": args.forward_only, "workload": WORKLOAD_NAME,
+            print(json.dumps({"forward_only": args.forward_only, "workload": WORKLOAD_NAME, "precision": forms[0],
                               "energy": info["log"][-1]["obj"].real}))
-        tsf.close()
+        f.ts.close()
         return 0
 
-    ts = pkg.CTMTensors(A, cfg, engine=eng)
+    fm = {n: Form(n) for n in forms}
+    main = fm[forms[0]]
 
-    def forward_step():
-        # inputs resident: A already on the device; re-initialise and iterate
-        eng.check(eng.lib.ipeps_env_init(ts.h))
-        pkg.run_ctm(ts, conv_fun="energy", H=H)
-
-    def device_step():
-        forward_step()
-        return pkg.energy_grad(ts, H, ad_iters)
-
-    def timed(fn, k):
-        times = []
-        for _ in range(k):
-            flush.zero_()
-            torch.cuda.synchronize()
-            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            s.record(ext)
-            fn()
-            e.record(ext)
-            e.synchronize()
-            times.append(s.elapsed_time(e) / 1e3)
-        return times
-
+    # ---- timed region of the headline form: K E+grad evaluations, events on the engine stream,
+    # L2 flushed between steps, clocks sampled meanwhile
     for _ in range(args.warmup):
-        device_step()
+        main.step()
     barrier()
-
-    # ---- timed region: K E+grad evaluations, events on the engine stream, L2 flushed between steps
-    eng.reset_stats()
+    main.eng.reset_stats()
     sampler = ClockSampler(local)
     sampler.start()
-    times = timed(device_step, args.steps)
+    times = main.timed(main.step, args.steps)
     barrier()
     clocks = sampler.stop()
-    st = eng.stats()
+    st = main.eng.stats()
     launches = sum(f["launches"] for f in st["families"].values())
     t_max = max_over_ranks(sum(times))
     value = args.steps * world / t_max
 
-    # ---- forward only: CTMRG moves/s on the same workload
-    tf = max_over_ranks(sum(timed(forward_step, args.steps)))
-    moves_value = moves_per_fwd * args.steps * world / tf
+    # ---- side measurements on min(K, 5) steps: the other form, forward-only moves/s, e2e
+    ks = max(1, min(args.steps, 5))
+    side = {}
+    for n in forms[1:]:
+        f = fm[n]
+        for _ in range(min(args.warmup, 3)):
+            f.step()
+        barrier()
+        side[n] = ks * world / max_over_ranks(sum(f.timed(f.step, ks)))
+    moves = {}
+    for n in forms:
+        f = fm[n]
+        moves[n] = moves_per_fwd * ks * world / max_over_ranks(sum(f.timed(f.forward, ks)))
 
-    # ---- e2e: public API with host buffers (A, H in; energy, gradient out) each step
-    def e2e_step():
-        pkg.fg(A, H, cfg, engine=eng)
-
-    te = max_over_ranks(sum(timed(e2e_step, max(1, args.steps))))
-    e2e_value = max(1, args.steps) * world / te
+    # e2e: public API with host buffers (A, H in; energy, gradient out) each step
+    te = max_over_ranks(sum(main.timed(main.e2e, ks)))
+    e2e_value = ks * world / te
     h2d = A.nbytes + 2 * H[0].nbytes * 2   # A, and H for the run and for the gradient call
     d2h = A.nbytes + 8 + 32 * iters        # gradient, energy, per-iteration log
     barrier()
 
-    # ---- live per-kernel profile of one E+grad step (events around each launch)
-    eng.prof_enable(True)
-    device_step()
-    prof = eng.prof_query()
-    eng.prof_enable(False)
+    # ---- live per-kernel-family profile of one E+grad step of each form (events around each launch)
+    prof = {}
+    for n in forms:
+        f = fm[n]
+        f.eng.prof_enable(True)
+        f.step()
+        prof[n] = f.eng.prof_query()
+        f.eng.prof_enable(False)
 
     if rank == 0:
         peaks, peak_kind = measured_peaks()
         fp64_peak = measure_fp64_peak(torch)
-        total_ms = sum(f["ms"] for f in prof.values())
-        dom = max(prof.items(), key=lambda kv: kv[1]["ms"])
-        gname = "gemm_f64" if args.precision == "fp64" else "gemm_tf32x3"
-        g = prof[gname]
-        achieved = g["flops"] / (g["ms"] / 1e3) / 1e12 if g["ms"] > 0 else 0.0
-        if args.precision == "fp64":
-            peak, peak_note = fp64_peak, "cuBLAS DGEMM 8192^3 measured in this run (FP64 has no entry in MEASURED_PEAKS.json)"
-        else:
-            peak, peak_note = peaks["bf16_tflops"] / 2 / 3, f"{peak_kind} bf16 / 2 (TF32) / 3 (three products)"
+
+        def roofline(n):
+            pr = prof[n]
+            total_ms = sum(v["ms"] for v in pr.values())
+            gname = "gemm_f64" if n == "fp64" else "gemm_tf32x3"
+            g = pr[gname]
+            achieved = g["flops"] / (g["ms"] / 1e3) / 1e12 if g["ms"] > 0 else 0.0
+            if n == "fp64":
+                peak, note = fp64_peak, ("cuBLAS DGEMM 8192^3 measured in this run "
+                                         "(FP64 has no entry in MEASURED_PEAKS.json)")
+                kern, bound = "gemm_f64 (DMMA m8n8k4 FP64 tensor cores)", "fp64"
+            else:
+                key = "bf16_tflops_sustained" if "bf16_tflops_sustained" in peaks else "bf16_tflops"
+                peak = peaks[key] / 2 / 3
+                note = f"{peak_kind} {key} / 2 (TF32) / 3 (three split products per credited flop)"
+                kern, bound = "gemm_tf32x3 (tcgen05.mma kind::tf32, TMEM accumulators)", "tensor"
+            dom = max(pr.items(), key=lambda kv: kv[1]["ms"])
+            return {"bound": bound, "kernel": kern, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                    "frac": achieved / peak if peak else None, "traffic": None, "peak_source": note,
+                    "kernel_share_of_device_time": g["ms"] / total_ms if total_ms else None,
+                    "launches_in_profiled_step": g["launches"],
+                    "dominant_family": dom[0],
+                    "families_ms": {k: round(v["ms"], 3) for k, v in pr.items()}}
+
+        acc = {}
+        gold = golden_energies()
+        for n in forms:
+            e30, E, g = fm[n].last
+            acc[n] = {"E": E, "E_iter%d" % iters: e30,
+                      "dE_vs_oracle_iter%d" % iters: (abs(e30 - gold[iters - 1]) if gold else None)}
+        if "fp64" in fm and "mixed" in fm:
+            _, E64, g64 = fm["fp64"].last
+            _, Em, gm = fm["mixed"].last
+            acc["mixed_vs_fp64"] = {"dE": abs(Em - E64),
+                                    "grad_rel": float(np.linalg.norm(gm - g64) / np.linalg.norm(g64))}
         cpu = None
         if not args.no_cpu_baseline:
-            v, mv, sample, nth, _ = cpu_oracle_eg_sample(D, d, chi, seed=1000, budget_s=args.cpu_budget,
+            v, mv, sample, nth, _ = cpu_oracle_eg_sample(seed=1000, budget_s=args.cpu_budget,
                                                          threads=os.cpu_count())
             cpu = {"value": v, "unit": "evals/s", "cores": nth, "kind": "port", "sample": sample, "moves_per_s": mv}
         out = {
-            "metric": "E+grad evals/s (Heisenberg D=%d chi=%d); CTMRG moves/s in moves_per_s" % (D, chi),
+            "metric": metric_name(),
             "value": value, "unit": "evals/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f64 (3xTF32 contractions)",
+            "vs_baseline": None, "dtype": "f64" if forms[0] == "fp64" else "f64 (3xTF32 contractions)",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD_NAME, "precision": args.precision,
+            "config": {"workload": WORKLOAD_NAME, "precision": forms[0],
                        "l2": "flushed between steps (512 MB write)", "replicas": world},
-            "moves_per_s": moves_value,
+            "moves_per_s": moves[forms[0]],
             "e2e": {"value": e2e_value, "unit": "evals/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": int(launches),
-            "roofline": {"bound": "fp64" if args.precision == "fp64" else "tensor",
-                         "kernel": "gemm_f64 (DMMA m8n8k4 FP64 tensor cores)" if args.precision == "fp64" else "gemm_tf32x3",
-                         "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": achieved / peak if peak else None, "traffic": None, "peak_source": peak_note,
-                         "kernel_share_of_device_time": g["ms"] / total_ms if total_ms else None,
-                         "launches_in_profiled_step": g["launches"]},
-            "dominant_family": {"name": dom[0], "share_of_device_time": dom[1]["ms"] / total_ms if total_ms else None},
-            "kernel_families_ms_profiled_step": {k: round(v["ms"], 3) for k, v in prof.items()},
+            "roofline": roofline(forms[0]),
             "projector": {"calls": st["projector_calls"], "jacobi_sweeps_per_call":
-                          st["jacobi_sweeps"] / max(1, st["projector_calls"])},
+                          st["jacobi_sweeps"] / max(1, st["projector_calls"]),
+                          "extra_passes": st["extra_passes"], "series_cap_hits": st["series_cap_hits"]},
+            "accuracy": acc,
             "cpu_baseline": cpu,
             "clocks": clocks,
         }
+        for n in forms[1:]:
+            out[n] = {"evals_per_s": side[n], "moves_per_s": moves[n], "steps": ks, "roofline": roofline(n)}
+        if "fp64" in side:
+            out["mixed_over_fp64"] = value / side["fp64"] if forms[0] == "mixed" else None
         print(json.dumps(out))
+    for f in fm.values():
+        f.ts.close()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -466,11 +583,10 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="both", choices=["both", "fp64", "mixed"])
     ap.add_argument("--cpu-budget", type=float, default=12.0)
-    ap.add_argument("--ref-budget", type=float, default=8.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="d4chi64", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="d5chi100", choices=sorted(WORKLOADS))
     ap.add_argument("--forward-only", type=int, default=0, metavar="ITERS",
                     help="profiling aid: run ITERS forward CTMRG iterations of the workload once, no timing")
     ap.add_argument("--gemm-shapes", action="store_true",

@@ -59,6 +59,8 @@ typedef struct {
   uint64_t projector_calls; /* truncated-SVD projectors computed */
   uint64_t jacobi_sweeps;   /* one-sided Jacobi sweeps summed over those projectors */
   uint64_t extra_passes;    /* extra power iterations triggered by the residual check */
+  uint64_t series_cap_hits; /* projector adjoints whose resolvent series hit its 16-term cap
+                               before the 1e-15 tolerance (gradient possibly inexact) */
 } ipeps_stats_t;
 
 /* ---- context (no reference counterpart: the reference is one CPU process) */
@@ -213,11 +215,13 @@ IPEPS_API int ipeps_gemm_f64(ipeps_ctx* ctx, char opA, char opB, int64_t m, int6
  * the legacy default stream); the call returns without synchronising.
  * For callers that cannot call cudaMalloc (device memory owned by a host
  * framework's pool, or sections where cudaMalloc/cudaFree are not allowed):
- * its split-K partial sums live in a fixed 4 MiB device array instead of an
- * allocation, so it rejects m*n > 262144 with IPEPS_EINVAL (and a message on
- * stderr).  The first call on a device sets up the array's address (make it
- * before any stream capture).  All calls share the array: calls that overlap
- * on the GPU race. */
+ * its split-K partial sums live in a fixed 4 MiB device array (524288
+ * doubles) instead of an allocation.  The split is capped so that the partial
+ * sums fit; outputs above 262144 elements (m*n) run unsplit and use no
+ * scratch.  Shapes beyond the kernel grid (n > 65535*64) are rejected with
+ * IPEPS_EINVAL and a message on stderr.  The first call on a device sets up
+ * the array's address (make it before any stream capture).  All calls share
+ * the array: calls that overlap on the GPU race. */
 IPEPS_API int ipeps_gemm_f64_noalloc(char opA, char opB, int64_t m, int64_t n, int64_t k, double alpha,
                                      const double* A, int64_t lda, const double* B, int64_t ldb, double beta,
                                      double* C, int64_t ldc, void* stream);

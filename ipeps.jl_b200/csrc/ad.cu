@@ -439,7 +439,9 @@ void projector_backward(Ctx& c, const Tensor& R1t, bool t1, const Tensor& R2t, b
     Tensor Yu = project_out(c, Ur, dUt), Yv = project_out(c, Vr, dVt);
     Tensor Xu = c.zeros(DType::F64, {N1, n}), Xv = c.zeros(DType::F64, {N2, n});
     double* d_cmax = reinterpret_cast<double*>(c.scal->p) + 40;
-    for (int m = 0; m < 16; ++m) {
+    constexpr int kSeriesTerms = 16;
+    bool series_done = false;
+    for (int m = 0; m < kSeriesTerms; ++m) {
       series_acc_kernel<<<gridn(c, N1 * n), 256, 0, c.stream>>>(Xu.f64(), Yu.f64(), N1, n, s.f64(), kSvdEta, m);
       series_acc_kernel<<<gridn(c, N2 * n), 256, 0, c.stream>>>(Xv.f64(), Yv.f64(), N2, n, s.f64(), kSvdEta, m);
       series_coef_max_kernel<<<1, 32, 0, c.stream>>>(s.f64(), n, kSvdEta, m, d_cmax);
@@ -448,7 +450,10 @@ void projector_backward(Ctx& c, const Tensor& R1t, bool t1, const Tensor& R2t, b
       IPEPS_CUDA(cudaMemcpyAsync(&cmax, d_cmax, 8, cudaMemcpyDeviceToHost, c.stream));
       const double ny = std::sqrt(dot_host(c, Yu, Yu) + dot_host(c, Yv, Yv));
       const double nx = std::sqrt(dot_host(c, Xu, Xu) + dot_host(c, Xv, Xv));
-      if (cmax * ny <= 1e-15 * nx || ny == 0.0) break;
+      if (cmax * ny <= 1e-15 * nx || ny == 0.0) {
+        series_done = true;
+        break;
+      }
       // Y <- P (M M^T) Y,  Y' <- P' (M^T M) Y'
       Tensor t = Rapply(c, R1t, t1, 'T', Yu);
       t = Rapply(c, R2t, t2, 'T', t);
@@ -460,6 +465,12 @@ void projector_backward(Ctx& c, const Tensor& R1t, bool t1, const Tensor& R2t, b
       t = Rapply(c, R1t, t1, 'T', t);
       t = Rapply(c, R2t, t2, 'T', t);
       Yv = project_out(c, Vr, t);
+    }
+    // the series stopped at its term cap: the discarded spectrum's share of the
+    // gradient is truncated (counted in ipeps_stats_t, bit 16 of the status word)
+    if (!series_done) {
+      c.series_cap_hits++;
+      flag_status(c, 16);
     }
     // Acol += M^T X_u ; Bcol += M X_v ; and the s_t-scaled terms
     Tensor MtXu = Rapply(c, R2t, t2, 'T', Rapply(c, R1t, t1, 'T', Xu));

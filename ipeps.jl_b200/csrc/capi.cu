@@ -35,7 +35,8 @@ int guarded(ipeps_ctx* ctx, F&& f) {
     if (ctx->c) IPEPS_CUDA(cudaMemsetAsync(ctx->c->d_status, 0, sizeof(int), ctx->c->stream));
     int st = f();
     if (ctx->c) {
-      // status bits: 2 non-finite value, 4 Jacobi sweep cap hit, 8 tensor-core pipeline wait timed out
+      // status bits: 2 non-finite value, 4 Jacobi sweep cap hit, 8 tensor-core pipeline wait timed out,
+      // 16 projector-adjoint resolvent series stopped at its term cap (counted in ipeps_stats_t)
       int dev_status = 0;
       IPEPS_CUDA(cudaMemcpyAsync(&dev_status, ctx->c->d_status, sizeof(int), cudaMemcpyDeviceToHost,
                                  ctx->c->stream));
@@ -137,6 +138,7 @@ int ipeps_stats(ipeps_ctx* ctx, ipeps_stats_t* out) {
     out->projector_calls = ctx->c->projector_calls;
     out->jacobi_sweeps = ctx->c->jacobi_sweeps;
     out->extra_passes = ctx->c->projector_extra_passes;
+    out->series_cap_hits = ctx->c->series_cap_hits;
     return IPEPS_OK;
   });
 }
@@ -149,6 +151,7 @@ int ipeps_stats_reset(ipeps_ctx* ctx) {
     ctx->c->projector_calls = 0;
     ctx->c->jacobi_sweeps = 0;
     ctx->c->projector_extra_passes = 0;
+    ctx->c->series_cap_hits = 0;
     return IPEPS_OK;
   });
 }

@@ -251,6 +251,7 @@ std::vector<double> move_pair(Env& e, int da, int db, ProjResult* ka, ProjResult
   Ctx& c2 = *e.aux;
   c2.precision = c1.precision;
   c2.prof = c1.prof;
+  c2.d_status = c1.d_status;  // device-side problems of either stream reach the caller's status word
   const Env keep = e;
   Env eb = e;
   eb.ctx = &c2;
@@ -295,7 +296,8 @@ std::vector<double> move_pair(Env& e, int da, int db, ProjResult* ka, ProjResult
   c1.jacobi_sweeps += c2.jacobi_sweeps;
   c1.projector_calls += c2.projector_calls;
   c1.projector_extra_passes += c2.projector_extra_passes;
-  c2.jacobi_sweeps = c2.projector_calls = c2.projector_extra_passes = 0;
+  c1.series_cap_hits += c2.series_cap_hits;
+  c2.jacobi_sweeps = c2.projector_calls = c2.projector_extra_passes = c2.series_cap_hits = 0;
   for (auto& r : c2.prof_rec) c1.prof_rec.push_back(r);
   c2.prof_rec.clear();
   if (err_a) std::rethrow_exception(err_a);
@@ -519,7 +521,8 @@ void merge_stats(Ctx& to, Ctx& from) {
   to.jacobi_sweeps += from.jacobi_sweeps;
   to.projector_calls += from.projector_calls;
   to.projector_extra_passes += from.projector_extra_passes;
-  from.jacobi_sweeps = from.projector_calls = from.projector_extra_passes = 0;
+  to.series_cap_hits += from.series_cap_hits;
+  from.jacobi_sweeps = from.projector_calls = from.projector_extra_passes = from.series_cap_hits = 0;
   for (auto& r : from.prof_rec) to.prof_rec.push_back(r);
   from.prof_rec.clear();
 }
@@ -561,6 +564,7 @@ struct PendingConv {
     if (!e.aux_eval) e.aux_eval = std::make_shared<Ctx>(c1.device);
     Ctx& c3 = *e.aux_eval;
     c3.prof = c1.prof;
+    c3.d_status = c1.d_status;
     snap = e;
     s = sp;
     iter = it;

@@ -6,6 +6,7 @@
 #include "common.cuh"
 
 #include <array>
+#include <atomic>
 #include <map>
 #include <tuple>
 
@@ -43,6 +44,9 @@ struct Ctx {
   uint64_t jacobi_sweeps = 0;
   uint64_t projector_calls = 0;
   uint64_t projector_extra_passes = 0;
+  // projector adjoints whose resolvent series stopped at its term cap before
+  // reaching the 1e-15 relative tolerance (the gradient may be inexact)
+  uint64_t series_cap_hits = 0;
   // split-K partial sums live here (grown on demand, stream ordered)
   std::shared_ptr<DBuf> ws;
   // small device scalars (max-abs, traces, status words)
@@ -90,6 +94,21 @@ struct Fp64Scope {
   ~Fp64Scope() { c.precision = prev; }
   Fp64Scope(const Fp64Scope&) = delete;
   Fp64Scope& operator=(const Fp64Scope&) = delete;
+};
+
+// The dynamic shared-memory limit of a kernel is a per-function, per-device
+// attribute: set it once on every device the kernel is launched on.
+struct SmemAttrOnce {
+  static constexpr int kMaxDevices = 64;
+  std::atomic<bool> done[kMaxDevices] = {};
+  template <class K>
+  void ensure(K kern, int bytes) {
+    int dev = 0;
+    IPEPS_CUDA(cudaGetDevice(&dev));
+    if (dev < kMaxDevices && done[dev].load()) return;
+    IPEPS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    if (dev < kMaxDevices) done[dev].store(true);
+  }
 };
 
 struct ProfScope {
@@ -164,6 +183,9 @@ void axpy(Ctx& c, cuDoubleComplex a, const Tensor& x, Tensor& y);
 Tensor conj(Ctx& c, const Tensor& x);
 // convert real tensor to complex128
 Tensor to_complex(Ctx& c, const Tensor& x);
+// ORs `bits` into the status word on the context stream (host-detected
+// conditions that the caller reads with the device-side ones)
+void flag_status(Ctx& c, int bits);
 // nonfinite scan: sets bit in c.d_status
 void check_finite(Ctx& c, const Tensor& x);
 // fill with N(0,1) (counter-based hash RNG, reproducible)

@@ -205,7 +205,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) gemm_bf16_kernel(ArgsB a) {
   }
 }
 
-std::atomic<bool> g_bf16_attr{false};
+SmemAttrOnce g_bf16_attr;
 
 }  // namespace
 
@@ -214,10 +214,7 @@ void gemm_bf16(Ctx& c, char opA, char opB, int64_t m, int64_t n, int64_t k, floa
   if (m <= 0 || n <= 0) return;
   IPEPS_CHECK(k > 0, "gemm_bf16: k == 0");
   IPEPS_CHECK((opA == 'N' || opA == 'T') && (opB == 'N' || opB == 'T'), "gemm_bf16: op must be N or T");
-  if (!g_bf16_attr) {
-    IPEPS_CUDA(cudaFuncSetAttribute(gemm_bf16_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
-    g_bf16_attr = true;
-  }
+  g_bf16_attr.ensure(gemm_bf16_kernel, SMEM_BYTES);
   const int64_t gx = (m + BM - 1) / BM, gy = (n + BN - 1) / BN;
   IPEPS_CHECK(gy <= 65535, "gemm_bf16: n too large for grid");
   ArgsB a{};

@@ -202,14 +202,8 @@ void launch_cfg(Ctx& c, int64_t m, int64_t n, int64_t k, double alpha, const dou
   constexpr int NT = WGM * WGN * 32;
   constexpr size_t smem = size_t(kStages) * (Tile<BM, AK>::size + Tile<BN, BK_>::size) * sizeof(double);
   auto kern = dmma_gemm_kernel<BM, BN, WGM, WGN, AK, BK_, VEC>;
-  // the dynamic shared-memory limit is a per-function, per-device attribute
-  static std::atomic<bool> attr_set[64];
-  int dev = 0;
-  IPEPS_CUDA(cudaGetDevice(&dev));
-  if (dev >= 64 || !attr_set[dev]) {
-    IPEPS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-    if (dev < 64) attr_set[dev] = true;
-  }
+  static SmemAttrOnce attr;
+  attr.ensure(kern, int(smem));
   const int64_t gx = (m + BM - 1) / BM, gy = (n + BN - 1) / BN;
   IPEPS_CHECK(gy <= 65535, "gemm: n too large for grid");
   const int64_t tiles = gx * gy;

@@ -259,8 +259,12 @@ void gemm_f64(Ctx& c, DType dt, char opA, char opB, int64_t m, int64_t n, int64_
 // host with a fixed budget), or a latency-critical section where
 // cudaMalloc/cudaFree, which may synchronise the device, are not allowed.
 // For them the split-K partial sums live in this fixed device array
-// (4 MiB; every GPU that loads the library holds it until the process
-// exits).  The caller passes device pointers for A, B and C and a stream.
+// (4 MiB = 524288 doubles; every GPU that loads the library holds it until
+// the process exits).  The caller passes device pointers for A, B and C and a
+// stream.  The split factor S is capped so that S*m*n partial sums fit in the
+// array; an output of more than 262144 elements therefore runs unsplit and
+// touches no scratch at all.  Requests the kernel grid cannot cover
+// (ceil(n/64) > 65535) are rejected with IPEPS_EINVAL and a message on stderr.
 //
 // The first call on a device looks up the array's device address with
 // cudaGetSymbolAddress (with that device current); make that first call
@@ -277,7 +281,6 @@ namespace ipeps {
 namespace {
 
 constexpr int64_t kNoAllocScratchDoubles = int64_t(1) << 19;  // 4 MiB of FP64 partial sums
-constexpr int64_t kNoAllocMaxOutput = kNoAllocScratchDoubles / 2;
 constexpr int kNoAllocMaxDevices = 64;
 
 static __device__ __align__(256) double g_noalloc_splitk_scratch[kNoAllocScratchDoubles];
@@ -318,18 +321,16 @@ extern "C" int ipeps_gemm_f64_noalloc(char opA, char opB, int64_t m, int64_t n, 
     return IPEPS_EINVAL;
   }
   if (oa == 2 || ob == 2) return IPEPS_EINVAL;  // real data: 'C' is not meaningful
-  if (m * n > kNoAllocMaxOutput) {
-    std::fprintf(stderr,
-                 "ipeps_gemm_f64_noalloc: m*n = %lld output elements exceeds the static scratch limit of %lld\n",
-                 static_cast<long long>(m * n), static_cast<long long>(kNoAllocMaxOutput));
-    return IPEPS_EINVAL;
-  }
   if (lda < ((oa == 0) ? m : k) || ldb < ((ob == 0) ? k : n) || ldc < m) return IPEPS_EINVAL;
-  double* scratch = nullptr;
-  if (noalloc_scratch(&scratch) != cudaSuccess) return IPEPS_ECUDA;
   constexpr int BM = 64, BN = 64, BK = 16, TM = 4, TN = 4, NT = (BM / TM) * (BN / TN);
   const int64_t gx = (m + BM - 1) / BM, gy = (n + BN - 1) / BN;
-  if (gy > 65535) return IPEPS_EINVAL;
+  if (gy > 65535 || gx > int64_t(0x7fffffff)) {
+    std::fprintf(stderr, "ipeps_gemm_f64_noalloc: m = %lld, n = %lld exceed the kernel grid (n <= %lld)\n",
+                 static_cast<long long>(m), static_cast<long long>(n), 65535LL * BN);
+    return IPEPS_EINVAL;
+  }
+  double* scratch = nullptr;
+  if (noalloc_scratch(&scratch) != cudaSuccess) return IPEPS_ECUDA;
   int sms = 148;
   int dev = 0;
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -337,6 +338,7 @@ extern "C" int ipeps_gemm_f64_noalloc(char opA, char opB, int64_t m, int64_t n, 
   const int64_t tiles = gx * gy, target = 2LL * sms;
   int64_t S = 1;
   if (tiles < target && k >= 8 * BK * 2) S = std::min<int64_t>(std::min<int64_t>((target + tiles - 1) / tiles, k / (8 * BK)), 64);
+  // cap by the scratch: S * m * n partial sums at most (S = 1 uses none)
   S = std::max<int64_t>(1, std::min<int64_t>(S, kNoAllocScratchDoubles / (m * n)));
   int64_t kchunk = (k + S - 1) / S;
   kchunk = ((kchunk + BK - 1) / BK) * BK;

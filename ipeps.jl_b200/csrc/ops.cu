@@ -409,6 +409,8 @@ __global__ void to_complex_kernel(const double* __restrict__ x, double2* __restr
     y[i] = make_double2(x[i], 0.0);
 }
 
+__global__ void flag_status_kernel(int* status, int bits) { atomicOr(status, bits); }
+
 __global__ void finite_kernel(const double* __restrict__ x, int64_t n, int* status) {
   bool bad = false;
   for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
@@ -511,6 +513,12 @@ void check_finite(Ctx& c, const Tensor& x) {
   finite_kernel<<<grid_for(c, n), 256, 0, c.stream>>>(x.f64(), n, c.d_status);
   IPEPS_LAUNCH_CHECK();
   c.count(KFam::Reduce, 0, double(x.bytes()));
+}
+
+void flag_status(Ctx& c, int bits) {
+  flag_status_kernel<<<1, 1, 0, c.stream>>>(c.d_status, bits);
+  IPEPS_LAUNCH_CHECK();
+  c.count(KFam::Reduce);
 }
 
 void randn(Ctx& c, Tensor& x) {

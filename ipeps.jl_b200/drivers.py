@@ -131,24 +131,64 @@ def tangent_basis(ts: host.CTMTensors, n_dm_Ad: np.ndarray):
     return vh.conj().T[:, 1:]
 
 
-def evaluate_es(effH: np.ndarray, effN: np.ndarray, nrmB_cut: float = 1e-3):
-    """evaluate_es (expectation.jl:152-183): symmetrise, keep the directions of
-    N above nrmB_cut (ratio to the largest eigenvalue, or a count when an int),
-    solve H x = E N x.  Returns the sorted real eigenvalues."""
+def prepare_basis(H, A, cfg: Dict[str, Any], engine: Optional[host.Engine] = None):
+    """prepare_basis (optim_es.jl:34-73) on the device, for a ground state A
+    (the reference loads it from gs.jld2): renormalise A (max-abs), converge
+    the environment from init_ctm1 with the energy criterion at 2 max_iter and
+    rg_tol^2, restore the configured Params, normalise A (normalize_gs),
+    subtract E0/2 from both bond Hamiltonians (substract_gs_energy) and take
+    the default tangent basis.  Returns (ts, H_sub, basis) with basis
+    (D^4 d, D^4 d - 1) complex; ts stays on the device for optim_es."""
+    A = np.asarray(A)
+    A = A / np.abs(A).max()
+    cfg0 = dict(cfg)
+    ts = host.CTMTensors(A, cfg0, engine=engine)
+    ts.Params["max_iter"] = 2 * int(cfg0.get("max_iter", 20))
+    ts.Params["rg_tol"] = float(cfg0.get("rg_tol", 1e-6)) ** 2
+    host.run_ctm(ts, conv_fun="energy", H=H)
+    ts.Params = dict(cfg0)
+    normalize_gs(ts)
+    H2 = substract_gs_energy(ts, H)
+    basis = tangent_basis(ts, host.single_dm_Ad(ts))
+    return ts, H2, basis
+
+
+def _es_subspace(effH: np.ndarray, effN: np.ndarray, nrmB_cut=1e-3):
+    """The common part of compute_es / evaluate_es (expectation.jl:13-56,
+    152-183): Hermitian parts, the eigenvectors of N sorted by decreasing
+    eigenvalue, and the selection by nrmB_cut (a ratio to the largest
+    eigenvalue, or, when an int, the values above the (cut+1)-th)."""
     H2 = (effH + effH.conj().T) / 2
     N2 = (effN + effN.conj().T) / 2
     ev, P = np.linalg.eigh(N2)
     idx = np.argsort(ev)[::-1]
     ev, P = ev[idx], P[:, idx]
-    if isinstance(nrmB_cut, int):
-        keep = slice(0, nrmB_cut)
+    if isinstance(nrmB_cut, (int, np.integer)) and not isinstance(nrmB_cut, bool):
+        keep = ev > ev[nrmB_cut]
     else:
-        keep = ev / ev[0] > nrmB_cut
+        keep = ev / ev.max() > nrmB_cut
     P = P[:, keep]
     Hp = P.conj().T @ H2 @ P
     Np = P.conj().T @ N2 @ P
-    w = np.linalg.eigvals(np.linalg.solve(Np, Hp))
-    return np.sort(w.real)
+    return (Hp + Hp.conj().T) / 2, (Np + Np.conj().T) / 2, P
+
+
+def compute_es(effH: np.ndarray, effN: np.ndarray, nrmB_cut=1e-3):
+    """compute_es (expectation.jl:13-56): the generalised eigenproblem
+    H x = E N x on the selected subspace.  Returns (es, vecs, P) sorted by
+    real part (es complex, as Julia's eigen(H2, N2))."""
+    import scipy.linalg as sl
+    Hp, Np, P = _es_subspace(effH, effN, nrmB_cut)
+    es, vecs = sl.eig(Hp, Np)
+    ix = np.argsort(es.real)
+    return es[ix], vecs[:, ix], P
+
+
+def evaluate_es(effH: np.ndarray, effN: np.ndarray, nrmB_cut=1e-3):
+    """evaluate_es (expectation.jl:152-183): the sorted real parts of the
+    generalised eigenvalues of compute_es."""
+    es, _, _ = compute_es(effH, effN, nrmB_cut)
+    return np.sort(es.real)
 
 
 def es_column(px: float, py: float, ts: host.CTMTensors, H, basis: np.ndarray, i: int, C=None):

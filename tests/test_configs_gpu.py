@@ -1,0 +1,213 @@
+"""GPU parity at the benchmark configurations, against the oracle's golden
+fixtures (tests/golden/make_golden_configs.py).
+
+* Transverse-field Ising h=2, D=2, chi=30 (A seed 0): CTMRG stopped by the
+  corner-spectrum criterion at rg_tol 1e-6 (ctmrg.jl:29-31) from init_ctm1,
+  then the energy and the gradient of the pullback of ad_max_iter = 4
+  iterations; and the fg! path (energy criterion).
+* Heisenberg D=4, chi=64 (A seed 1000): 30 CTMRG iterations, the energy after
+  each, the left-move spectrum of the last one, the gradient, and central
+  differences (step 1e-6) along 16 seeded directions against the oracle's
+  directional derivatives.
+* Heisenberg D=3, chi=48 (A seed 21): prepare_basis (converged, normalised
+  ground state, E0/2 subtracted) and get_es_grad of three basis vectors at
+  (px, py) = (pi, 0) and (pi/2, pi/2).
+
+Bars: FP64 form energy 1e-10 absolute, leading singular values 1e-10
+relative, gradients 1e-6 relative (2-norm); mixed form energy 1e-8 absolute,
+gradient 1e-6 relative.
+"""
+import json
+import math
+import os
+
+import numpy as np
+import pytest
+
+import ipeps_oracle as O
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def _gold(name):
+    with open(os.path.join(GOLD, name + ".json")) as f:
+        return json.load(f)
+
+
+def _cvec(pairs):
+    a = np.asarray(pairs)
+    return a[:, 0] + 1j * a[:, 1]
+
+
+@pytest.fixture(scope="module")
+def engines(pkg):
+    from conftest import gpu_available
+    if not gpu_available():
+        pytest.skip("no CUDA device")
+    e = {"fp64": pkg.Engine(0), "mixed": pkg.Engine(0, precision="mixed")}
+    yield e
+    for x in e.values():
+        x.close()
+
+
+BARS = {"fp64": (1e-10, 1e-6), "mixed": (1e-8, 1e-6)}
+
+
+# ------------------------------------------------------------------ TFIM D=2 chi=30
+@pytest.mark.parametrize("form", ["fp64", "mixed"])
+def test_tfim_chi30_spectrum_criterion_and_gradient(engines, pkg, form):
+    g = _gold("config1")
+    eng = engines[form]
+    ebar, gbar = BARS[form]
+    A = O.random_A(2, 2, seed=g["seed"]).numpy()
+    H = [h.numpy() for h in O.ising(g["h"])]
+    cfg = pkg.default_config()
+    cfg.update(chi=g["chi"], min_iter=g["min_iter"], max_iter=g["max_iter"], rg_tol=g["rg_tol"],
+               ad_max_iter=g["ad_max_iter"])
+    ts = pkg.CTMTensors(A, cfg, engine=eng)
+    ts, info = pkg.run_ctm(ts, conv_fun=None)
+    sp = g["spectrum"]
+    # the run stops on the spectrum criterion at the oracle's iteration
+    assert info["converged"] and info["iters"] == sp["iters"], (info["iters"], sp["iters"])
+    E, _ = pkg.get_gs_energy(ts, H)
+    assert abs(E.real - sp["E_converged"]) <= ebar, (E, sp["E_converged"])
+    Ead, grad = pkg.energy_grad(ts, H)
+    go = np.asarray(sp["grad"])
+    assert abs(Ead - sp["E_ad"]) <= ebar, (Ead, sp["E_ad"])
+    rel = np.linalg.norm(grad.ravel(order="F") - go) / np.linalg.norm(go)
+    assert rel <= gbar, rel
+    ts.close()
+    # fg! (optim_gs.jl:53-91): energy criterion at the same rg_tol
+    Ef, gf, _ = pkg.fg(A, H, cfg, engine=eng)
+    ec = g["energy_criterion"]
+    assert abs(Ef - ec["E"]) <= ebar, (Ef, ec["E"])
+    gfo = np.asarray(ec["grad"])
+    assert np.linalg.norm(gf.ravel(order="F") - gfo) <= gbar * np.linalg.norm(gfo)
+
+
+def test_tfim_chi30_last_spectrum(engines, pkg):
+    """The left-move spectrum of the iteration at which the spectrum criterion
+    stops (FP64 form): leading values 1e-10 relative, all kept values 1e-8."""
+    g = _gold("config1")
+    A = O.random_A(2, 2, seed=g["seed"]).numpy()
+    cfg = pkg.default_config()
+    cfg.update(chi=g["chi"], min_iter=g["min_iter"], max_iter=g["spectrum"]["iters"] - 1,
+               rg_tol=0.0)
+    ts = pkg.CTMTensors(A, cfg, engine=engines["fp64"])
+    pkg.run_ctm(ts, conv_fun=None)
+    ts, s = pkg.rg_step(ts)
+    so = np.asarray(g["spectrum"]["s_last"])
+    assert len(s) == len(so)
+    lead = min(10, len(so))
+    assert np.allclose(s[:lead], so[:lead], rtol=1e-10)
+    assert np.allclose(s, so, rtol=1e-8, atol=1e-12 * so[0])
+    ts.close()
+
+
+# ------------------------------------------------------------------ Heisenberg D=4 chi=64
+@pytest.fixture(scope="module")
+def d4_runs(engines, pkg):
+    """30 iterations of the D=4 chi=64 workload in each form: energies, last
+    spectrum, E+grad, and the converged C/T (for finite differences)."""
+    g = _gold("config2")
+    A = O.random_A(4, 2, seed=g["seed"]).numpy()
+    H = [h.numpy() for h in O.heisenberg(1.0)]
+    out = {}
+    for form, eng in engines.items():
+        cfg = pkg.default_config()
+        cfg.update(chi=64, min_iter=g["iters"] - 1, max_iter=g["iters"] - 1, rg_tol=0.0, ad_max_iter=4)
+        ts = pkg.CTMTensors(A, cfg, engine=eng)
+        ts, info = pkg.run_ctm(ts, conv_fun="energy", H=H)
+        ts, s = pkg.rg_step(ts)
+        E30, _ = pkg.get_gs_energy(ts, H)
+        C = [ts.get_CT(k) for k in range(1, 5)]
+        Ead, grad = pkg.energy_grad(ts, H)
+        out[form] = dict(traj=[l["obj"].real for l in info["log"]] + [E30.real], s=s, Ead=Ead,
+                         grad=grad.ravel(order="F"), C=C, cfg=cfg)
+        ts.close()
+    return A, H, g, out
+
+
+@pytest.mark.parametrize("form", ["fp64", "mixed"])
+def test_heisenberg_d4_chi64_energy_spectrum_gradient(d4_runs, form):
+    A, H, g, out = d4_runs
+    r = out[form]
+    ebar, gbar = BARS[form]
+    traj = np.asarray(r["traj"])
+    eo = np.asarray(g["energies"])
+    # the mixed form runs its last iterations in FP64 (polish); compare the end of the run
+    if form == "fp64":
+        assert np.abs(traj - eo).max() <= ebar, np.abs(traj - eo).max()
+    assert abs(traj[-1] - eo[-1]) <= ebar, (traj[-1], eo[-1])
+    so = np.asarray(g["s_last"])
+    assert len(r["s"]) == len(so)
+    srel = 1e-10 if form == "fp64" else 1e-8
+    assert np.allclose(r["s"][:16], so[:16], rtol=srel), np.abs(r["s"][:16] / so[:16] - 1).max()
+    assert np.allclose(r["s"], so, rtol=1e-6 if form == "fp64" else 1e-5, atol=1e-12 * so[0])
+    assert abs(r["Ead"] - g["E_ad"]) <= ebar, (r["Ead"], g["E_ad"])
+    go = np.asarray(g["grad"])
+    rel = np.linalg.norm(r["grad"] - go) / np.linalg.norm(go)
+    assert rel <= gbar, rel
+
+
+def test_heisenberg_d4_chi64_finite_differences(engines, pkg, d4_runs):
+    """Central differences (step 1e-6) of the energy of the E+grad unit (4
+    CTMRG iterations from the fixed 30-iteration environment, then the
+    energy) along 16 seeded directions, against the oracle's directional
+    derivatives g.v.  The reference adjoint broadens 1/(s_i^2 - s_j^2)
+    (eta = 1e-12), so it is not the exact derivative: the bar is 1e-3
+    relative to max(|g.v|, 1e-2 |g| |v|)."""
+    A, H, g, out = d4_runs
+    r = out["fp64"]
+    eng = engines["fp64"]
+    cfg = dict(r["cfg"])
+    cfg.update(min_iter=4, max_iter=4)
+
+    def energy(x):
+        t = pkg.CTMTensors(x, cfg, engine=eng, init=False)
+        for k in range(4):
+            t.set_CT(k + 1, *r["C"][k])
+        pkg.run_ctm(t, conv_fun="energy", H=H)
+        e, _ = pkg.get_gs_energy(t, H)
+        t.close()
+        return e.real
+
+    rng = np.random.default_rng(g["direction_seed"])
+    dirs = rng.standard_normal((16, A.size))
+    go = np.asarray(g["grad"])
+    h = 1e-6
+    for i in range(16):
+        v = dirs[i].reshape(A.shape, order="F")
+        fd = (energy(A + h * v) - energy(A - h * v)) / (2 * h)
+        dd = g["directional"][i]
+        scale = max(abs(dd), 1e-2 * np.linalg.norm(go) * np.linalg.norm(dirs[i]))
+        assert abs(fd - dd) <= 1e-3 * scale, (i, fd, dd)
+
+
+# ------------------------------------------------------------------ Heisenberg D=3 chi=48, nested
+def test_heisenberg_d3_chi48_es_grad(engines, pkg):
+    g = _gold("config5")
+    eng = engines["fp64"]
+    A = O.random_A(3, 2, seed=g["seed"]).numpy()
+    H = [h.numpy() for h in O.heisenberg(1.0)]
+    cfg = pkg.default_config()
+    cfg.update(chi=g["chi"], min_iter=4, max_iter=40, rg_tol=g["gs_rg_tol"], ad_max_iter=g["ad_max_iter"])
+    ts = pkg.CTMTensors(A, cfg, engine=eng)
+    pkg.run_ctm(ts, conv_fun="energy", H=H)
+    drivers = pkg.drivers
+    drivers.normalize_gs(ts)
+    H2 = drivers.substract_gs_energy(ts, H)
+    C = [ts.get_CT(k) for k in range(1, 5)]
+    for case in g["cases"]:
+        t = pkg.CTMTensors(ts.A, dict(ts.Params), engine=eng, init=False)
+        for k in range(4):
+            t.set_CT(k + 1, *C[k])
+        t.Params.update(px=case["px"], py=case["py"], max_iter=g["es_max_iter"], min_iter=4, rg_tol=g["es_rg_tol"])
+        gH, gN = pkg.get_es_grad(t, H2, _cvec(case["Bi"]))
+        t.close()
+        gHo, gNo = _cvec(case["gH"]), _cvec(case["gN"])
+        eh = np.linalg.norm(gH - gHo) / np.linalg.norm(gHo)
+        en = np.linalg.norm(gN - gNo) / np.linalg.norm(gNo)
+        assert eh <= 1e-6 and en <= 1e-6, (case["px"], case["py"], case["col"], eh, en)
+    ts.close()

@@ -111,7 +111,7 @@ def test_single_move_spectra(engine, pkg):
             assert np.allclose(sg[:lead], so[:lead], rtol=1e-10), (it, d, sg[:lead], so[:lead])
 
 
-@pytest.mark.parametrize("idx", [0, 1, 3])
+@pytest.mark.parametrize("idx", [0, 1, 2, 3])
 def test_converged_energy_matches_golden(engine, pkg, idx):
     with open(os.path.join(GOLD, "ctm_energies.json")) as f:
         case = json.load(f)["cases"][idx]

@@ -29,7 +29,7 @@ def npa(t):
     return t.detach().numpy() if isinstance(t, torch.Tensor) else np.asarray(t)
 
 
-@pytest.mark.parametrize("idx", [0, 1, 3])
+@pytest.mark.parametrize("idx", [0, 1, 2, 3])
 def test_mixed_converged_energy(mixed_engine, pkg, idx):
     with open(os.path.join(GOLD, "ctm_energies.json")) as f:
         case = json.load(f)["cases"][idx]
