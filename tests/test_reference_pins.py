@@ -1,0 +1,79 @@
+"""The oracle against numbers the reference itself computed and saved
+(simulation/test_test_D2_X32/*.jld2, decoded into tests/golden/ref_pins.npz by
+tests/golden/make_reference_pins.py).
+
+* gs.jld2: the fg! energy of the reference's last optim_gs iterate (honeycomb
+  XX model, complex A (2,2,2,2,4), default config chi = 32): reproduced to
+  1e-12 (converge from init_ctm1 with the energy criterion, then the
+  ad_max_iter = 4 iterations of run_gs and get_gs_energy, optim_gs.jl:53-91).
+* es_{px}_{py}.jld2: effN = basis' * gN of optim_es (optim_es.jl:127-153)
+  from the saved normalised ground-state environment and tangent basis:
+  three columns at two momenta reproduced to 1e-9 relative.
+"""
+import importlib.util
+import math
+import os
+
+import numpy as np
+import pytest
+import torch
+
+import ipeps_oracle as O
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+REF = "/root/reference/simulation/test_test_D2_X32"
+
+
+def pins():
+    return np.load(os.path.join(GOLD, "ref_pins.npz"))
+
+
+def es_ts(p):
+    cfg = O.default_config()
+    T = torch.tensor
+    return O.CTMTensors(A=T(p["es_A"]), Ad=T(p["es_A"].conj()), Cs=[T(p[f"es_C{k}"]) for k in range(1, 5)],
+                        Es=[T(p[f"es_E{k}"]) for k in range(1, 5)], Params=dict(cfg))
+
+
+def test_oracle_reproduces_reference_gs_energy():
+    p = pins()
+    H = O.honeycomb(1, 1, dir="XX")
+    cfg = O.default_config()
+    x = O.renormalize(torch.tensor(p["gs_A"]))
+    with torch.no_grad():
+        ts = O._detach_ts(O.get_conv_boundary(x, H, cfg))
+        prm = dict(ts.Params)
+        prm["max_iter"] = prm["ad_max_iter"]
+        E = O.run_gs(ts.replace(Params=prm), H, x)
+    assert abs(complex(E).real - p["gs_energies"][-1]) <= 1e-12, (complex(E).real, p["gs_energies"][-1])
+
+
+@pytest.mark.parametrize("mom", [("0.1", "0"), ("1", "1")])
+def test_oracle_reproduces_reference_effN(mom):
+    p = pins()
+    ts = es_ts(p)
+    basis = p["es_basis"]
+    H2 = O.substract_gs_energy(ts, O.ising(2.0))
+    prm = dict(ts.Params)
+    prm.update(px=float(mom[0]) * math.pi, py=float(mom[1]) * math.pi)
+    t1 = ts.replace(Params=prm)
+    ref = p[f"effN_{mom[0]}_{mom[1]}"]
+    for i in (0, 15, 30):
+        _, gN = O.get_es_grad(t1, H2, torch.tensor(basis[:, i]))
+        col = basis.conj().T @ gN.resolve_conj().numpy()
+        assert np.linalg.norm(col - ref[:, i]) <= 1e-9 * np.linalg.norm(ref[:, i]), (mom, i)
+
+
+@pytest.mark.skipif(not os.path.isdir(REF), reason="reference tree not present")
+def test_jld2_reader_matches_committed_pins(pkg):
+    jld2 = pkg.jld2
+    p = pins()
+    gs = jld2.load(os.path.join(REF, "gs.jld2"))
+    assert np.array_equal(gs["A"], p["gs_A"]) and np.array_equal(gs["energies"], p["gs_energies"])
+    b = jld2.load(os.path.join(REF, "basis.jld2"))
+    assert np.array_equal(b["basis"], p["es_basis"])
+    assert [c.shape for c in b["ts"]["Cs"]] == [p[f"es_C{k}"].shape for k in range(1, 5)]
+    e = jld2.load(os.path.join(REF, "es_1_1.jld2"))
+    assert np.array_equal(e["effN"], p["effN_1_1"])
+    # effN is Hermitian up to the columns' separate CTMRG convergence (rg_tol 1e-6)
+    assert np.abs(e["effN"] - e["effN"].conj().T).max() <= 1e-6 * np.abs(e["effN"]).max()
