@@ -17,6 +17,7 @@ are compared.
 from __future__ import annotations
 
 import math
+import os
 from typing import Any, Callable, Dict, List, Optional
 
 import numpy as np
@@ -28,15 +29,54 @@ def _sphere_project(x, g):
     return g - np.vdot(x, g).real * x
 
 
-def optim_gs(H, A0, cfg: Dict[str, Any], m: int = 10, g_tol: float = 1e-6, f_tol: float = 1e-7,
+def load_gs(path: str) -> Dict[str, Any]:
+    """A ground-state checkpoint: the reference's gs.jld2 (A, energies,
+    gradnorms; optim_gs.jl:36) or this package's gs.npz (the same keys)."""
+    if path.endswith(".jld2"):
+        from . import jld2
+        d = jld2.load(path)
+    else:
+        d = dict(np.load(path))
+    return {"A": np.asarray(d["A"]), "energies": list(np.atleast_1d(d.get("energies", []))),
+            "gradnorms": list(np.atleast_1d(d.get("gradnorms", [])))}
+
+
+def _save_gs(path: str, A, energies, gradnorms):
+    os.makedirs(os.path.dirname(path), exist_ok=True)
+    np.savez(path, A=A, energies=np.asarray(energies), gradnorms=np.asarray(gradnorms))
+
+
+def optim_gs(H, A0, cfg, m: int = 10, g_tol: float = 1e-6, f_tol: float = 1e-7,
              iterations: int = 200, engine: Optional[host.Engine] = None,
              callback: Optional[Callable[[int, float, float], None]] = None,
-             fg_fn: Optional[Callable] = None):
+             fg_fn: Optional[Callable] = None, save_dir: Optional[str] = None):
     """L-BFGS over A on the unit sphere with the device E+grad unit (fg!).
 
+    cfg: a config dict, or a TOML file name (optim_gs.jl:1-12; the default
+    config when the file does not exist).  With cfg["resume"] and a checkpoint
+    in the run directory (get_dir: the reference's gs.jld2, or gs.npz), the
+    run restarts from its A and continues its energy/gradnorm lists
+    (optim_gs.jl:47-53).  With cfg["save"] and an explicit directory (save_dir,
+    or cfg["dir"] != 0) A, energies and gradnorms are written to gs.npz there
+    after every step (the reference writes gs.jld2; nothing is written under
+    the working directory by default).
     ``fg_fn(A, H, cfg, engine=...) -> (E, g, info)`` replaces host.fg (e.g. the
     warm-started unit of warmstart.WarmStart.fg).  Returns dict(A, energies,
     gradnorms, evals)."""
+    if isinstance(cfg, str):
+        cfg = host.load_config(cfg)
+    run_dir = save_dir or host.get_dir(cfg)
+    prev_E: List[float] = []
+    prev_g: List[float] = []
+    if cfg.get("resume", False):
+        for name in ("gs.npz", "gs.jld2"):
+            path = os.path.join(run_dir, name)
+            if os.path.exists(path):
+                ck = load_gs(path)
+                A0, prev_E, prev_g = ck["A"], ck["energies"], ck["gradnorms"]
+                break
+    if np.iscomplexobj(A0):
+        raise ValueError("optim_gs: complex A has no device gradient (real A only)")
     x = np.asarray(A0, dtype=np.float64).ravel(order="F")
     shape = np.asarray(A0).shape
     x = x / np.linalg.norm(x)
@@ -54,7 +94,8 @@ def optim_gs(H, A0, cfg: Dict[str, Any], m: int = 10, g_tol: float = 1e-6, f_tol
 
     f, g = fg(x)
     gp = _sphere_project(x, g)
-    energies, gradnorms = [f], [float(np.linalg.norm(gp))]
+    energies, gradnorms = prev_E + [f], prev_g + [float(np.linalg.norm(gp))]
+    save = bool(cfg.get("save", False)) and (save_dir is not None or cfg.get("dir", 0) != 0)
     S: List[np.ndarray] = []
     Y: List[np.ndarray] = []
     for it in range(iterations):
@@ -103,6 +144,8 @@ def optim_gs(H, A0, cfg: Dict[str, Any], m: int = 10, g_tol: float = 1e-6, f_tol
         gradnorms.append(float(np.linalg.norm(gp)))
         if callback:
             callback(it + 1, f, gradnorms[-1])
+        if save:
+            _save_gs(os.path.join(run_dir, "gs.npz"), x.reshape(shape, order="F"), energies, gradnorms)
         if df < f_tol * max(abs(f), 1.0):
             break
     return {"A": x.reshape(shape, order="F"), "energies": energies, "gradnorms": gradnorms, "evals": evals}

@@ -41,7 +41,7 @@ EXPORTED = [
     "ipeps_ctm_log", "ipeps_energy", "ipeps_gs_norm", "ipeps_nested_set_B", "ipeps_es_energy",
     "ipeps_all_norm", "ipeps_tcon", "ipeps_projector", "ipeps_projector_c", "ipeps_ctx_stream", "ipeps_prof_enable",
     "ipeps_prof_query", "ipeps_energy_grad", "ipeps_env_set_mixed", "ipeps_es_energy_grad",
-    "ipeps_single_dm_Ad", "ipeps_gemm_f64", "ipeps_gemm_bf16", "ipeps_mlp_create", "ipeps_mlp_destroy", "ipeps_mlp_num_params",
+    "ipeps_single_dm_Ad", "ipeps_gemm_f64", "ipeps_gemm_tf32x3", "ipeps_gemm_bf16", "ipeps_mlp_create", "ipeps_mlp_destroy", "ipeps_mlp_num_params",
     "ipeps_mlp_get_params", "ipeps_mlp_set_params", "ipeps_mlp_forward", "ipeps_mlp_grad", "ipeps_mlp_train_step",
 ]
 
@@ -121,6 +121,8 @@ def load_library(path: str = LIB_PATH) -> ct.CDLL:
         "ipeps_single_dm_Ad": [P, dp],
         "ipeps_gemm_f64": [P, ct.c_char, ct.c_char, ct.c_int64, ct.c_int64, ct.c_int64, D, dp, ct.c_int64, dp,
                            ct.c_int64, D, dp, ct.c_int64, I],
+        "ipeps_gemm_tf32x3": [P, ct.c_char, ct.c_char, ct.c_int64, ct.c_int64, ct.c_int64, D, dp, ct.c_int64, dp,
+                              ct.c_int64, D, dp, ct.c_int64, I, dp],
         "ipeps_gemm_bf16": [P, ct.c_char, ct.c_char, ct.c_int64, ct.c_int64, ct.c_int64, ct.c_float, fp,
                             ct.c_int64, fp, ct.c_int64, ct.c_float, fp, ct.c_int64],
         "ipeps_mlp_create": [P, I, I, I, I, U64, ct.POINTER(P)],
@@ -230,6 +232,50 @@ def default_config() -> Dict[str, Any]:
             "basis": False, "basis_t": "default", "basis_cut": 1e-3, "basis_name": 0,
             "es_resume": 1, "es_num": 0, "ad": True, "save": True, "part_save": False,
             "nrmB_cut": 1e-3, "wp": 1}
+
+
+def load_config(filename: Optional[str] = None) -> Dict[str, Any]:
+    """The config dict of optim_gs / prepare_basis / optim_es (optim_gs.jl:1-12,
+    optim_es.jl:22-32): TOML.parsefile(filename) when the file exists, else the
+    reference's default config.  Keys absent from the file are not added (as
+    TOML.parsefile), so a custom file must carry what the run reads."""
+    if filename and os.path.isfile(filename):
+        import tomllib
+        with open(filename, "rb") as f:
+            return tomllib.load(f)
+    return default_config()
+
+
+def get_dir(params: Dict[str, Any], cwd: Optional[str] = None) -> str:
+    """get_dir (src/utility/io.jl:72-90): simulation/$(model)_$(out_prefix)_D$(D)_X$(chi)
+    under the working directory when dir == 0, else params["dir"] (not created here)."""
+    if params.get("dir", 0) == 0:
+        return os.path.join(cwd or os.getcwd(), "simulation", "%s_%s_D%s_X%s" % (
+            params.get("model", "none"), params.get("out_prefix", "none"), params.get("D", "none"),
+            params.get("chi", "none")))
+    return str(params["dir"])
+
+
+def get_gs_name(params: Dict[str, Any], cwd: Optional[str] = None) -> str:
+    """get_gs_name (src/utility/io.jl:1-6)"""
+    return os.path.join(get_dir(params, cwd), "gs.jld2")
+
+
+def get_basis_name(params: Dict[str, Any], cwd: Optional[str] = None) -> str:
+    """get_basis_name (src/utility/io.jl:8-18)"""
+    name = params.get("basis_name", 0)
+    return os.path.join(get_dir(params, cwd), "basis.jld2" if name == 0 else f"{name}.jld2")
+
+
+def _jl_num(x) -> str:
+    """Julia's string() of a momentum: 0.1 -> "0.1", 1.0 -> "1.0", 1 -> "1"."""
+    return repr(x) if isinstance(x, float) else str(x)
+
+
+def get_es_name(params: Dict[str, Any], px, py, cwd: Optional[str] = None) -> str:
+    """get_es_name (src/utility/io.jl:20-40) for the whole-momentum file
+    (part_save = false): es_$(px)_$(py).jld2"""
+    return os.path.join(get_dir(params, cwd), f"es_{_jl_num(px)}_{_jl_num(py)}.jld2")
 
 
 def _H_pair(H):
@@ -585,6 +631,24 @@ def gemm_f64(opA: str, opB: str, A, B, alpha: float = 1.0, beta: float = 0.0, C=
     eng.check(eng.lib.ipeps_gemm_f64(eng.h, opA.encode(), opB.encode(), m, n, k, float(alpha), _dp(A), A.shape[0],
                                      _dp(B), B.shape[0], float(beta), _dp(C), C.shape[0], int(reps)))
     return C
+
+
+def gemm_tf32x3(opA: str, opB: str, A, B, alpha: float = 1.0, beta: float = 0.0, C=None,
+                engine: Optional[Engine] = None, reps: int = 1, timing: bool = False):
+    """C = alpha op(A) op(B) + beta C on the engine's 3xTF32 tcgen05 GEMM; host
+    arrays.  With timing=True returns (C, device ms of one product)."""
+    eng = engine or default_engine()
+    A = _fortran(A, np.float64)
+    B = _fortran(B, np.float64)
+    m = A.shape[0] if opA == "N" else A.shape[1]
+    k = A.shape[1] if opA == "N" else A.shape[0]
+    n = B.shape[1] if opB == "N" else B.shape[0]
+    C = np.zeros((m, n), order="F") if C is None else _fortran(C, np.float64).copy(order="F")
+    ms = np.zeros(1)
+    eng.check(eng.lib.ipeps_gemm_tf32x3(eng.h, opA.encode(), opB.encode(), m, n, k, float(alpha), _dp(A),
+                                        A.shape[0], _dp(B), B.shape[0], float(beta), _dp(C), C.shape[0], int(reps),
+                                        _dp(ms)))
+    return (C, float(ms[0])) if timing else C
 
 
 def gemm_bf16(opA: str, opB: str, A, B, alpha: float = 1.0, beta: float = 0.0, C=None,

@@ -711,6 +711,144 @@ def _hmul(H, x):
     return H.to(dt) @ x.to(dt)
 
 
+# --------------------------------------------------------------------------
+# 4x4 plaquette energy (evaluation.jl:339-398, 443-518) and its ES driver
+# (optim_es_h4.jl:133-168): H is the MPO list [s1, s2, s3, s4] of get_local_h
+# --------------------------------------------------------------------------
+
+
+def get_op_Ad4(s1, s2, s3, s4, A1d, A2d, A3d, A4d):
+    """evaluation.jl:501-518: each Ad with its MPO factor, the virtual and
+    Hamiltonian bonds fused."""
+    op1 = tcon([s1, A1d], [[-6, 1, -4], [-1, -2, -3, -5, 1]])
+    d = _shape(op1)
+    op1 = wrap_reshape(op1, d[0], d[1], d[2], d[3] * d[4], d[5])
+    op2 = tcon([s2, A2d], [[-2, -7, 1, -4], [-1, -3, -5, -6, 1]])
+    d = _shape(op2)
+    op2 = wrap_reshape(op2, d[0], d[1] * d[2], d[3] * d[4], d[5], d[6])
+    op3 = tcon([s3, A3d], [[-1, -7, 1, -3], [-2, -4, -5, -6, 1]])
+    d = _shape(op3)
+    op3 = wrap_reshape(op3, d[0] * d[1], d[2] * d[3], d[4], d[5], d[6])
+    op4 = tcon([s4, A4d], [[-4, -6, 1], [-1, -2, -3, -5, 1]])
+    d = _shape(op4)
+    op4 = wrap_reshape(op4, d[0], d[1], d[2], d[3] * d[4], d[5])
+    return op1, op2, op3, op4
+
+
+def _shape(x):
+    return tuple((x[1] if isinstance(x, NestedTensor) else x).shape)
+
+
+def _fuse3(x):
+    d = _shape(x)
+    return wrap_reshape(x, d[0] * d[1] * d[2], -1)
+
+
+def energy_norm_4x4(C1, C2, C3, C4, E1l, E1r, E2u, E2d, E3l, E3r, E4u, E4d, A1, A2, A3, A4,
+                    A1d, A2d, A3d, A4d, op1, op2, op3, op4):
+    """evaluation.jl:443-498: <H_plaquette> and the norm of the 2x2 cluster."""
+    C1E1 = tcon([C1, E1l], [[-1, 1], [1, -2, -3, -4]])
+    CEE4 = tcon([C1E1, E4u], [[1, -2, -5, -3], [1, -1, -6, -4]])
+    CEEA1 = tcon([CEE4, A1], [[-1, -2, -3, -4, 1, 2], [1, 2, -5, -6, -7]])
+    e_LU = _fuse3(tcon([CEEA1, op1], [[-1, -4, 1, 2, -2, -5, 3], [1, 2, -3, -6, 3]]))
+    n_LU = _fuse3(tcon([CEEA1, A1d], [[-1, -4, 1, 2, -2, -5, 3], [1, 2, -3, -6, 3]]))
+
+    C4E3 = tcon([C4, E3l], [[-1, 1], [1, -2, -3, -4]])
+    CEE4 = tcon([C4E3, E4d], [[1, -2, -6, -4], [-1, 1, -5, -3]])
+    CEEA4 = tcon([CEE4, A4], [[-1, -2, -3, -4, 1, 2], [-5, 1, 2, -6, -7]])
+    e_LB = _fuse3(tcon([CEEA4, op4], [[-1, -4, 1, 2, -2, -5, 3], [-3, 1, 2, -6, 3]]))
+    n_LB = _fuse3(tcon([CEEA4, A4d], [[-1, -4, 1, 2, -2, -5, 3], [-3, 1, 2, -6, 3]]))
+
+    C2E1 = tcon([C2, E1r], [[1, -2], [-1, 1, -3, -4]])
+    CEE2 = tcon([C2E1, E2u], [[-1, 1, -5, -3], [1, -2, -6, -4]])
+    CEEA2 = tcon([CEE2, A2], [[-1, -2, -3, -4, 1, 2], [1, -5, -6, 2, -7]])
+    e_RU = _fuse3(tcon([CEEA2, op2], [[-1, -4, 1, 2, -2, -5, 3], [1, -3, -6, 2, 3]]))
+    n_RU = _fuse3(tcon([CEEA2, A2d], [[-1, -4, 1, 2, -2, -5, 3], [1, -3, -6, 2, 3]]))
+
+    C3E3 = tcon([C3, E3r], [[-1, 1], [-2, 1, -3, -4]])
+    CEE2 = tcon([C3E3, E2d], [[1, -2, -5, -3], [-1, 1, -6, -4]])
+    CEEA3 = tcon([CEE2, A3], [[-1, -2, -5, -6, 1, 2], [-3, -4, 1, 2, -7]])
+    e_RB = _fuse3(tcon([CEEA3, op3], [[-1, -4, -2, -5, 1, 2, 3], [-3, -6, 1, 2, 3]]))
+    n_RB = _fuse3(tcon([CEEA3, A3d], [[-1, -4, -2, -5, 1, 2, 3], [-3, -6, 1, 2, 3]]))
+
+    e_left = tcon([wrap_permutedims(e_LU, [2, 1]), e_LB], [[-1, 1], [1, -2]])
+    e_right = tcon([e_RU, e_RB], [[-1, 1], [1, -2]])
+    energy = tcon([e_left, e_right], [[1, 2], [1, 2]])
+    n_left = tcon([wrap_permutedims(n_LU, [2, 1]), n_LB], [[-1, 1], [1, -2]])
+    n_right = tcon([n_RU, n_RB], [[-1, 1], [1, -2]])
+    norm = tcon([n_left, n_right], [[1, 2], [1, 2]])
+    return energy, norm
+
+
+def get_gs_energy_4x4(ts, H):
+    """evaluation.jl:339-356"""
+    s1, s2, s3, s4 = H
+    C1, C2, C3, C4 = ts.Cs
+    E1, E2, E3, E4 = ts.Es
+    A, Ad = ts.A, ts.Ad
+    ops = get_op_Ad4(s1, s2, s3, s4, Ad, Ad, Ad, Ad)
+    energy, norm = energy_norm_4x4(C1, C2, C3, C4, E1, E1, E2, E2, E3, E3, E4, E4, A, A, A, A,
+                                   Ad, Ad, Ad, Ad, *ops)
+    return energy / norm
+
+
+def get_es_energy_4x4(ts, H):
+    """evaluation.jl:358-398: component 4 of the nested energy over component 1 of the norm."""
+    s1, s2, s3, s4 = H
+    A, Ad = get_all_A(ts), get_all_Ad(ts)
+    C1, C2, C3, C4 = get_all_Cs(ts)
+    E1, E2, E3, E4 = get_all_Es(ts)
+    px = ts.Params.get("px", 0.0)
+    py = ts.Params.get("py", 0.0)
+    A1, A2, A3, A4 = A, A, A, A
+    A1d, A2d, A3d, A4d = Ad, Ad, Ad, Ad
+    E1r = shift(E1, px)
+    A2, A2d = shift(A2, px), shift(A2d, px)
+    A3, A3d = shift(A3, px), shift(A3d, px)
+    E3r = shift(E3, px)
+    C2 = shift(C2, px)
+    C3 = shift(C3, px)
+    E2u = shift(E2, px)
+    E2d = shift(E2, px)
+    C4 = shift(C4, py)
+    C3 = shift(C3, py)
+    E3l = shift(E3, py)
+    E3r = shift(E3r, py)
+    E4d = shift(E4, py)
+    E2d = shift(E2d, py)
+    A4, A4d = shift(A4, py), shift(A4d, py)
+    A3, A3d = shift(A3, py), shift(A3d, py)
+    ops = get_op_Ad4(s1, s2, s3, s4, A1d, A2d, A3d, A4d)
+    energy, norm = energy_norm_4x4(C1, C2, C3, C4, E1, E1r, E2u, E2d, E3l, E3r, E4, E4d, A1, A2, A3, A4,
+                                   A1d, A2d, A3d, A4d, *ops)
+    return energy[4] / norm[1]
+
+
+def run_es_h4(ts, H, B):
+    """optim_es_h4.jl:159-168"""
+    ts1 = ts.replace(B=B, Bd=conj(B))
+    ts1, _ = run_ctm(ts1, conv_fun=lambda t: get_es_energy_4x4(t, H) / get_all_norm(t)[0])
+    return get_es_energy_4x4(ts1, H), ts1
+
+
+def get_es_grad_h4(ts, H, Bi):
+    """optim_es_h4.jl:133-157: (gH, gN) as flat complex vectors (column-major)."""
+    B = freshape(Bi, *ts.A.shape)
+    ts1 = ts.replace(B=B, Bd=conj(B))
+    with torch.no_grad():
+        ts1, _ = run_ctm(ts1, conv_fun=lambda t: get_es_energy_4x4(t, H) / get_all_norm(t)[0])
+    ts1 = _detach_ts(ts1)
+    p = dict(ts1.Params)
+    p["max_iter"] = p.get("ad_max_iter", 4)
+    ts1 = ts1.replace(Params=p)
+    Bv = B.detach().clone().requires_grad_(True)
+    y, ts2 = run_es_h4(ts1, H, Bv)
+    (gH,) = torch.autograd.grad(y.real if torch.is_complex(y) else y, Bv)
+    with torch.no_grad():
+        Nb, gN = get_all_norm(_detach_ts(ts2))
+    return freshape(gH.detach(), -1), freshape(gN.detach(), -1)
+
+
 def get_gs_norm(ts):
     """evaluation.jl:47-59"""
     n_dm = get_single_dm(*ts.Cs, *ts.Es)

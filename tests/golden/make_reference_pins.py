@@ -9,11 +9,12 @@ computed:
 * gs.jld2 (the last optim_gs run of test/optim_gs.jl: honeycomb XX model,
   complex A of shape (2,2,2,2,4), default config chi=32): the optimised A and
   the energy of fg! at it (energies[end]).
-* basis.jld2 + es_{px}_{py}.jld2 (test/optim_es.jl, D=2 d=2): the normalised
-  ground state with its converged environment (ts.A, ts.Cs, ts.Es), the
-  tangent basis, and effN = basis' * gN per momentum (optim_es.jl:140-141).
-  (effH is not pinned: basis.jld2 stores the Hamiltonian in a form the
-  current reference code no longer produces.)
+* basis.jld2 + es_{px}_{py}.jld2 (the plaquette excited-state driver,
+  optim_es_h4.jl, D=2 d=2): the normalised ground state with its converged
+  environment (ts.A, ts.Cs, ts.Es), the tangent basis, the plaquette
+  Hamiltonian with E0 subtracted as the MPO list [s1, s2, s3, s4] of
+  get_local_h (basis.jld2 "H"), and effH = basis' * gH / 2,
+  effN = basis' * gN per momentum (optim_es_h4.jl:104-107).
 
 Usage (reads the reference tree, so it runs where that tree is):
     python tests/golden/make_reference_pins.py /path/to/iPEPS.jl
@@ -44,9 +45,12 @@ def main(ref_root):
     for k in range(4):
         out[f"es_C{k + 1}"] = ts["Cs"][k]
         out[f"es_E{k + 1}"] = ts["Es"][k]
+    for k in range(4):
+        out[f"es_H{k + 1}"] = b["H"][k]
     for px, py in MOMENTA:
         e = jld2.load(os.path.join(sim, f"es_{px}_{py}.jld2"))
         out[f"effN_{px}_{py}"] = e["effN"]
+        out[f"effH_{px}_{py}"] = e["effH"]
     np.savez_compressed(os.path.join(HERE, "ref_pins.npz"), **out)
     print({k: v.shape for k, v in out.items()})
 

@@ -6,9 +6,10 @@ tests/golden/make_reference_pins.py).
   XX model, complex A (2,2,2,2,4), default config chi = 32): reproduced to
   1e-12 (converge from init_ctm1 with the energy criterion, then the
   ad_max_iter = 4 iterations of run_gs and get_gs_energy, optim_gs.jl:53-91).
-* es_{px}_{py}.jld2: effN = basis' * gN of optim_es (optim_es.jl:127-153)
-  from the saved normalised ground-state environment and tangent basis:
-  three columns at two momenta reproduced to 1e-9 relative.
+* es_{px}_{py}.jld2 (written by the plaquette driver optim_es_h4):
+  effH = basis' * gH / 2 and effN = basis' * gN (optim_es_h4.jl:104-107) from
+  the saved normalised ground-state environment, tangent basis and plaquette
+  MPO: two columns at two momenta reproduced to 1e-9 relative.
 """
 import importlib.util
 import math
@@ -48,20 +49,36 @@ def test_oracle_reproduces_reference_gs_energy():
     assert abs(complex(E).real - p["gs_energies"][-1]) <= 1e-12, (complex(E).real, p["gs_energies"][-1])
 
 
+def es_H(p):
+    return [torch.tensor(p[f"es_H{k}"]) for k in range(1, 5)]
+
+
 @pytest.mark.parametrize("mom", [("0.1", "0"), ("1", "1")])
-def test_oracle_reproduces_reference_effN(mom):
+def test_oracle_reproduces_reference_effH_effN(mom):
+    """get_es_grad_h4 (optim_es_h4.jl:133-157) with the saved plaquette MPO:
+    the nested CTMRG, the pullback w.r.t. B and get_all_norm."""
     p = pins()
     ts = es_ts(p)
     basis = p["es_basis"]
-    H2 = O.substract_gs_energy(ts, O.ising(2.0))
+    H = es_H(p)
     prm = dict(ts.Params)
     prm.update(px=float(mom[0]) * math.pi, py=float(mom[1]) * math.pi)
     t1 = ts.replace(Params=prm)
-    ref = p[f"effN_{mom[0]}_{mom[1]}"]
-    for i in (0, 15, 30):
-        _, gN = O.get_es_grad(t1, H2, torch.tensor(basis[:, i]))
-        col = basis.conj().T @ gN.resolve_conj().numpy()
-        assert np.linalg.norm(col - ref[:, i]) <= 1e-9 * np.linalg.norm(ref[:, i]), (mom, i)
+    refH, refN = p[f"effH_{mom[0]}_{mom[1]}"], p[f"effN_{mom[0]}_{mom[1]}"]
+    for i in (0, 30):
+        gH, gN = O.get_es_grad_h4(t1, H, torch.tensor(basis[:, i]))
+        colH = basis.conj().T @ gH.resolve_conj().numpy() / 2
+        colN = basis.conj().T @ gN.resolve_conj().numpy()
+        assert np.linalg.norm(colH - refH[:, i]) <= 1e-9 * np.linalg.norm(refH[:, i]), (mom, i)
+        assert np.linalg.norm(colN - refN[:, i]) <= 1e-9 * np.linalg.norm(refN[:, i]), (mom, i)
+
+
+def test_oracle_plaquette_energy_of_subtracted_hamiltonian_vanishes():
+    """The saved MPO is get_local_h(h4 - E0 hI) (optim_es_h4.jl:170-183): its
+    4x4 ground-state energy on the saved environment is 0."""
+    p = pins()
+    E = O.get_gs_energy_4x4(es_ts(p), es_H(p))
+    assert abs(complex(E)) <= 1e-12
 
 
 @pytest.mark.skipif(not os.path.isdir(REF), reason="reference tree not present")
