@@ -577,6 +577,32 @@ def run_gemm_shapes():
     return 0
 
 
+def run_tf32_shapes():
+    """ipeps_gemm_tf32x3 (3xTF32 on tcgen05: operand splits + GEMM, device time
+    by CUDA events, mean over 10 repetitions) on the engine's shapes; credited
+    flops are 2MNK of the FP64-equivalent product, against the TF32 tensor
+    peak / 3 (three split products per credited flop)."""
+    pkg = load_pkg()
+    eng = pkg.Engine(0)
+    peaks, kind = measured_peaks()
+    key = "bf16_tflops"
+    peak = peaks[key] / 2 / 3
+    shapes = [("N", "N", 2500, 160, 2500), ("T", "N", 2500, 160, 2500), ("T", "N", 160, 160, 2500),
+              ("N", "N", 2500, 2500, 100), ("N", "N", 250000, 50, 25), ("N", "T", 4096, 4096, 4096),
+              ("N", "N", 8192, 8192, 8192)]
+    rng = np.random.default_rng(0)
+    for oa, ob, m, n, k in shapes:
+        A = rng.standard_normal((m, k) if oa == "N" else (k, m))
+        B = rng.standard_normal((k, n) if ob == "N" else (n, k))
+        _, ms = pkg.host.gemm_tf32x3(oa, ob, A, B, engine=eng, reps=11, timing=True)
+        fl = 2.0 * m * n * k
+        print(json.dumps({"op": oa + ob, "m": m, "n": n, "k": k, "us": round(ms * 1e3, 1),
+                          "tflops": round(fl / (ms / 1e3) / 1e12, 2),
+                          "frac_of_peak": round(fl / (ms / 1e3) / 1e12 / peak, 3),
+                          "peak": round(peak, 1), "peak_source": f"{kind} {key} / 2 / 3"}), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -592,9 +618,13 @@ def main():
     ap.add_argument("--gemm-shapes", action="store_true",
                     help="kernel aid: FP64 GEMM throughput of the engine's DMMA kernel and of cuBLAS on the "
                          "projector's and the contractions' shapes, one JSON line per shape")
+    ap.add_argument("--tf32-shapes", action="store_true",
+                    help="kernel aid: 3xTF32 tcgen05 GEMM throughput (splits included) on the engine's shapes")
     args = ap.parse_args()
     if args.gemm_shapes:
         return run_gemm_shapes()
+    if args.tf32_shapes:
+        return run_tf32_shapes()
     global WORKLOAD, WORKLOAD_NAME
     WORKLOAD = WORKLOADS[args.workload]
     WORKLOAD_NAME = workload_name(WORKLOAD)

@@ -177,6 +177,27 @@ IPEPS_API int ipeps_all_norm(ipeps_env* env, double* Nb, double* envB);
 IPEPS_API int ipeps_es_energy_grad(ipeps_env* env, const double* Hh, const double* Hv, int d2, int ad_iters,
                                    double* E, double* gB);
 
+/* ---- plaquette (4x4 cluster) observables of the h4 drivers (src/graph/evaluation.jl:339-398,
+ * 443-518; src/optimize/optim_gs_h4.jl, optim_es_h4.jl).  The plaquette Hamiltonian is the
+ * MPO [s1, s2, s3, s4] of get_local_h (src/model/local_h.jl:1-31): s1 (d,d,a), s2 (a,d,d,b),
+ * s3 (b,d,d,c), s4 (c,d,d), each a complex128 column-major array. */
+typedef struct {
+  const double* data; /* interleaved (re, im) */
+  int nd;
+  int64_t dims[4];
+} ipeps_ctensor_t;
+/* nested = 0: get_gs_energy_4x4 (evaluation.jl:339-356); nested = 1: get_es_energy_4x4
+ * (evaluation.jl:358-398, needs B).  E receives the complex value (2 doubles). */
+IPEPS_API int ipeps_energy_4x4(ipeps_env* env, const ipeps_ctensor_t* H4, int nested, double* E);
+/* run_ctm with conv_fun = get_gs_energy_4x4 (nested = 0) or get_es_energy_4x4 / get_all_norm
+ * (nested = 1) (optim_es_h4.jl:33,139); as ipeps_ctm_run otherwise. */
+IPEPS_API int ipeps_ctm_run_4x4(ipeps_env* env, const ipeps_ctensor_t* H4, int nested, int* iters,
+                                double* last_diff, int* converged);
+/* Pullback of run_es_h4 w.r.t. B (get_es_grad_h4, optim_es_h4.jl:133-168): as
+ * ipeps_es_energy_grad with the plaquette energy; E = real(get_es_energy_4x4). */
+IPEPS_API int ipeps_es_energy_grad_4x4(ipeps_env* env, const ipeps_ctensor_t* H4, int ad_iters, double* E,
+                                       double* gB);
+
 /* ---- learned warm start (no counterpart in the reference: its CTMRG always starts
  * from init_ctm1, ctm_tensor.jl:97-130).  A 3-layer perceptron n_in -> n_hidden ->
  * n_hidden -> n_out (GELU) whose matrix products run on BF16 tensor-core GEMMs
@@ -208,6 +229,17 @@ IPEPS_API int ipeps_mlp_train_step(ipeps_mlp* mlp, const float* X, const float* 
 IPEPS_API int ipeps_gemm_f64(ipeps_ctx* ctx, char opA, char opB, int64_t m, int64_t n, int64_t k, double alpha,
                              const double* A, int64_t lda, const double* B, int64_t ldb, double beta, double* C,
                              int64_t ldc, int reps);
+
+/* ---- 3xTF32 GEMM on the tcgen05 tensor cores (no counterpart in the reference: the
+ * contraction kernel of the mixed form, exposed for tests and kernel timing).
+ * C = alpha*op(A)*op(B) + beta*C, column-major FP64 host arrays, op in {'N','T'}: each
+ * operand is split into TF32 hi/lo planes, the products lo*hi + hi*lo + hi*hi accumulate
+ * in FP32 in tensor memory, split-K partial sums in FP64.  The product runs `reps` times
+ * from the same input C; *ms_per_rep (optional) receives the device time of one product
+ * (splits included; the first repetition is excluded when reps > 1). */
+IPEPS_API int ipeps_gemm_tf32x3(ipeps_ctx* ctx, char opA, char opB, int64_t m, int64_t n, int64_t k, double alpha,
+                                const double* A, int64_t lda, const double* B, int64_t ldb, double beta, double* C,
+                                int64_t ldc, int reps, double* ms_per_rep);
 
 /* ---- allocation-free FP64 GEMM (no counterpart in the reference).
  * C = alpha*op(A)*op(B) + beta*C, column-major, op in {'N','T'}; A, B, C are

@@ -1,6 +1,8 @@
 // Reverse-mode tape, backward rules, the truncated-SVD projector adjoint and
 // the energy + gradient driver.
 #include "ad.cuh"
+
+#include <cstdlib>
 #include "linalg.cuh"
 #include "moves.cuh"
 
@@ -546,12 +548,20 @@ struct IterCk {
 double energy_grad(Env& e, const Tensor& Hh, const Tensor& Hv, int ad_iters, Tensor* gA) {
   Ctx& c = *e.ctx;
   IPEPS_CHECK(e.dt == DType::F64 && !e.nested, "energy_grad: real single-site A only");
-  // The pullback runs in FP64 in both forms.  Recomputing the enlarged corners
-  // with 3xTF32 contractions inside the backward perturbs them at ~1e-7
-  // relative, and the truncated-SVD adjoint amplifies that through its
-  // 1/(s_i^2 - s_j^2) terms to gradient errors of a few 1e-6; the mixed form
-  // gains its speed in the convergence iterations before this call.
-  Fp64Scope fp64_all(c);
+  // Mixed form: the checkpointed iterations and their recomputation on the
+  // tapes run in the context's precision (deterministic 3xTF32 products, so
+  // the recomputed enlarged corners equal the ones the saved projector
+  // factors were computed from), the energy and its seed in FP64.
+  // ad_fp64 keeps the whole pullback in FP64.
+  const int prec = c.precision;
+  const char* adenv = std::getenv("IPEPS_MIXED_AD");
+  const bool ad_fp64 = !(adenv && adenv[0] == '1');
+  if (ad_fp64) c.precision = kPrecFP64;
+  struct RestorePrec {
+    Ctx& c;
+    int p;
+    ~RestorePrec() { c.precision = p; }
+  } restore_prec{c, prec};
   // forward: ad_iters iterations with checkpoints of C/T and the projector factors
   std::vector<IterCk> ck;
   {
@@ -581,8 +591,9 @@ double energy_grad(Env& e, const Tensor& Hh, const Tensor& Hv, int ad_iters, Ten
   Tensor gAcc, gAdc;
   double Ere = 0;
   {
-    Fp64Scope fp64(c);  // the energy and its seed in FP64 in both forms
     Tape tp(c);
+    const int prec_bw = c.precision;
+    c.precision = kPrecFP64;  // the energy and its seed in FP64 in both forms
     ADPolicy p{tp};
     AV C[4], E[4];
     for (int i = 0; i < 4; ++i) {
@@ -611,6 +622,7 @@ double energy_grad(Env& e, const Tensor& Hh, const Tensor& Hv, int ad_iters, Ten
     IPEPS_CHECK(roh.t.dt == DType::F64, "energy_grad: real density matrices expected");
     tp.acc(roh.id, seed(Hh, roh.t, Eh, t[0].tr.real()));
     tp.acc(rov.id, seed(Hv, rov.t, Ev, t[1].tr.real()));
+    c.precision = prec_bw;  // cotangents in the pullback's precision
     tp.backward();
     for (int i = 0; i < 4; ++i) {
       gC[i] = tp.grad(C[i].id);

@@ -71,6 +71,9 @@ double energy_grad(Env& e, const Tensor& Hh, const Tensor& Hv, int ad_iters, Ten
 // Pullback of run_es (optim_es.jl:196-210) with respect to B from the nested
 // environment held by e: runs ad_iters nested iterations, returns
 // get_es_energy and gH = dE/dB (complex, convention dE/dRe + i dE/dIm).
-double es_energy_grad(Env& e, const Tensor& Hh, const Tensor& Hv, int ad_iters, Tensor* gB);
+// h4 (optional): the plaquette energy get_es_energy_4x4 instead of the bond
+// energies (run_es_h4 / get_es_grad_h4, optim_es_h4.jl:133-168); Hh, Hv unused then
+double es_energy_grad(Env& e, const Tensor& Hh, const Tensor& Hv, int ad_iters, Tensor* gB,
+                      const std::array<Tensor, 4>* h4 = nullptr);
 
 }  // namespace ipeps

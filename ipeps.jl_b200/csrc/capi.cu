@@ -543,6 +543,73 @@ extern "C" int ipeps_es_energy_grad(ipeps_env* env, const double* Hh, const doub
   });
 }
 
+namespace {
+
+ipeps::H4 upload_H4(ipeps::Ctx& c, const ipeps_ctensor_t* H) {
+  IPEPS_CHECK(H != nullptr, "plaquette Hamiltonian required");
+  static const int want_nd[4] = {3, 4, 4, 3};
+  ipeps::H4 h;
+  for (int k = 0; k < 4; ++k) {
+    IPEPS_CHECK(H[k].data && H[k].nd == want_nd[k], "plaquette MPO factor " + std::to_string(k + 1) +
+                                                        ": expected a " + std::to_string(want_nd[k]) + "-d tensor");
+    std::vector<int64_t> dims(H[k].dims, H[k].dims + H[k].nd);
+    for (int64_t d : dims) IPEPS_CHECK(d > 0, "plaquette MPO factor with an empty dimension");
+    h[k] = upload(c, H[k].data, DType::C128, dims);
+  }
+  IPEPS_CHECK(h[0].dims[2] == h[1].dims[0] && h[1].dims[3] == h[2].dims[0] && h[2].dims[3] == h[3].dims[0],
+              "plaquette MPO bond dimensions do not chain");
+  return h;
+}
+
+}  // namespace
+
+extern "C" int ipeps_energy_4x4(ipeps_env* env, const ipeps_ctensor_t* H4, int nested, double* E) {
+  if (!env) return IPEPS_EINVAL;
+  return guarded(env->owner, [&] {
+    ipeps::H4 h = upload_H4(*env->e.ctx, H4);
+    std::complex<double> v = nested ? ipeps::es_energy_4x4(env->e, h) : ipeps::gs_energy_4x4(env->e, h);
+    if (E) { E[0] = v.real(); E[1] = v.imag(); }
+    return IPEPS_OK;
+  });
+}
+
+extern "C" int ipeps_ctm_run_4x4(ipeps_env* env, const ipeps_ctensor_t* H4, int nested, int* iters,
+                                 double* last_diff, int* converged) {
+  if (!env) return IPEPS_EINVAL;
+  return guarded(env->owner, [&] {
+    ipeps::H4 h = upload_H4(*env->e.ctx, H4);
+    uint64_t m0 = env->e.moves;
+    double s0 = env->e.move_seconds;
+    bool conv = false;
+    double diff = 0;
+    int it = ipeps::run_ctm(env->e, nested ? ipeps::kConvEs4x4 : ipeps::kConvEnergy4x4, nullptr, nullptr, &diff,
+                            &conv, &h);
+    account(env, m0, s0);
+    if (iters) *iters = it;
+    if (last_diff) *last_diff = diff;
+    if (converged) *converged = conv ? 1 : 0;
+    return IPEPS_OK;
+  });
+}
+
+extern "C" int ipeps_es_energy_grad_4x4(ipeps_env* env, const ipeps_ctensor_t* H4, int ad_iters, double* E,
+                                        double* gB) {
+  if (!env) return IPEPS_EINVAL;
+  return guarded(env->owner, [&] {
+    IPEPS_CHECK(ad_iters >= 1, "ad_iters must be >= 1");
+    auto& c = *env->e.ctx;
+    ipeps::H4 h = upload_H4(c, H4);
+    uint64_t m0 = env->e.moves;
+    double s0 = env->e.move_seconds;
+    Tensor g, none;
+    double e = ipeps::es_energy_grad(env->e, none, none, ad_iters, &g, &h);
+    account(env, m0, s0);
+    if (E) *E = e;
+    if (gB) download(c, gB, g);
+    return IPEPS_OK;
+  });
+}
+
 extern "C" int ipeps_single_dm_Ad(ipeps_env* env, double* out) {
   if (!env) return IPEPS_EINVAL;
   return guarded(env->owner, [&] {
@@ -603,6 +670,42 @@ int ipeps_gemm_f64(ipeps_ctx* ctx, char opA, char opB, int64_t m, int64_t n, int
       ipeps::gemm_f64_dmma(c, opA, opB, m, n, k, alpha, static_cast<double*>(dA.p), lda, static_cast<double*>(dB.p),
                            ldb, beta, static_cast<double*>(dC.p), ldc);
     }
+    d2h(c, C, dC.p, dC.bytes);
+    c.sync();
+    return IPEPS_OK;
+  });
+}
+
+int ipeps_gemm_tf32x3(ipeps_ctx* ctx, char opA, char opB, int64_t m, int64_t n, int64_t k, double alpha,
+                      const double* A, int64_t lda, const double* B, int64_t ldb, double beta, double* C,
+                      int64_t ldc, int reps, double* ms_per_rep) {
+  return guarded(ctx, [&] {
+    IPEPS_CHECK(A && B && C && m > 0 && n > 0 && k > 0 && reps >= 1, "bad gemm_tf32x3 arguments");
+    IPEPS_CHECK((opA == 'N' || opA == 'T') && (opB == 'N' || opB == 'T'), "gemm_tf32x3: op must be 'N' or 'T'");
+    auto& c = *ctx->c;
+    const int64_t acols = (opA == 'N') ? k : m, bcols = (opB == 'N') ? n : k;
+    IPEPS_CHECK(lda >= ((opA == 'N') ? m : k) && ldb >= ((opB == 'N') ? k : n) && ldc >= m, "bad leading dimension");
+    ipeps::DBuf dA(size_t(lda * acols) * 8, c.sh), dB(size_t(ldb * bcols) * 8, c.sh), dC(size_t(ldc * n) * 8, c.sh),
+        dC0(size_t(ldc * n) * 8, c.sh);
+    h2d(c, dA.p, A, dA.bytes);
+    h2d(c, dB.p, B, dB.bytes);
+    h2d(c, dC0.p, C, dC0.bytes);
+    cudaEvent_t e0 = c.take_event(), e1 = c.take_event();
+    float total = 0;
+    for (int r = 0; r < reps; ++r) {
+      IPEPS_CUDA(cudaMemcpyAsync(dC.p, dC0.p, dC.bytes, cudaMemcpyDeviceToDevice, c.stream));
+      IPEPS_CUDA(cudaEventRecord(e0, c.stream));
+      ipeps::gemm_tf32x3(c, opA, opB, m, n, k, alpha, static_cast<double*>(dA.p), lda, static_cast<double*>(dB.p),
+                         ldb, beta, static_cast<double*>(dC.p), ldc);
+      IPEPS_CUDA(cudaEventRecord(e1, c.stream));
+      IPEPS_CUDA(cudaEventSynchronize(e1));
+      float t = 0;
+      IPEPS_CUDA(cudaEventElapsedTime(&t, e0, e1));
+      if (r > 0 || reps == 1) total += t;
+    }
+    c.ev_pool.push_back(e0);
+    c.ev_pool.push_back(e1);
+    if (ms_per_rep) *ms_per_rep = double(total) / double(reps > 1 ? reps - 1 : 1);
     d2h(c, C, dC.p, dC.bytes);
     c.sync();
     return IPEPS_OK;

@@ -191,7 +191,7 @@ std::vector<double> ctm_move(Env& e, int dir, ProjResult* keep) {
   {
     QuarterPair<NTPolicy> q = quarters(p, dir, Cs0, Es0, NT(e.A), NT(e.Ad));
     MatRef R1{q.R1.c[0], q.t1}, R2{q.R2.c[0], q.t2};
-    pr = get_projector(c, R1, R2, e.prm.chi, e.prm.svd, &e.cache[dir], keep != nullptr);
+    pr = get_projector(c, R1, R2, e.prm.chi, e.prm.svd, &e.cache[dir], keep != nullptr && e.keep_adjoint);
   }
   Arr4<NTPolicy> Cs, Es;
   for (int i = 0; i < 4; ++i) {
@@ -408,8 +408,13 @@ std::vector<Traces> dm_traces(Ctx& c, const std::vector<std::pair<Tensor, Tensor
 }
 
 // evaluation.jl:15-29 with get_dms (only_gs) evaluation.jl:124-156
-void gs_energy(Env& e, const Tensor& Hh, const Tensor& Hv, std::complex<double>* E, std::complex<double>* Na) {
+void gs_energy(Env& e, const Tensor& Hh, const Tensor& Hv, std::complex<double>* E, std::complex<double>* Na,
+               bool ctx_precision) {
+  // FP64 contractions unless the caller asks for the context's precision (the
+  // mixed form's convergence energies of its 3xTF32 iterations); the traces are FP64
+  const int prec = e.ctx->precision;
   Fp64Scope fp64(*e.ctx);
+  if (ctx_precision) e.ctx->precision = prec;
   Ctx& c = *e.ctx;
   NTPolicy p{c};
   NT C1(e.Cs[0]), C2(e.Cs[1]), C3(e.Cs[2]), C4(e.Cs[3]);
@@ -504,6 +509,38 @@ std::complex<double> all_norm(Env& e, Tensor* envB) {
   return scalar_of(c, Nb) / n1;
 }
 
+// evaluation.jl:339-356 (get_gs_energy_4x4): <H_plaquette> / <1> of the
+// 2 x 2 cluster, H given as the MPO [s1, s2, s3, s4] of get_local_h
+std::complex<double> gs_energy_4x4(Env& e, const H4& h) {
+  Fp64Scope fp64(*e.ctx);
+  Ctx& c = *e.ctx;
+  NTPolicy p{c};
+  Arr4<NTPolicy> s{NT(h[0]), NT(h[1]), NT(h[2]), NT(h[3])};
+  NT A(e.A), Ad(e.Ad);
+  Arr4<NTPolicy> As{A, A, A, A}, Ads{Ad, Ad, Ad, Ad};
+  Arr4<NTPolicy> op = get_op_Ad4(p, s, Ads);
+  NT C1(e.Cs[0]), C2(e.Cs[1]), C3(e.Cs[2]), C4(e.Cs[3]);
+  NT E1(e.Es[0]), E2(e.Es[1]), E3(e.Es[2]), E4(e.Es[3]);
+  auto en = energy_norm_4x4(p, C1, C2, C3, C4, E1, E1, E2, E2, E3, E3, E4, E4, As, Ads, op);
+  return scalar_of(c, en[0].c[0]) / scalar_of(c, en[1].c[0]);
+}
+
+// evaluation.jl:358-398 (get_es_energy_4x4): component 4 of the nested
+// plaquette energy over component 1 of the norm
+std::complex<double> es_energy_4x4(Env& e, const H4& h) {
+  Fp64Scope fp64(*e.ctx);
+  Ctx& c = *e.ctx;
+  IPEPS_CHECK(e.nested, "es_energy_4x4: no B set");
+  NTPolicy p{c};
+  Arr4<NTPolicy> s{NT(h[0]), NT(h[1]), NT(h[2]), NT(h[3])};
+  Arr4<NTPolicy> C{e.all_C(0), e.all_C(1), e.all_C(2), e.all_C(3)};
+  Arr4<NTPolicy> E{e.all_E(0), e.all_E(1), e.all_E(2), e.all_E(3)};
+  auto sh = [&](const NT& x, double ph) { return nshift(c, x, ph); };
+  auto en = es_plaquette(p, sh, s, e.all_A(), e.all_Ad(), C, E, e.px, e.py);
+  IPEPS_CHECK(en[0].has(3), "es_energy_4x4: empty fourth component");
+  return scalar_of(c, en[0].c[3]) / scalar_of(c, en[1].c[0]);
+}
+
 namespace {
 
 // Moves the counters and timing records of `from` into `to`.
@@ -529,13 +566,15 @@ void merge_stats(Ctx& to, Ctx& from) {
 
 // The convergence value of run_ctm: get_gs_energy (mode 0) or
 // get_es_energy / get_all_norm (mode 2).
-std::complex<double> conv_value(Env& e, int conv_mode, const Tensor& Hh, const Tensor& Hv) {
-  if (conv_mode == 0) {
+std::complex<double> conv_value(Env& e, int conv_mode, const Tensor* Hh, const Tensor* Hv, const H4* h4) {
+  if (conv_mode == kConvEnergy) {
     std::complex<double> E, Na;
-    gs_energy(e, Hh, Hv, &E, &Na);
+    gs_energy(e, *Hh, *Hv, &E, &Na, true);
     return E;
   }
-  return es_energy(e, Hh, Hv) / all_norm(e, nullptr);
+  if (conv_mode == kConvEnergy4x4) return gs_energy_4x4(e, *h4);
+  if (conv_mode == kConvEs4x4) return es_energy_4x4(e, *h4) / all_norm(e, nullptr);
+  return es_energy(e, *Hh, *Hv) / all_norm(e, nullptr);
 }
 
 // One convergence evaluation in flight on the evaluation context, from its own
@@ -544,8 +583,9 @@ std::complex<double> conv_value(Env& e, int conv_mode, const Tensor& Hh, const T
 struct PendingConv {
   Env& e;
   int conv_mode;
-  const Tensor& Hh;
-  const Tensor& Hv;
+  const Tensor* Hh;
+  const Tensor* Hv;
+  const H4* h4;
   bool active = false;
   std::thread th;
   std::complex<double> val;
@@ -555,7 +595,8 @@ struct PendingConv {
   uint64_t rng1 = 0, rng2 = 0;
   int iter = 0;
 
-  PendingConv(Env& env, int mode, const Tensor& hh, const Tensor& hv) : e(env), conv_mode(mode), Hh(hh), Hv(hv) {}
+  PendingConv(Env& env, int mode, const Tensor* hh, const Tensor* hv, const H4* h)
+      : e(env), conv_mode(mode), Hh(hh), Hv(hv), h4(h) {}
   ~PendingConv() {
     if (th.joinable()) th.join();
   }
@@ -565,6 +606,7 @@ struct PendingConv {
     Ctx& c3 = *e.aux_eval;
     c3.prof = c1.prof;
     c3.d_status = c1.d_status;
+    c3.precision = c1.precision;  // the energy of an iteration in that iteration's precision
     snap = e;
     s = sp;
     iter = it;
@@ -583,7 +625,7 @@ struct PendingConv {
     th = std::thread([this, &c3, ev]() mutable {
       try {
         IPEPS_CUDA(cudaSetDevice(c3.device));
-        val = conv_value(ev, conv_mode, Hh, Hv);
+        val = conv_value(ev, conv_mode, Hh, Hv, h4);
       } catch (...) {
         err = std::current_exception();
       }
@@ -623,7 +665,12 @@ struct PendingConv {
 }  // namespace
 
 // ctmrg.jl:1-55
-int run_ctm(Env& e, int conv_mode, const Tensor* Hh, const Tensor* Hv, double* last_diff, bool* converged) {
+int run_ctm(Env& e, int conv_mode, const Tensor* Hh, const Tensor* Hv, double* last_diff, bool* converged,
+            const H4* h4) {
+  const bool by_value = conv_mode != kConvSpectrum;
+  IPEPS_CHECK(!by_value || ((conv_mode == kConvEnergy4x4 || conv_mode == kConvEs4x4) ? h4 != nullptr
+                                                                                    : (Hh && Hv)),
+              "run_ctm: Hamiltonian missing for the convergence criterion");
   std::vector<double> diffs{1.0};
   std::complex<double> conv = 1.0;
   std::vector<double> conv_s{1.0};
@@ -645,13 +692,13 @@ int run_ctm(Env& e, int conv_mode, const Tensor* Hh, const Tensor* Hv, double* l
     int p;
     ~Restore() { c.precision = p; }
   } restore{c, prec0};
-  if ((conv_mode == 0 || conv_mode == 2) && e.parallel_moves) {
+  if (by_value && e.parallel_moves) {
     // Pipelined: the energy of iteration i is evaluated while iteration i+1
     // runs.  When iteration i turns out converged, iteration i+1 is rolled
     // back, so the returned environment and log are those of the sequential
     // loop.  In the mixed form the switch to FP64 sees the change per
     // iteration one iteration later than the sequential loop does.
-    PendingConv pc(e, conv_mode, *Hh, *Hv);
+    PendingConv pc(e, conv_mode, Hh, Hv, h4);
     std::vector<int> fp64_upto(size_t(std::max(e.prm.max_iter, 0)) + 2, 0);
     auto record = [&](std::complex<double> v) {
       const std::complex<double> old = conv;
@@ -691,16 +738,9 @@ int run_ctm(Env& e, int conv_mode, const Tensor* Hh, const Tensor* Hv, double* l
     std::vector<double> s = rg_step(e);
     if (polish && c.precision == kPrecFP64) fp64_done++;
     CtmLogEntry le{i, 0, 0, 0, int(s.size())};
-    if (conv_mode == 0 || conv_mode == 2) {
+    if (by_value) {
       std::complex<double> old = conv;
-      if (conv_mode == 0) {
-        std::complex<double> E, Na;
-        gs_energy(e, *Hh, *Hv, &E, &Na);
-        conv = E;
-      } else {
-        double Ees = es_energy(e, *Hh, *Hv);
-        conv = Ees / all_norm(e, nullptr);
-      }
+      conv = conv_value(e, conv_mode, Hh, Hv, h4);
       diffs.push_back(std::abs(conv - old));
       le.obj_re = conv.real();
       le.obj_im = conv.imag();

@@ -66,6 +66,10 @@ struct Env {
   // disjoint environment slots.  The second move of a pair runs on `aux`, a
   // context with its own stream (created on first use).
   bool parallel_moves = true;
+  // moves that keep their projector (keep != nullptr) also keep the resolved
+  // singular triplets for the projector adjoint; the nested pullback needs
+  // P1/P2 only (complex environments have no projector adjoint)
+  bool keep_adjoint = true;
   std::shared_ptr<Ctx> aux;
   // run_ctm evaluates the convergence criterion of iteration i on `aux_eval`
   // (a third stream, its own host thread) while iteration i+1 runs; a
@@ -95,7 +99,9 @@ std::vector<double> rg_step(Env& e);
 // projectors with their resolved triplets.  Returns the left-move spectrum.
 std::vector<double> ctm_moves4(Env& e, ProjResult* keep);
 // energy (evaluation.jl:15-29): E (complex) and Na (complex)
-void gs_energy(Env& e, const Tensor& Hh, const Tensor& Hv, std::complex<double>* E, std::complex<double>* Na);
+// (ctx_precision: contractions in the context's precision instead of FP64; traces FP64)
+void gs_energy(Env& e, const Tensor& Hh, const Tensor& Hv, std::complex<double>* E, std::complex<double>* Na,
+               bool ctx_precision = false);
 // nested energy (evaluation.jl:31-45): real(E[4])
 double es_energy(Env& e, const Tensor& Hh, const Tensor& Hv);
 // get_all_norm (evaluation.jl:61-77): returns Nb, writes envB (complex, size of A)
@@ -104,8 +110,25 @@ std::complex<double> all_norm(Env& e, Tensor* envB);
 std::complex<double> gs_norm(Env& e);
 // get_single_dm contracted with Ad (optim_es.jl:247-251), shape of A
 Tensor single_dm_Ad(Env& e);
-// run_ctm (ctmrg.jl:1-55). conv_mode 0: energy (gs), 1: spectrum, 2: es energy / all_norm.
+// plaquette Hamiltonian as the MPO [s1, s2, s3, s4] of get_local_h (local_h.jl:1-31):
+// s1 (d, d, a), s2 (a, d, d, b), s3 (b, d, d, c), s4 (c, d, d)
+using H4 = std::array<Tensor, 4>;
+// get_gs_energy_4x4 (evaluation.jl:339-356)
+std::complex<double> gs_energy_4x4(Env& e, const H4& h);
+// get_es_energy_4x4 (evaluation.jl:358-398)
+std::complex<double> es_energy_4x4(Env& e, const H4& h);
+
+enum ConvMode : int {
+  kConvEnergy = 0,     // get_gs_energy (optim_gs.jl:121)
+  kConvSpectrum = 1,   // left-move spectrum (ctmrg.jl:29-31)
+  kConvEs = 2,         // get_es_energy / get_all_norm (optim_es.jl:175)
+  kConvEnergy4x4 = 3,  // get_gs_energy_4x4 (optim_es_h4.jl:33)
+  kConvEs4x4 = 4,      // get_es_energy_4x4 / get_all_norm (optim_es_h4.jl:139)
+};
+// run_ctm (ctmrg.jl:1-55) with the convergence criterion of conv_mode
+// (Hh, Hv for the bond energies, h4 for the plaquette ones).
 // Returns iterations done; *last_diff = diffs[end]; *converged.
-int run_ctm(Env& e, int conv_mode, const Tensor* Hh, const Tensor* Hv, double* last_diff, bool* converged);
+int run_ctm(Env& e, int conv_mode, const Tensor* Hh, const Tensor* Hv, double* last_diff, bool* converged,
+            const H4* h4 = nullptr);
 
 }  // namespace ipeps

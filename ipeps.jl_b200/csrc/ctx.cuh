@@ -153,6 +153,19 @@ void gemm_f64_dmma(Ctx& c, char opA, char opB, int64_t m, int64_t n, int64_t k, 
 // BF16 operands (rounded from FP32 while staged), FP32 accumulation and result; op in {N, T}
 void gemm_bf16(Ctx& c, char opA, char opB, int64_t m, int64_t n, int64_t k, float alpha, const float* A, int64_t lda,
                const float* B, int64_t ldb, float beta, float* C, int64_t ldc);
+// An FP64 operand split once into TF32 hi/lo planes for the 3xTF32 GEMM:
+// rows x Kp FP32 each, K contiguous (K-major), Kp = K rounded up to 32 with
+// zero padding, the lo plane stacked after the hi plane.
+struct Planes {
+  Tensor buf;
+  int64_t rows = 0, K = 0, Kp = 0;
+  bool empty() const { return buf.empty(); }
+};
+// X(r, k) = kcontig ? X[k + r*ld] : X[r + k*ld], r < rows, k < K
+Planes split_kmajor(Ctx& c, const double* X, int64_t ld, bool kcontig, int64_t rows, int64_t K);
+// C = alpha * A B + beta * C with A given as m x k planes and B as n x k planes (B^T rows)
+void gemm_tf32x3_planes(Ctx& c, const Planes& A, const Planes& B, int64_t m, int64_t n, int64_t k, double alpha,
+                        double beta, double* C, int64_t ldc);
 void gemm_tf32x3(Ctx& c, char opA, char opB, int64_t m, int64_t n, int64_t k, double alpha,
                  const double* A, int64_t lda, const double* B, int64_t ldb, double beta, double* C,
                  int64_t ldc);

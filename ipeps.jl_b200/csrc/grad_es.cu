@@ -105,6 +105,14 @@ AV ad_div_const(Tape& tp, const AV& a, const Tensor& m) {
   return out;
 }
 
+// value of a one-element (0-d) tensor on the host
+std::complex<double> host_scalar(Ctx& c, const Tensor& t) {
+  double h[2] = {0, 0};
+  IPEPS_CUDA(cudaMemcpyAsync(h, t.data(), t.dt == DType::F64 ? 8 : 16, cudaMemcpyDeviceToHost, c.stream));
+  c.sync();
+  return {h[0], t.dt == DType::F64 ? 0.0 : h[1]};
+}
+
 // nested autodiff value: 4 components, an empty tensor is EmptyT
 struct NAV {
   std::array<AV, 4> c;
@@ -195,10 +203,20 @@ NAV leaf_nav(Tape& tp, const std::array<Tensor, 4>& comps) {
 
 }  // namespace
 
-double es_energy_grad(Env& e, const Tensor& Hh, const Tensor& Hv, int ad_iters, Tensor* gB) {
+double es_energy_grad(Env& e, const Tensor& Hh, const Tensor& Hv, int ad_iters, Tensor* gB, const H4* h4) {
   Ctx& c = *e.ctx;
   Fp64Scope fp64_all(c);  // the pullback in FP64 in both forms, as in energy_grad
-  IPEPS_CHECK(e.nested && e.dt == DType::F64, "es_energy_grad: nested environment over a real A expected");
+  IPEPS_CHECK(e.nested, "es_energy_grad: no B set");
+  // the checkpointed moves keep P1/P2 only (no projector adjoint: the projectors are B-independent)
+  struct KeepAdj {
+    Env& e;
+    bool v;
+    ~KeepAdj() { e.keep_adjoint = v; }
+  } keep_adj{e, e.keep_adjoint};
+  e.keep_adjoint = false;
+  auto conv_of = [&]() {
+    return h4 ? es_energy_4x4(e, *h4) / all_norm(e, nullptr) : es_energy(e, Hh, Hv) / all_norm(e, nullptr);
+  };
   auto slots = [&](std::array<std::array<Tensor, 4>, 4>& C, std::array<std::array<Tensor, 4>, 4>& E) {
     for (int s = 0; s < 4; ++s) {
       C[s] = {e.Cs[s], e.B_Cs[s], e.Bd_Cs[s], e.BB_Cs[s]};
@@ -221,7 +239,7 @@ double es_energy_grad(Env& e, const Tensor& Hh, const Tensor& Hv, int ad_iters, 
       ck.push_back(std::move(k));
       // run_ctm's early exit with conv_fun = get_es_energy / get_all_norm (optim_es.jl:200)
       if (e.prm.min_iter < ad_iters && i < ad_iters) {
-        std::complex<double> v = es_energy(e, Hh, Hv) / all_norm(e, nullptr);
+        std::complex<double> v = conv_of();
         const double diff = std::abs(v - conv);
         conv = v;
         if (i >= e.prm.min_iter && diff < e.prm.rg_tol) break;
@@ -258,6 +276,22 @@ double es_energy_grad(Env& e, const Tensor& Hh, const Tensor& Hv, int ad_iters, 
     Ad.c[2] = Bdl;
     const double px = e.px, py = e.py;
     auto sh = [&](const NAV& x, double ph) { return nav_shift(tp, x, ph); };
+    if (h4) {
+      // get_es_energy_4x4 (evaluation.jl:358-398): Re(e4 / n1); n1 (the plain
+      // norm) does not depend on B, so the seed of e4 is conj(1 / n1)
+      Arr4<NADPolicy> sv, Cv{C[0], C[1], C[2], C[3]}, Ev{E[0], E[1], E[2], E[3]};
+      for (int k = 0; k < 4; ++k) sv[k].c[0] = tp.constant((*h4)[k]);
+      auto en = es_plaquette(p, sh, sv, A, Ad, Cv, Ev, px, py);
+      IPEPS_CHECK(en[0].has(3) && en[1].has(0), "es_energy_grad: empty plaquette component");
+      const std::complex<double> e4 = host_scalar(c, en[0].c[3].t), n1 = host_scalar(c, en[1].c[0].t);
+      Eres = (e4 / n1).real();
+      const std::complex<double> w = std::conj(1.0 / n1);
+      Tensor sd = c.alloc(DType::C128, en[0].c[3].t.shape());
+      const double hw[2] = {w.real(), w.imag()};
+      IPEPS_CUDA(cudaMemcpyAsync(sd.data(), hw, 16, cudaMemcpyHostToDevice, c.stream));
+      c.sync();
+      tp.acc(en[0].c[3].id, as_dtype(c, sd, en[0].c[3].t.dt));
+    } else {
     NAV roh = get_dm_h(p, C[0], sh(C[1], px), sh(C[2], px), C[3], E[0], sh(E[0], px), sh(E[1], px), E[2],
                        sh(E[2], px), E[3], A, sh(A, px), Ad, sh(Ad, px));
     NAV rov = get_dm_v(p, C[0], C[1], sh(C[2], py), sh(C[3], py), E[0], E[1], sh(E[1], py), sh(E[2], py), E[3],
@@ -284,6 +318,7 @@ double es_energy_grad(Env& e, const Tensor& Hh, const Tensor& Hv, int ad_iters, 
     };
     tp.acc(roh.c[3].id, seed(Hh, roh.c[3], Nh));
     tp.acc(rov.c[3].id, seed(Hv, rov.c[3], Nv));
+    }
     tp.backward();
     for (int s = 0; s < 4; ++s)
       for (int i = 1; i < 4; ++i) {

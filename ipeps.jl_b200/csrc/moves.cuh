@@ -218,6 +218,104 @@ typename P::T get_dm_v(P& p, const typename P::T& C1, const typename P::T& C2, c
   return p.rs(rov, {d * d, d * d});
 }
 
+// evaluation.jl:501-518: each Ad with its factor of the plaquette MPO
+// [s1, s2, s3, s4] (get_local_h), virtual and Hamiltonian bonds fused
+template <class P>
+Arr4<P> get_op_Ad4(P& p, const Arr4<P>& s, const Arr4<P>& Ad) {
+  using T = typename P::T;
+  Arr4<P> op;
+  T o1 = p.tc(s[0], {-6, 1, -4}, Ad[0], {-1, -2, -3, -5, 1});
+  op[0] = p.rs(o1, {p.dim(o1, 0), p.dim(o1, 1), p.dim(o1, 2), p.dim(o1, 3) * p.dim(o1, 4), p.dim(o1, 5)});
+  T o2 = p.tc(s[1], {-2, -7, 1, -4}, Ad[1], {-1, -3, -5, -6, 1});
+  op[1] = p.rs(o2, {p.dim(o2, 0), p.dim(o2, 1) * p.dim(o2, 2), p.dim(o2, 3) * p.dim(o2, 4), p.dim(o2, 5),
+                    p.dim(o2, 6)});
+  T o3 = p.tc(s[2], {-1, -7, 1, -3}, Ad[2], {-2, -4, -5, -6, 1});
+  op[2] = p.rs(o3, {p.dim(o3, 0) * p.dim(o3, 1), p.dim(o3, 2) * p.dim(o3, 3), p.dim(o3, 4), p.dim(o3, 5),
+                    p.dim(o3, 6)});
+  T o4 = p.tc(s[3], {-4, -6, 1}, Ad[3], {-1, -2, -3, -5, 1});
+  op[3] = p.rs(o4, {p.dim(o4, 0), p.dim(o4, 1), p.dim(o4, 2), p.dim(o4, 3) * p.dim(o4, 4), p.dim(o4, 5)});
+  return op;
+}
+
+template <class P>
+typename P::T fuse3(P& p, const typename P::T& x) {
+  return p.rs(x, {prod3(p, x), -1});
+}
+
+// evaluation.jl:443-498: energy and norm of the 2 x 2 cluster (plaquette)
+//   C1 - E1l - E1r - C2
+//   E4u - A1 -- A2 - E2u
+//   E4d - A4 -- A3 - E2d
+//   C4 - E3l - E3r - C3
+template <class P>
+std::array<typename P::T, 2> energy_norm_4x4(P& p, const typename P::T& C1, const typename P::T& C2,
+                                              const typename P::T& C3, const typename P::T& C4,
+                                              const typename P::T& E1l, const typename P::T& E1r,
+                                              const typename P::T& E2u, const typename P::T& E2d,
+                                              const typename P::T& E3l, const typename P::T& E3r,
+                                              const typename P::T& E4u, const typename P::T& E4d, const Arr4<P>& A,
+                                              const Arr4<P>& Ad, const Arr4<P>& op) {
+  using T = typename P::T;
+  T C1E1 = p.tc(C1, {-1, 1}, E1l, {1, -2, -3, -4});
+  T CEE4 = p.tc(C1E1, {1, -2, -5, -3}, E4u, {1, -1, -6, -4});
+  T CEEA1 = p.tc(CEE4, {-1, -2, -3, -4, 1, 2}, A[0], {1, 2, -5, -6, -7});
+  T eLU = fuse3(p, p.tc(CEEA1, {-1, -4, 1, 2, -2, -5, 3}, op[0], {1, 2, -3, -6, 3}));
+  T nLU = fuse3(p, p.tc(CEEA1, {-1, -4, 1, 2, -2, -5, 3}, Ad[0], {1, 2, -3, -6, 3}));
+
+  T C4E3 = p.tc(C4, {-1, 1}, E3l, {1, -2, -3, -4});
+  T CEE4b = p.tc(C4E3, {1, -2, -6, -4}, E4d, {-1, 1, -5, -3});
+  T CEEA4 = p.tc(CEE4b, {-1, -2, -3, -4, 1, 2}, A[3], {-5, 1, 2, -6, -7});
+  T eLB = fuse3(p, p.tc(CEEA4, {-1, -4, 1, 2, -2, -5, 3}, op[3], {-3, 1, 2, -6, 3}));
+  T nLB = fuse3(p, p.tc(CEEA4, {-1, -4, 1, 2, -2, -5, 3}, Ad[3], {-3, 1, 2, -6, 3}));
+
+  T C2E1 = p.tc(C2, {1, -2}, E1r, {-1, 1, -3, -4});
+  T CEE2 = p.tc(C2E1, {-1, 1, -5, -3}, E2u, {1, -2, -6, -4});
+  T CEEA2 = p.tc(CEE2, {-1, -2, -3, -4, 1, 2}, A[1], {1, -5, -6, 2, -7});
+  T eRU = fuse3(p, p.tc(CEEA2, {-1, -4, 1, 2, -2, -5, 3}, op[1], {1, -3, -6, 2, 3}));
+  T nRU = fuse3(p, p.tc(CEEA2, {-1, -4, 1, 2, -2, -5, 3}, Ad[1], {1, -3, -6, 2, 3}));
+
+  T C3E3 = p.tc(C3, {-1, 1}, E3r, {-2, 1, -3, -4});
+  T CEE2b = p.tc(C3E3, {1, -2, -5, -3}, E2d, {-1, 1, -6, -4});
+  T CEEA3 = p.tc(CEE2b, {-1, -2, -5, -6, 1, 2}, A[2], {-3, -4, 1, 2, -7});
+  T eRB = fuse3(p, p.tc(CEEA3, {-1, -4, -2, -5, 1, 2, 3}, op[2], {-3, -6, 1, 2, 3}));
+  T nRB = fuse3(p, p.tc(CEEA3, {-1, -4, -2, -5, 1, 2, 3}, Ad[2], {-3, -6, 1, 2, 3}));
+
+  T eL = p.tc(p.pm(eLU, {1, 0}), {-1, 1}, eLB, {1, -2});
+  T eR = p.tc(eRU, {-1, 1}, eRB, {1, -2});
+  T nL = p.tc(p.pm(nLU, {1, 0}), {-1, 1}, nLB, {1, -2});
+  T nR = p.tc(nRU, {-1, 1}, nRB, {1, -2});
+  return {p.tc(eL, {1, 2}, eR, {1, 2}), p.tc(nL, {1, 2}, nR, {1, 2})};
+}
+
+// The arguments of energy_norm_4x4 for get_es_energy_4x4 (evaluation.jl:358-398):
+// the nested environment with the phase shifts of the sites right of (px) and
+// below (py) the first
+template <class P, class Shift>
+std::array<typename P::T, 2> es_plaquette(P& p, Shift sh, const Arr4<P>& s, const typename P::T& A,
+                                          const typename P::T& Ad, Arr4<P> C, const Arr4<P>& E, double px,
+                                          double py) {
+  using T = typename P::T;
+  T E1r = sh(E[0], px);
+  T A2 = sh(A, px), A2d = sh(Ad, px);
+  T A3 = sh(A, px), A3d = sh(Ad, px);
+  T E3r = sh(E[2], px);
+  C[1] = sh(C[1], px);
+  C[2] = sh(C[2], px);
+  T E2u = sh(E[1], px), E2d = sh(E[1], px);
+  C[3] = sh(C[3], py);
+  C[2] = sh(C[2], py);
+  T E3l = sh(E[2], py);
+  E3r = sh(E3r, py);
+  T E4d = sh(E[3], py);
+  E2d = sh(E2d, py);
+  T A4 = sh(A, py), A4d = sh(Ad, py);
+  A3 = sh(A3, py);
+  A3d = sh(A3d, py);
+  Arr4<P> As{A, A2, A3, A4}, Ads{Ad, A2d, A3d, A4d};
+  Arr4<P> op = get_op_Ad4(p, s, Ads);
+  return energy_norm_4x4(p, C[0], C[1], C[2], C[3], E[0], E1r, E2u, E2d, E3l, E3r, E[3], E4d, As, Ads, op);
+}
+
 // evaluation.jl:110-122
 template <class P>
 typename P::T get_single_dm(P& p, const typename P::T& C1, const typename P::T& C2, const typename P::T& C3,

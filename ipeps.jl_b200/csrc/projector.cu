@@ -21,6 +21,59 @@
 
 namespace ipeps {
 
+namespace {
+
+// TF32 hi/lo planes of an enlarged-corner matrix Rt (r0 x c0, column-major)
+// for the mixed form, split once per projector call and shared by all its
+// products: `row` holds Rt itself as the A operand (rows r0, K = c0), `col`
+// holds Rt^T (rows c0, K = r0), which is also Rt as a B operand.
+const Planes& planes_row(Ctx& c, const Tensor& Rt, PlaneCache* pc) {
+  if (pc->row.empty()) pc->row = split_kmajor(c, Rt.f64(), Rt.dims[0], false, Rt.dims[0], Rt.dims[1]);
+  return pc->row;
+}
+const Planes& planes_col(Ctx& c, const Tensor& Rt, PlaneCache* pc) {
+  if (pc->col.empty()) pc->col = split_kmajor(c, Rt.f64(), Rt.dims[0], true, Rt.dims[1], Rt.dims[0]);
+  return pc->col;
+}
+
+bool use_planes(const Ctx& c, const MatRef& R, const PlaneCache* pc) {
+  return pc && c.precision == kPrecMixed && R.t.dt == DType::F64;
+}
+
+}  // namespace
+
+Tensor apply(Ctx& c, const MatRef& R, char op, const Tensor& X, PlaneCache* pc) {
+  if (use_planes(c, R, pc)) {
+    const bool t = (op == 'T') != R.trans;
+    const int64_t m = (op == 'N') ? R.rows() : R.cols();
+    const int64_t kk = (op == 'N') ? R.cols() : R.rows();
+    IPEPS_CHECK(X.dims[0] == kk, "apply: shape mismatch");
+    const int64_t n = X.nd > 1 ? X.dims[1] : 1;
+    Tensor Y = c.alloc(DType::F64, {m, n});
+    const Planes& PA = t ? planes_col(c, R.t, pc) : planes_row(c, R.t, pc);
+    const Planes PB = split_kmajor(c, X.f64(), X.dims[0], true, n, kk);
+    gemm_tf32x3_planes(c, PA, PB, m, n, kk, 1.0, 0.0, Y.f64(), m);
+    return Y;
+  }
+  return apply(c, R, op, X);
+}
+
+Tensor apply_left_T(Ctx& c, const Tensor& X, const MatRef& R, char op, PlaneCache* pc) {
+  if (use_planes(c, R, pc)) {
+    const bool t = (op == 'T') != R.trans;
+    const int64_t kk = (op == 'N') ? R.rows() : R.cols();
+    const int64_t n = (op == 'N') ? R.cols() : R.rows();
+    IPEPS_CHECK(X.dims[0] == kk, "apply_left_T: shape mismatch");
+    const int64_t m = X.dims[1];
+    Tensor Y = c.alloc(DType::F64, {m, n});
+    const Planes PA = split_kmajor(c, X.f64(), X.dims[0], true, m, kk);
+    const Planes& PB = t ? planes_row(c, R.t, pc) : planes_col(c, R.t, pc);
+    gemm_tf32x3_planes(c, PA, PB, m, n, kk, 1.0, 0.0, Y.f64(), m);
+    return Y;
+  }
+  return apply_left_T(c, X, R, op);
+}
+
 Tensor apply(Ctx& c, const MatRef& R, char op, const Tensor& X) {
   // op(R) * X
   bool t = (op == 'T') != R.trans;
@@ -116,13 +169,14 @@ struct RealOps {
   Ctx& c;
   const MatRef& R1;
   const MatRef& R2;
+  PlaneCache pc1, pc2;  // mixed form: TF32 planes of R1, R2
   static constexpr DType dt = DType::F64;
   static constexpr int words = 1;
   int64_t N1() const { return R1.rows(); }
   int64_t K1() const { return R1.cols(); }
   int64_t N2() const { return R2.cols(); }
-  Tensor M(const Tensor& X) { return apply(c, R1, 'N', apply(c, R2, 'N', X)); }   // M X
-  Tensor MH(const Tensor& X) { return apply(c, R2, 'T', apply(c, R1, 'T', X)); }  // M^T X
+  Tensor M(const Tensor& X) { return apply(c, R1, 'N', apply(c, R2, 'N', X, &pc2), &pc1); }   // M X
+  Tensor MH(const Tensor& X) { return apply(c, R2, 'T', apply(c, R1, 'T', X, &pc1), &pc2); }  // M^T X
   Tensor orth_(const Tensor& Y, int passes) { return orth(c, Y, passes, nullptr); }
   // X = Bh^H Q2 (k x k) for Bh = M^H Q (N2 x k)
   Tensor small(const Tensor& Bh, const Tensor& Q2, int k) {
@@ -141,8 +195,8 @@ struct RealOps {
     if (kw > 160 && want + sp.min_oversample <= 160) return 160;
     return kw;
   }
-  Tensor P1(const Tensor& V) { return apply(c, R2, 'N', V); }          // R2 V      (K1 x n)
-  Tensor P2(const Tensor& U) { return apply_left_T(c, U, R1, 'N'); }   // U^T R1    (n x K1)
+  Tensor P1(const Tensor& V) { return apply(c, R2, 'N', V, &pc2); }          // R2 V      (K1 x n)
+  Tensor P2(const Tensor& U) { return apply_left_T(c, U, R1, 'N', &pc1); }   // U^T R1    (n x K1)
 };
 
 Tensor cmm(Ctx& c, char oa, char ob, int64_t m, int64_t n, int64_t k, const Tensor& A, int64_t lda, const Tensor& B,
@@ -354,7 +408,9 @@ ProjResult projector_impl(Ctx& c, Ops& o, int chi, const SvdParams& sp, ProjCach
     c.sync();
     // done when below tolerance, or when it stopped decreasing (the FP64 floor of
     // R1 (R2 v), ~eps ||R1|| ||R2||, can sit above resid_tol * s_1)
-    if (res <= sp.resid_tol * smax || res > 0.5 * prev_res) break;
+    const double rtol = (c.precision == kPrecMixed && dt == DType::F64) ? std::max(sp.resid_tol, sp.resid_tol_mixed)
+                                                                         : sp.resid_tol;
+    if (res <= rtol * smax || res > 0.5 * prev_res) break;
     prev_res = res;
     // not converged: one more power iteration from the current right vectors
     Om = Vk;
@@ -419,7 +475,7 @@ ProjResult get_projector(Ctx& c, const MatRef& R1, const MatRef& R2, int chi, co
     ComplexOps o(c, R1, R2);
     return projector_impl(c, o, chi, sp, cache, keep_factors);
   }
-  RealOps o{c, R1, R2};
+  RealOps o{c, R1, R2, {}, {}};
   return projector_impl(c, o, chi, sp, cache, keep_factors);
 }
 

@@ -28,6 +28,9 @@ struct SvdParams {
   // last-iteration energy error is 5e-14 at 1e-11, 4e-11 at 3e-10 and 1.4e-9 at
   // 1e-9; 1e-10 keeps the 1e-10 bar with a margin and saves ~1/4 of the passes.
   double resid_tol = 1e-10;
+  // the same check in the mixed form, whose 3xTF32 products carry FP32-level
+  // errors (~1e-6 of s_1 in the residual itself)
+  double resid_tol_mixed = 1e-6;
   bool warm_start = true;
   int jacobi_max_sweeps = 40;
   double jacobi_tol = 0.0;  // <= 0: m * eps (rounding level of the column dot products)
@@ -74,6 +77,13 @@ ProjResult get_projector(Ctx& c, const MatRef& R1, const MatRef& R2, int chi, co
 Tensor apply(Ctx& c, const MatRef& R, char op, const Tensor& X);
 // X^T * op(R)   (returns X^T op(R))
 Tensor apply_left_T(Ctx& c, const Tensor& X, const MatRef& R, char op);
+// TF32 hi/lo planes of one enlarged-corner matrix, split on first use (mixed form)
+struct PlaneCache {
+  Planes row, col;
+};
+// the same products; in the mixed form R's planes are taken from (or added to) pc
+Tensor apply(Ctx& c, const MatRef& R, char op, const Tensor& X, PlaneCache* pc);
+Tensor apply_left_T(Ctx& c, const Tensor& X, const MatRef& R, char op, PlaneCache* pc);
 
 // Orthonormalise the columns of Y (N x k) by shifted CholeskyQR; if Rout is
 // non-null it receives R with Y = Q R.

@@ -7,6 +7,8 @@ small matrices); only their calls into CTMRG go to the device.
     prepare_basis(H, A, cfg)    src/optimize/optim_es.jl:34-73
     optim_es(px, py, prep, cfg) src/optimize/optim_es.jl:91-165
     evaluate_es(effH, effN)     src/graph/expectation.jl:152-183
+    prepare_basis_h4 / optim_es_h4 (the plaquette Hamiltonian)
+                                src/optimize/optim_es_h4.jl
 
 The L-BFGS is a plain two-loop recursion with the sphere manifold of
 Optim.jl (gradient projected onto the tangent space, iterate retracted by
@@ -264,6 +266,100 @@ def optim_es(px: float, py: float, ts: host.CTMTensors, H, basis: np.ndarray,
     C = [ts.get_CT(k) for k in range(1, 5)]
     for i in (range(nb) if indices is None else indices):
         effH[:, i], effN[:, i] = es_column(px, py, ts, H, basis, i, C)
+    return effH, effN
+
+
+# ---------------------------------------------------------------- plaquette (h4) drivers
+def _wrap_svd(M: np.ndarray):
+    """wrap_svd (wrapper.jl:25-55) without a rank cap: SVD sorted descending,
+    keep s/s_max > 1e-12 (plus one when |s[n+1] - s[n]| < 1e-10)."""
+    u, s, vh = np.linalg.svd(M, full_matrices=False)
+    n = int(np.sum(s / s[0] > 1e-12)) if s[0] > 0 else 1
+    if n < len(s) and abs(s[n] - s[n - 1]) < 1e-10:
+        n += 1
+    return u[:, :n], s[:n], vh[:n].conj().T
+
+
+def get_local_h(h: np.ndarray) -> List[np.ndarray]:
+    """get_local_h (local_h.jl:1-31): the plaquette Hamiltonian h of shape
+    (d^2, d^2, d^2, d^2) as the MPO [s1, s2, s3, s4] by successive SVDs
+    (column-major reshapes, as Julia)."""
+    h = np.asarray(h, dtype=np.complex128)
+    dims = h.shape
+    d = int(round(math.sqrt(dims[0])))
+    sl = []
+    u, s, v = _wrap_svd(h.reshape(dims[0], -1, order="F"))
+    sl.append((u * np.sqrt(s)).reshape(d, d, -1, order="F"))
+    sdots = np.sqrt(s)[:, None] * v.conj().T
+    for i in range(len(dims) - 2):
+        dl = sdots.shape[0]
+        sdots = sdots.reshape(dl * dims[i], -1, order="F")
+        u, s, v = _wrap_svd(sdots)
+        sl.append((u * np.sqrt(s)).reshape(dl, d, d, -1, order="F"))
+        sdots = np.sqrt(s)[:, None] * v.conj().T
+    sl.append(sdots.reshape(sdots.shape[0], d, d, order="F"))
+    return sl
+
+
+def tout_site(a: np.ndarray, b: np.ndarray) -> np.ndarray:
+    """tout_site (honeycomb.jl:37-42): c[i,j,k,l] = a[i,j] b[k,l] reshaped to (d1 d2, d3 d4)."""
+    c = np.einsum("ij,kl->ijkl", a, b)
+    s = c.shape
+    return c.reshape(s[0] * s[1], s[2] * s[3], order="F")
+
+
+def substract_gs_energy_h4(ts: host.CTMTensors, h: np.ndarray) -> np.ndarray:
+    """substract_gs_energy_h4 (optim_es_h4.jl:170-183): h - E0 hI with E0 the
+    plaquette energy of the environment in ts."""
+    E0 = host.get_gs_energy_4x4(ts, get_local_h(h))
+    d = int(round(math.sqrt(h.shape[0])))
+    II = np.eye(d, dtype=np.complex128)
+    hI = tout_site(tout_site(II, II), tout_site(II, II)).reshape(d * d, d * d, d * d, d * d, order="F")
+    return np.asarray(h, dtype=np.complex128) - E0 * hI
+
+
+def prepare_basis_h4(h: np.ndarray, A, cfg: Dict[str, Any], engine: Optional[host.Engine] = None):
+    """prepare_basis_h4 (optim_es_h4.jl:13-55): converge with the plaquette
+    energy at 2 max_iter and rg_tol^2, normalise A, subtract E0 hI, take the
+    default tangent basis.  Returns (ts, H4, basis) with H4 the MPO of the
+    subtracted Hamiltonian (what the reference saves in basis.jld2)."""
+    A = np.asarray(A)
+    A = A / np.abs(A).max()
+    cfg0 = dict(cfg)
+    ts = host.CTMTensors(A, cfg0, engine=engine)
+    ts.Params["max_iter"] = 2 * int(cfg0.get("max_iter", 20))
+    ts.Params["rg_tol"] = float(cfg0.get("rg_tol", 1e-6)) ** 2
+    host.run_ctm_4x4(ts, get_local_h(h), nested=False)
+    ts.Params = dict(cfg0)
+    normalize_gs(ts)
+    H4 = get_local_h(substract_gs_energy_h4(ts, h))
+    basis = tangent_basis(ts, host.single_dm_Ad(ts))
+    return ts, H4, basis
+
+
+def es_column_h4(px: float, py: float, ts: host.CTMTensors, H4, basis: np.ndarray, i: int, C=None):
+    """One basis vector of optim_es_h4 (optim_es_h4.jl:92-108): (effH[:, i], effN[:, i])."""
+    C = C if C is not None else [ts.get_CT(k) for k in range(1, 5)]
+    t = host.CTMTensors(ts.A, dict(ts.Params), engine=ts.engine, init=False)
+    try:
+        for k in range(4):
+            t.set_CT(k + 1, *C[k])
+        t.Params["px"], t.Params["py"] = px * math.pi, py * math.pi
+        gH, gN = host.get_es_grad_h4(t, H4, basis[:, i])
+    finally:
+        t.close()
+    return basis.conj().T @ gH / 2, basis.conj().T @ gN
+
+
+def optim_es_h4(px: float, py: float, ts: host.CTMTensors, H4, basis: np.ndarray,
+                indices: Optional[List[int]] = None):
+    """optim_es_h4 (optim_es_h4.jl:57-131) for one momentum (units of pi)."""
+    nb = basis.shape[1]
+    effH = np.zeros((nb, nb), dtype=np.complex128)
+    effN = np.zeros((nb, nb), dtype=np.complex128)
+    C = [ts.get_CT(k) for k in range(1, 5)]
+    for i in (range(nb) if indices is None else indices):
+        effH[:, i], effN[:, i] = es_column_h4(px, py, ts, H4, basis, i, C)
     return effH, effN
 
 

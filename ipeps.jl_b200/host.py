@@ -41,7 +41,7 @@ EXPORTED = [
     "ipeps_ctm_log", "ipeps_energy", "ipeps_gs_norm", "ipeps_nested_set_B", "ipeps_es_energy",
     "ipeps_all_norm", "ipeps_tcon", "ipeps_projector", "ipeps_projector_c", "ipeps_ctx_stream", "ipeps_prof_enable",
     "ipeps_prof_query", "ipeps_energy_grad", "ipeps_env_set_mixed", "ipeps_es_energy_grad",
-    "ipeps_single_dm_Ad", "ipeps_gemm_f64", "ipeps_gemm_tf32x3", "ipeps_gemm_bf16", "ipeps_mlp_create", "ipeps_mlp_destroy", "ipeps_mlp_num_params",
+    "ipeps_single_dm_Ad", "ipeps_energy_4x4", "ipeps_ctm_run_4x4", "ipeps_es_energy_grad_4x4", "ipeps_gemm_f64", "ipeps_gemm_tf32x3", "ipeps_gemm_bf16", "ipeps_mlp_create", "ipeps_mlp_destroy", "ipeps_mlp_num_params",
     "ipeps_mlp_get_params", "ipeps_mlp_set_params", "ipeps_mlp_forward", "ipeps_mlp_grad", "ipeps_mlp_train_step",
 ]
 
@@ -50,6 +50,11 @@ class IPEPSError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"[ipeps status {code}] {msg}")
         self.code = code
+
+
+class CTensor(ct.Structure):
+    """ipeps_ctensor_t: a complex128 column-major array of rank <= 4."""
+    _fields_ = [("data", ct.c_void_p), ("nd", ct.c_int), ("dims", ct.c_int64 * 4)]
 
 
 class Stats(ct.Structure):
@@ -118,9 +123,14 @@ def load_library(path: str = LIB_PATH) -> ct.CDLL:
         "ipeps_energy_grad": [P, dp, dp, I, I, dp, dp],
         "ipeps_env_set_mixed": [P, I, D],
         "ipeps_es_energy_grad": [P, dp, dp, I, I, dp, dp],
+        "ipeps_energy_4x4": [P, ct.POINTER(CTensor), I, dp],
+        "ipeps_ctm_run_4x4": [P, ct.POINTER(CTensor), I, ip, dp, ip],
+        "ipeps_es_energy_grad_4x4": [P, ct.POINTER(CTensor), I, dp, dp],
         "ipeps_single_dm_Ad": [P, dp],
         "ipeps_gemm_f64": [P, ct.c_char, ct.c_char, ct.c_int64, ct.c_int64, ct.c_int64, D, dp, ct.c_int64, dp,
                            ct.c_int64, D, dp, ct.c_int64, I],
+        "ipeps_gemm_tf32x3": [P, ct.c_char, ct.c_char, ct.c_int64, ct.c_int64, ct.c_int64, D, dp, ct.c_int64, dp,
+                              ct.c_int64, D, dp, ct.c_int64, I, dp],
         "ipeps_gemm_tf32x3": [P, ct.c_char, ct.c_char, ct.c_int64, ct.c_int64, ct.c_int64, D, dp, ct.c_int64, dp,
                               ct.c_int64, D, dp, ct.c_int64, I, dp],
         "ipeps_gemm_bf16": [P, ct.c_char, ct.c_char, ct.c_int64, ct.c_int64, ct.c_int64, ct.c_float, fp,
@@ -480,6 +490,83 @@ def bottom_rg(ts, chi=None):
     return _move(ts, chi, 3)
 
 
+class _H4:
+    """The plaquette MPO [s1, s2, s3, s4] (get_local_h) as C-ABI tensors; keeps
+    the column-major complex copies alive for the duration of a call."""
+
+    def __init__(self, H4):
+        if len(H4) != 4:
+            raise ValueError("the plaquette Hamiltonian is the MPO list [s1, s2, s3, s4]")
+        self.arrs = [_fortran(h, np.complex128) for h in H4]
+        self.c = (CTensor * 4)()
+        for k, a in enumerate(self.arrs):
+            self.c[k].data = a.ctypes.data
+            self.c[k].nd = a.ndim
+            for i, d in enumerate(a.shape):
+                self.c[k].dims[i] = d
+
+
+def get_gs_energy_4x4(ts: CTMTensors, H4) -> complex:
+    """get_gs_energy_4x4 (evaluation.jl:339-356): plaquette energy of the 2 x 2 cluster."""
+    h = _H4(H4)
+    out = np.zeros(2)
+    ts.engine.check(ts.lib.ipeps_energy_4x4(ts.h, h.c, 0, _dp(out)))
+    return complex(out[0], out[1])
+
+
+def get_es_energy_4x4(ts: CTMTensors, H4) -> complex:
+    """get_es_energy_4x4 (evaluation.jl:358-398): nested plaquette energy (B set)."""
+    h = _H4(H4)
+    out = np.zeros(2)
+    ts.engine.check(ts.lib.ipeps_energy_4x4(ts.h, h.c, 1, _dp(out)))
+    return complex(out[0], out[1])
+
+
+def run_ctm_4x4(ts: CTMTensors, H4, nested: bool = False):
+    """run_ctm with conv_fun = get_gs_energy_4x4 (nested False) or
+    get_es_energy_4x4 / get_all_norm (nested True) (optim_es_h4.jl:33,139).
+    Returns (ts, info) as run_ctm."""
+    ts._push_params()
+    h = _H4(H4)
+    iters, conv = ct.c_int(0), ct.c_int(0)
+    diff = ct.c_double(0)
+    ts.engine.check(ts.lib.ipeps_ctm_run_4x4(ts.h, h.c, int(bool(nested)), ct.byref(iters), ct.byref(diff),
+                                             ct.byref(conv)))
+    return ts, _run_info(ts, iters, diff, conv)
+
+
+def es_energy_grad_4x4(ts: CTMTensors, H4, ad_iters: Optional[int] = None):
+    """Pullback of run_es_h4 (optim_es_h4.jl:159-168) w.r.t. B from the nested
+    environment held by ts: returns (E, gH), gH complex (D,D,D,D,d)."""
+    h = _H4(H4)
+    n = int(ts.Params.get("ad_max_iter", 4) if ad_iters is None else ad_iters)
+    ts._push_params()
+    E = np.zeros(1)
+    g = np.empty(ts.A.shape, dtype=np.complex128, order="F")
+    ts.engine.check(ts.lib.ipeps_es_energy_grad_4x4(ts.h, h.c, n, _dp(E), _dp(g)))
+    return float(E[0]), g
+
+
+def get_es_grad_h4(ts: CTMTensors, H4, Bi):
+    """get_es_grad_h4 (optim_es_h4.jl:133-157) on the device; as get_es_grad
+    with the plaquette energy.  Returns (gH, gN) flat complex (column-major)."""
+    B = np.asarray(Bi, dtype=np.complex128).reshape(ts.A.shape, order="F")
+    ts.set_B(B, ts.Params.get("px", 0.0), ts.Params.get("py", 0.0))
+    run_ctm_4x4(ts, H4, nested=True)
+    E, gH = es_energy_grad_4x4(ts, H4)
+    Nb, gN = get_all_norm(ts)
+    return gH.reshape(-1, order="F"), gN.reshape(-1, order="F")
+
+
+def _run_info(ts, iters, diff, conv):
+    n = ct.c_int(100000)
+    log = np.empty((100000, 4))
+    ts.engine.check(ts.lib.ipeps_ctm_log(ts.h, _dp(log), ct.byref(n)))
+    return {"iters": iters.value, "diff": diff.value, "converged": bool(conv.value),
+            "log": [{"iter": i + 1, "diff": float(r[0]), "obj": complex(r[1], r[2]), "chi": int(r[3])}
+                    for i, r in enumerate(log[: n.value])]}
+
+
 def run_ctm(ts: CTMTensors, conv_fun: Optional[str] = None, H=None):
     """ctmrg.jl:1-55.
 
@@ -631,6 +718,24 @@ def gemm_f64(opA: str, opB: str, A, B, alpha: float = 1.0, beta: float = 0.0, C=
     eng.check(eng.lib.ipeps_gemm_f64(eng.h, opA.encode(), opB.encode(), m, n, k, float(alpha), _dp(A), A.shape[0],
                                      _dp(B), B.shape[0], float(beta), _dp(C), C.shape[0], int(reps)))
     return C
+
+
+def gemm_tf32x3(opA: str, opB: str, A, B, alpha: float = 1.0, beta: float = 0.0, C=None,
+                engine: Optional[Engine] = None, reps: int = 1, timing: bool = False):
+    """C = alpha op(A) op(B) + beta C on the engine's 3xTF32 tcgen05 GEMM; host
+    arrays.  With timing=True returns (C, device ms of one product)."""
+    eng = engine or default_engine()
+    A = _fortran(A, np.float64)
+    B = _fortran(B, np.float64)
+    m = A.shape[0] if opA == "N" else A.shape[1]
+    k = A.shape[1] if opA == "N" else A.shape[0]
+    n = B.shape[1] if opB == "N" else B.shape[0]
+    C = np.zeros((m, n), order="F") if C is None else _fortran(C, np.float64).copy(order="F")
+    ms = np.zeros(1)
+    eng.check(eng.lib.ipeps_gemm_tf32x3(eng.h, opA.encode(), opB.encode(), m, n, k, float(alpha), _dp(A),
+                                        A.shape[0], _dp(B), B.shape[0], float(beta), _dp(C), C.shape[0], int(reps),
+                                        _dp(ms)))
+    return (C, float(ms[0])) if timing else C
 
 
 def gemm_tf32x3(opA: str, opB: str, A, B, alpha: float = 1.0, beta: float = 0.0, C=None,

@@ -4,8 +4,9 @@
 * the fg! energy of the reference's last optim_gs iterate (honeycomb XX,
   complex A (2,2,2,2,4), chi = 32): converge with the energy criterion, then
   the 4 iterations of run_gs and the energy, within 1e-10 of the saved value;
-* effN columns of optim_es from the saved ground-state environment and
-  tangent basis at two momenta, within 1e-8 relative.
+* effH and effN columns of the plaquette driver optim_es_h4 from the saved
+  ground-state environment, tangent basis and plaquette MPO at two momenta,
+  within 1e-8 relative.
 """
 import math
 import os
@@ -38,19 +39,24 @@ def test_gpu_reproduces_reference_gs_energy(engine, pkg):
 
 
 @pytest.mark.parametrize("mom", [("0.1", "0"), ("1", "1")])
-def test_gpu_reproduces_reference_effN(engine, pkg, mom):
+def test_gpu_reproduces_reference_effH_effN(engine, pkg, mom):
+    """optim_es_h4 columns (get_es_grad_h4 with the saved plaquette MPO) from
+    the saved environment: complex A, nested plaquette energy and its
+    pullback w.r.t. B, get_all_norm."""
     p = pins()
     cfg = pkg.default_config()
-    A = p["es_A"]
-    ts = pkg.CTMTensors(A, cfg, engine=engine, init=False)
+    ts = pkg.CTMTensors(p["es_A"], cfg, engine=engine, init=False)
     C = [(p[f"es_C{k}"], p[f"es_E{k}"]) for k in range(1, 5)]
     for k in range(4):
         ts.set_CT(k + 1, *C[k])
-    H2 = pkg.drivers.substract_gs_energy(ts, [h.numpy() for h in O.ising(2.0)])
+    H4 = [p[f"es_H{k}"] for k in range(1, 5)]
+    # the saved MPO is the subtracted Hamiltonian: zero plaquette energy
+    assert abs(pkg.get_gs_energy_4x4(ts, H4)) <= 1e-12
     basis = p["es_basis"]
-    ref = p[f"effN_{mom[0]}_{mom[1]}"]
+    refH, refN = p[f"effH_{mom[0]}_{mom[1]}"], p[f"effN_{mom[0]}_{mom[1]}"]
     for i in (0, 15, 30):
-        _, colN = pkg.drivers.es_column(float(mom[0]), float(mom[1]), ts, H2, basis, i, C)
-        assert np.linalg.norm(colN - ref[:, i]) <= 1e-8 * np.linalg.norm(ref[:, i]), (
-            mom, i, np.linalg.norm(colN - ref[:, i]) / np.linalg.norm(ref[:, i]))
+        colH, colN = pkg.drivers.es_column_h4(float(mom[0]), float(mom[1]), ts, H4, basis, i, C)
+        eh = np.linalg.norm(colH - refH[:, i]) / np.linalg.norm(refH[:, i])
+        en = np.linalg.norm(colN - refN[:, i]) / np.linalg.norm(refN[:, i])
+        assert eh <= 1e-8 and en <= 1e-8, (mom, i, eh, en)
     ts.close()
