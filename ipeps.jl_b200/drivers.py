@@ -269,6 +269,26 @@ def optim_es(px: float, py: float, ts: host.CTMTensors, H, basis: np.ndarray,
     return effH, effN
 
 
+def correlation_TM(ts: host.CTMTensors, direction: str = "h", N: int = 10, full: bool = False):
+    """correlation_TM (expectation.jl:193-220): the transfer matrix of two
+    edge tensors, TM = tcon([E4, E2], [[-1,-3,1,2],[-2,-4,1,2]]) ("h") or of
+    E1, E3 ("v"), reshaped to (chi^2, chi^2), contracted on the device; its
+    N largest-magnitude eigenvalues (all when full), as the reference returns
+    them: (|es| sorted descending and > 0, es, TM)."""
+    Es = [ts.get_CT(k)[1] for k in range(1, 5)]
+    a, b = (Es[3], Es[1]) if direction == "h" else (Es[0], Es[2])
+    TM = host.tcon([a, b], [[-1, -3, 1, 2], [-2, -4, 1, 2]], engine=ts.engine)
+    n = TM.shape[0] * TM.shape[1]
+    TM = TM.reshape(n, -1, order="F")
+    if full or N >= n - 1:
+        es = np.linalg.eigvals(TM)
+    else:
+        from scipy.sparse.linalg import eigs
+        es = eigs(TM, k=N, which="LM", return_eigenvectors=False)
+    es1 = np.sort(np.abs(es))[::-1]
+    return es1[es1 > 0], es, TM
+
+
 # ---------------------------------------------------------------- plaquette (h4) drivers
 def _wrap_svd(M: np.ndarray):
     """wrap_svd (wrapper.jl:25-55) without a rank cap: SVD sorted descending,

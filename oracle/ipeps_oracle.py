@@ -849,6 +849,22 @@ def get_es_grad_h4(ts, H, Bi):
     return freshape(gH.detach(), -1), freshape(gN.detach(), -1)
 
 
+def correlation_TM(ts, direction="h", N=10):
+    """expectation.jl:193-220: transfer matrix of (E4, E2) or (E1, E3) and its
+    eigenvalue magnitudes, descending (the full spectrum here; the reference
+    takes the N largest with eigsolve)."""
+    E1, E2, E3, E4 = ts.Es
+    if direction == "h":
+        TM = tcon([E4, E2], [[-1, -3, 1, 2], [-2, -4, 1, 2]])
+    else:
+        TM = tcon([E1, E3], [[-1, -3, 1, 2], [-2, -4, 1, 2]])
+    d = TM.shape
+    TM = freshape(TM, d[0] * d[1], -1)
+    es = torch.linalg.eigvals(TM)
+    es1 = torch.sort(es.abs(), descending=True).values
+    return es1[:N], TM
+
+
 def get_gs_norm(ts):
     """evaluation.jl:47-59"""
     n_dm = get_single_dm(*ts.Cs, *ts.Es)

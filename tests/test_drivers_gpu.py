@@ -63,3 +63,24 @@ def test_optim_es_band_energies_match_oracle(engine, pkg):
     assert np.allclose(es[:4], eo[:4], rtol=0, atol=1e-6), (es[:4], eo[:4])
     assert np.allclose(es, eo, rtol=1e-6, atol=1e-6)
     ts.close()
+
+
+@pytest.mark.parametrize("direction", ["h", "v"])
+def test_correlation_TM_matches_oracle(engine, pkg, direction):
+    """correlation_TM (expectation.jl:193-220): the leading transfer-matrix
+    eigenvalue magnitudes of the converged environment, 1e-9 relative (the
+    spectrum is gauge invariant)."""
+    A = O.random_A(2, 2, seed=12)
+    H = O.heisenberg(1.0)
+    cfg = O.default_config()
+    cfg.update(chi=10, min_iter=4, max_iter=40, rg_tol=1e-11)
+    ts_o = O.make_ctm_tensors(A, cfg)
+    with torch.no_grad():
+        ts_o, _ = O.run_ctm(ts_o, conv_fun=lambda t: O.get_gs_energy(t, H)[0])
+        eo, _ = O.correlation_TM(ts_o, direction, N=4)
+    ts = pkg.CTMTensors(A.numpy(), cfg, engine=engine)
+    pkg.run_ctm(ts, conv_fun="energy", H=[h.numpy() for h in H])
+    es1, es, TM = pkg.drivers.correlation_TM(ts, direction, N=4)
+    ts.close()
+    eo = eo.numpy()
+    assert np.allclose(es1[:4], eo[:4], rtol=1e-9), (es1[:4], eo[:4])
