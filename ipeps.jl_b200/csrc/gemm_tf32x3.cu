@@ -435,7 +435,8 @@ void gemm_tf32x3_planes(Ctx& c, const Planes& PA, const Planes& PB, int64_t m, i
   const int stages = std::min(MAX_STAGES, (SMEM_BUDGET - 1024 - 256) / stage_bytes);
   IPEPS_CHECK(stages >= 2, "gemm_tf32x3: tile does not fit in shared memory");
   const int smem = 1024 + stages * stage_bytes + 256;
-  g_attr.ensure(tf32x3_kernel, smem);
+  // the attribute is set once per device, so to the largest size any tile width uses
+  g_attr.ensure(tf32x3_kernel, SMEM_BUDGET);
 
   Args a{};
   a.M = int(m);

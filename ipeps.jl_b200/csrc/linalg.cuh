@@ -33,6 +33,11 @@ void trsm_right_upper(Ctx& c, const double* Y, int64_t ldy, int64_t N, int k, co
 // rotations when it fits; tol <= 0 means m * eps
 void jacobi_svd_auto(Ctx& c, double* X, int m, int k, int64_t ldx, double* J, int64_t ldj, double* S,
                      int max_sweeps, double tol, int* d_sweeps);
+// The same SVD on a cluster of 8 CTAs (J carried with X, distributed shared
+// memory between rounds); jacobi_cluster_fits says whether (m, k) fits.
+bool jacobi_cluster_fits(int m, int k);
+void jacobi_svd_cluster(Ctx& c, double* X, int m, int k, int64_t ldx, double* J, int64_t ldj, double* S,
+                        int max_sweeps, double tol, int* d_sweeps);
 // Complex (complex128) counterparts for complex iPEPS tensors, one CTA each;
 // complex_small_fits(m, k) says whether all three fit in shared memory.
 bool complex_small_fits(int m, int k);

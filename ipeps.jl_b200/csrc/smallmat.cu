@@ -293,6 +293,8 @@ __device__ __forceinline__ bool rr_pair(int pi, int r, int kk, int k, int& p, in
 }
 
 constexpr int kJacThreads = 512;  // 64 groups of 8 lanes, one column pair each per round
+// sketch width from which the Jacobi SVD runs on a cluster of 8 CTAs
+constexpr int kClusterJacobiMinK = 96;
 
 // One-sided Jacobi on X (m x k, rows zero-padded to 16 NV) held in shared
 // memory.  Each 8-lane group takes one column pair per round: it reads both
@@ -477,16 +479,13 @@ __global__ void __launch_bounds__(kApplyRows * 32) jacobi_apply_kernel(const dou
     for (int j = lane; j < k; j += 32) J[i + int64_t(j) * ldj] = row[j];
 }
 
-// shared-memory opt-in done once per kernel (concurrent moves may race to it: atomics)
-std::atomic<bool> g_chol_attr{false}, g_trsm_attr[9], g_jlog_attr[11], g_apply_attr{false};
+// shared-memory opt-in, once per kernel and device
+SmemAttrOnce g_chol_attr, g_trsm_attr[9], g_jlog_attr[11], g_apply_attr;
 
 template <int NV>
 void launch_jacobi(Ctx& c, double* X, int m, int k, int64_t ldx, double2* rot, int max_sweeps, double tol, double* S,
                    int* d_sweeps, size_t smem) {
-  if (!g_jlog_attr[NV]) {
-    IPEPS_CUDA(cudaFuncSetAttribute(jacobi_log_kernel<NV>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemMax)));
-    g_jlog_attr[NV] = true;
-  }
+  g_jlog_attr[NV].ensure(jacobi_log_kernel<NV>, int(kSmemMax));
   jacobi_log_kernel<NV><<<1, kJacThreads, smem, c.stream>>>(X, m, k, ldx, rot, max_sweeps, tol, S, c.d_status, d_sweeps);
   IPEPS_LAUNCH_CHECK();
 }
@@ -495,10 +494,7 @@ template <int NS>
 void launch_trsm(Ctx& c, const double* Y, int64_t ldy, int64_t N, int k, const double* R, int64_t ldr,
                  const double* Rrow, double* Q, int64_t ldq) {
   const size_t smem = trsm_smem_bytes(k);
-  if (!g_trsm_attr[NS]) {
-    IPEPS_CUDA(cudaFuncSetAttribute(trsm_rows_kernel<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemMax)));
-    g_trsm_attr[NS] = true;
-  }
+  g_trsm_attr[NS].ensure(trsm_rows_kernel<NS>, int(kSmemMax));
   const unsigned grid = unsigned((N + kTrsmRows - 1) / kTrsmRows);
   trsm_rows_kernel<NS><<<grid, kTrsmRows * 32, smem, c.stream>>>(Y, ldy, N, k, R, ldr, Rrow, Q, ldq);
   IPEPS_LAUNCH_CHECK();
@@ -510,10 +506,7 @@ bool chol_fits(int k) { return k >= 1 && chol_smem_doubles(k) * 8 <= kSmemMax; }
 
 void chol_blocked(Ctx& c, double* G, int k, int64_t ldg, double shift_factor, double* Rrow) {
   IPEPS_CHECK(chol_fits(k), "chol_blocked: k too large for shared memory");
-  if (!g_chol_attr) {
-    IPEPS_CUDA(cudaFuncSetAttribute(chol_blocked_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemMax)));
-    g_chol_attr = true;
-  }
+  g_chol_attr.ensure(chol_blocked_kernel, int(kSmemMax));
   ProfScope ps(c, KFam::SmallLinalg);
   chol_blocked_kernel<<<1, kCholThreads, chol_smem_doubles(k) * 8, c.stream>>>(G, k, ldg, shift_factor, Rrow);
   IPEPS_LAUNCH_CHECK();
@@ -543,6 +536,10 @@ void trsm_right_upper(Ctx& c, const double* Y, int64_t ldy, int64_t N, int k, co
 void jacobi_svd_auto(Ctx& c, double* X, int m, int k, int64_t ldx, double* J, int64_t ldj, double* S,
                      int max_sweeps, double tol, int* d_sweeps) {
   if (tol <= 0) tol = double(m) * 2.220446049250313e-16;  // rounding level of the column dot products
+  if (k >= kClusterJacobiMinK && jacobi_cluster_fits(m, k)) {
+    jacobi_svd_cluster(c, X, m, k, ldx, J, ldj, S, max_sweeps, tol, d_sweeps);
+    return;
+  }
   const int nv = (m + 15) / 16;
   const size_t smem = (size_t(16) * nv * k + k) * 8;
   if (k < 2 || nv > 10 || k > 2 * kMaxPairs || smem > kSmemMax || apply_smem_bytes(k) > kSmemMax) {
@@ -570,10 +567,7 @@ void jacobi_svd_auto(Ctx& c, double* X, int m, int k, int64_t ldx, double* J, in
   }
   {
     ProfScope ps(c, KFam::Jacobi);
-    if (!g_apply_attr) {
-      IPEPS_CUDA(cudaFuncSetAttribute(jacobi_apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemMax)));
-      g_apply_attr = true;
-    }
+    g_apply_attr.ensure(jacobi_apply_kernel, int(kSmemMax));
     const unsigned grid = unsigned((k + kApplyRows - 1) / kApplyRows);
     jacobi_apply_kernel<<<grid, kApplyRows * 32, apply_smem_bytes(k), c.stream>>>(rp, k, d_sweeps, J, ldj);
     IPEPS_LAUNCH_CHECK();

@@ -281,7 +281,7 @@ __global__ void __launch_bounds__(kApplyCRows * 32) jacobi_c_apply_kernel(const 
   for (int j = lane; j < k; j += 32) J[i + int64_t(j) * ldj] = row[j];
 }
 
-std::atomic<bool> g_cholc_attr{false}, g_trsmc_attr{false}, g_jacc_attr{false}, g_appc_attr{false};
+SmemAttrOnce g_cholc_attr, g_trsmc_attr, g_jacc_attr, g_appc_attr;
 
 size_t cholc_smem(int k) { return (size_t(k) * (k + 1) / 2 + size_t(k)) * 16; }
 size_t trsmc_smem(int k) { return (size_t(k) * (k + 1) / 2 + size_t(kTrsmCRows) * k) * 16 + size_t(k) * 8; }
@@ -295,10 +295,7 @@ bool complex_small_fits(int m, int k) {
 
 void chol_c(Ctx& c, void* G, int k, int64_t ldg, double shift_factor) {
   IPEPS_CHECK(cholc_smem(k) <= kSmemMaxC, "chol_c: k too large for shared memory");
-  if (!g_cholc_attr) {
-    IPEPS_CUDA(cudaFuncSetAttribute(chol_c_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemMaxC)));
-    g_cholc_attr = true;
-  }
+  g_cholc_attr.ensure(chol_c_kernel, int(kSmemMaxC));
   ProfScope ps(c, KFam::SmallLinalg);
   chol_c_kernel<<<1, kCholCThreads, cholc_smem(k), c.stream>>>(static_cast<double2*>(G), k, ldg, shift_factor);
   IPEPS_LAUNCH_CHECK();
@@ -308,10 +305,7 @@ void chol_c(Ctx& c, void* G, int k, int64_t ldg, double shift_factor) {
 void trsm_c(Ctx& c, const void* Y, int64_t ldy, int64_t N, int k, const void* R, int64_t ldr, void* Q, int64_t ldq) {
   IPEPS_CHECK(trsmc_smem(k) <= kSmemMaxC, "trsm_c: k too large for shared memory");
   if (N == 0) return;
-  if (!g_trsmc_attr) {
-    IPEPS_CUDA(cudaFuncSetAttribute(trsm_c_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemMaxC)));
-    g_trsmc_attr = true;
-  }
+  g_trsmc_attr.ensure(trsm_c_kernel, int(kSmemMaxC));
   ProfScope ps(c, KFam::SmallLinalg);
   const unsigned grid = unsigned((N + kTrsmCRows - 1) / kTrsmCRows);
   trsm_c_kernel<<<grid, kTrsmCRows * 32, trsmc_smem(k), c.stream>>>(static_cast<const double2*>(Y), ldy, N, k,
@@ -325,10 +319,7 @@ void jacobi_c_svd(Ctx& c, void* X, int m, int k, int64_t ldx, void* J, int64_t l
                   double tol, int* d_sweeps) {
   IPEPS_CHECK(jacc_smem(m, k) <= kSmemMaxC, "jacobi_c_svd: sketch too wide for shared memory");
   if (tol <= 0) tol = double(m) * 2.220446049250313e-16;
-  if (!g_jacc_attr) {
-    IPEPS_CUDA(cudaFuncSetAttribute(jacobi_c_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemMaxC)));
-    g_jacc_attr = true;
-  }
+  g_jacc_attr.ensure(jacobi_c_kernel, int(kSmemMaxC));
   const int kk = (k + 1) & ~1;
   // two double2 per pair slot: (cs, sn) and e^{-i phi}
   Tensor rot = c.alloc(DType::F64, {int64_t(max_sweeps) * (kk - 1) * kk * 2});
@@ -343,11 +334,7 @@ void jacobi_c_svd(Ctx& c, void* X, int m, int k, int64_t ldx, void* J, int64_t l
   {
     ProfScope ps(c, KFam::Jacobi);
     const size_t smem = size_t(kApplyCRows) * k * 16;
-    if (!g_appc_attr) {
-      IPEPS_CUDA(
-          cudaFuncSetAttribute(jacobi_c_apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemMaxC)));
-      g_appc_attr = true;
-    }
+    g_appc_attr.ensure(jacobi_c_apply_kernel, int(kSmemMaxC));
     const unsigned grid = unsigned((k + kApplyCRows - 1) / kApplyCRows);
     jacobi_c_apply_kernel<<<grid, kApplyCRows * 32, smem, c.stream>>>(rp, k, d_sweeps, static_cast<double2*>(J), ldj);
     IPEPS_LAUNCH_CHECK();

@@ -246,3 +246,24 @@ def test_degenerate_rule_keeps_zero_singular_value(engine, pkg):
     assert info["converged"] and np.isfinite(E.real)
     assert abs(E.real - Eo) <= 1e-10, (E.real, Eo, [c.shape for c in ts.Cs], [tuple(c.shape) for c in ts_o.Cs])
     ts.close()
+
+
+def test_projector_wide_sketch_matches_oracle(engine, pkg):
+    """A sketch of 128+ columns (chi = 80 of N = 400), whose Rayleigh-Ritz SVD
+    runs on the 8-CTA cluster Jacobi: leading singular values 1e-10 relative,
+    P1 P2 1e-8 relative."""
+    rng = np.random.default_rng(21)
+    N, chi = 400, 80
+    U, _ = np.linalg.qr(rng.standard_normal((N, N)))
+    V, _ = np.linalg.qr(rng.standard_normal((N, N)))
+    s = np.exp(-0.08 * np.arange(N))
+    R1 = U @ np.diag(np.sqrt(s)) @ rng.standard_normal((N, N)) * 0.1
+    R2 = np.linalg.solve(rng.standard_normal((N, N)) * 0.1, np.diag(np.sqrt(s)) @ V.T)
+    P1o, P2o, So = O.get_projector(torch.tensor(R1), torch.tensor(R2), chi)
+    P1, P2, S = pkg.get_projector(R1, R2, chi, engine=engine)
+    So = npa(So)
+    assert len(S) == len(So)
+    assert np.allclose(S[:20], So[:20], rtol=1e-10)
+    assert np.allclose(S, So, rtol=1e-7)
+    Po = npa(P1o) @ npa(P2o)
+    assert np.linalg.norm(P1 @ P2 - Po) <= 1e-8 * np.linalg.norm(Po)
