@@ -115,7 +115,9 @@ IPEPS_API int ipeps_env_set_svd_params(ipeps_env* env, int over_num, int over_de
                                        int inter_passes, int seed_older);
 /* mixed form (IPEPS_PREC_MIXED contexts only): run_ctm switches to FP64 for the
  * last polish_iters iterations, or once the change per iteration drops below
- * polish_tol, and accepts convergence only after polish_iters FP64 iterations
+ * polish_tol * rg_tol (default 100: close to the requested convergence; with
+ * rg_tol = 0 only the last iterations), and accepts convergence only after
+ * polish_iters FP64 iterations
  * (0 = stay in the mixed form).  No counterpart in the reference (FP64 only). */
 IPEPS_API int ipeps_env_set_mixed(ipeps_env* env, int polish_iters, double polish_tol);
 /* A (D,D,D,D,d); Ad = NULL means conj(A) (CTMTensors(A, cfg), ctm_tensor.jl:63) */
@@ -193,6 +195,11 @@ IPEPS_API int ipeps_energy_4x4(ipeps_env* env, const ipeps_ctensor_t* H4, int ne
  * (nested = 1) (optim_es_h4.jl:33,139); as ipeps_ctm_run otherwise. */
 IPEPS_API int ipeps_ctm_run_4x4(ipeps_env* env, const ipeps_ctensor_t* H4, int nested, int* iters,
                                 double* last_diff, int* converged);
+/* Pullback of run_gs_h4 w.r.t. A (the fg! of optim_gs_h4, optim_gs_h4.jl:53-91,113-123):
+ * ad_iters CTMRG iterations from the current environment with the plaquette energy as
+ * convergence value, E = real(get_gs_energy_4x4), dA real (D,D,D,D,d); real A only. */
+IPEPS_API int ipeps_energy_grad_4x4(ipeps_env* env, const ipeps_ctensor_t* H4, int ad_iters, double* E,
+                                    double* dA);
 /* Pullback of run_es_h4 w.r.t. B (get_es_grad_h4, optim_es_h4.jl:133-168): as
  * ipeps_es_energy_grad with the plaquette energy; E = real(get_es_energy_4x4). */
 IPEPS_API int ipeps_es_energy_grad_4x4(ipeps_env* env, const ipeps_ctensor_t* H4, int ad_iters, double* E,

@@ -441,7 +441,10 @@ void projector_backward(Ctx& c, const Tensor& R1t, bool t1, const Tensor& R2t, b
     Tensor Yu = project_out(c, Ur, dUt), Yv = project_out(c, Vr, dVt);
     Tensor Xu = c.zeros(DType::F64, {N1, n}), Xv = c.zeros(DType::F64, {N2, n});
     double* d_cmax = reinterpret_cast<double*>(c.scal->p) + 40;
-    constexpr int kSeriesTerms = 16;
+    const char* cap_env = std::getenv("IPEPS_SERIES_CAP");
+    const char* tol_env = std::getenv("IPEPS_SERIES_TOL");
+    const int kSeriesTerms = cap_env ? std::atoi(cap_env) : 16;
+    const double series_tol = tol_env ? std::atof(tol_env) : 1e-15;
     bool series_done = false;
     for (int m = 0; m < kSeriesTerms; ++m) {
       series_acc_kernel<<<gridn(c, N1 * n), 256, 0, c.stream>>>(Xu.f64(), Yu.f64(), N1, n, s.f64(), kSvdEta, m);
@@ -452,7 +455,7 @@ void projector_backward(Ctx& c, const Tensor& R1t, bool t1, const Tensor& R2t, b
       IPEPS_CUDA(cudaMemcpyAsync(&cmax, d_cmax, 8, cudaMemcpyDeviceToHost, c.stream));
       const double ny = std::sqrt(dot_host(c, Yu, Yu) + dot_host(c, Yv, Yv));
       const double nx = std::sqrt(dot_host(c, Xu, Xu) + dot_host(c, Xv, Xv));
-      if (cmax * ny <= 1e-15 * nx || ny == 0.0) {
+      if (cmax * ny <= series_tol * nx || ny == 0.0) {
         series_done = true;
         break;
       }
@@ -545,7 +548,43 @@ struct IterCk {
 
 }  // namespace
 
-double energy_grad(Env& e, const Tensor& Hh, const Tensor& Hv, int ad_iters, Tensor* gA) {
+namespace {
+
+__global__ void real_part_kernel(const double2* x, double* y, int64_t n) {
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+    y[i] = x[i].x;
+}
+
+// the cotangent of a real variable from a possibly complex one: its real part
+Tensor real_of(Ctx& c, const Tensor& x) {
+  if (x.empty() || x.dt == DType::F64) return x;
+  Tensor y = c.alloc(DType::F64, x.shape());
+  const int64_t n = x.numel();
+  const unsigned g = unsigned(std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, int64_t(c.sm_count) * 8)));
+  real_part_kernel<<<g, 256, 0, c.stream>>>(static_cast<const double2*>(x.data()), y.f64(), n);
+  IPEPS_LAUNCH_CHECK();
+  return y;
+}
+
+std::complex<double> scalar_host(Ctx& c, const Tensor& t) {
+  double h[2] = {0, 0};
+  IPEPS_CUDA(cudaMemcpyAsync(h, t.data(), t.dt == DType::F64 ? 8 : 16, cudaMemcpyDeviceToHost, c.stream));
+  c.sync();
+  return {h[0], t.dt == DType::F64 ? 0.0 : h[1]};
+}
+
+// a one-element cotangent of dtype dt with value v (the real part when dt is real)
+Tensor scalar_seed(Ctx& c, const Tensor& like, std::complex<double> v) {
+  Tensor g = c.alloc(like.dt, like.shape());
+  const double h[2] = {v.real(), v.imag()};
+  IPEPS_CUDA(cudaMemcpyAsync(g.data(), h, like.dt == DType::F64 ? 8 : 16, cudaMemcpyHostToDevice, c.stream));
+  c.sync();
+  return g;
+}
+
+}  // namespace
+
+double energy_grad(Env& e, const Tensor& Hh, const Tensor& Hv, int ad_iters, Tensor* gA, const H4* h4) {
   Ctx& c = *e.ctx;
   IPEPS_CHECK(e.dt == DType::F64 && !e.nested, "energy_grad: real single-site A only");
   // Mixed form: the checkpointed iterations and their recomputation on the
@@ -573,16 +612,19 @@ double energy_grad(Env& e, const Tensor& Hh, const Tensor& Hv, int ad_iters, Ten
       ctm_moves4(e, k.proj.data());
       ck.push_back(std::move(k));
       // run_ctm's early exit (ctmrg.jl:44) can only trigger once i >= min_iter
-      if (i >= e.prm.min_iter && i < ad_iters) {
+      auto energy_now = [&]() {
+        if (h4) return gs_energy_4x4(e, *h4);
         std::complex<double> E, Na;
         gs_energy(e, Hh, Hv, &E, &Na);
+        return E;
+      };
+      if (i >= e.prm.min_iter && i < ad_iters) {
+        const std::complex<double> E = energy_now();
         const double diff = std::abs(E - conv);
         conv = E;
         if (diff < e.prm.rg_tol) break;
       } else if (i < ad_iters && e.prm.min_iter < ad_iters) {
-        std::complex<double> E, Na;
-        gs_energy(e, Hh, Hv, &E, &Na);
-        conv = E;
+        conv = energy_now();
       }
     }
   }
@@ -601,6 +643,28 @@ double energy_grad(Env& e, const Tensor& Hh, const Tensor& Hv, int ad_iters, Ten
       E[i] = tp.leaf(e.Es[i]);
     }
     AV A = tp.leaf(e.A), Ad = tp.leaf(e.Ad);
+    if (h4) {
+      // get_gs_energy_4x4 (evaluation.jl:339-356): Re(en / nrm), both on the
+      // tape; seeds conj(1 / nrm) and conj(-en / nrm^2)
+      Arr4<ADPolicy> sv, As{A, A, A, A}, Ads{Ad, Ad, Ad, Ad};
+      for (int k = 0; k < 4; ++k) sv[k] = tp.constant((*h4)[k]);
+      Arr4<ADPolicy> op = get_op_Ad4(p, sv, Ads);
+      auto en = energy_norm_4x4(p, C[0], C[1], C[2], C[3], E[0], E[0], E[1], E[1], E[2], E[2], E[3], E[3], As,
+                                Ads, op);
+      const std::complex<double> ev = scalar_host(c, en[0].t), nv = scalar_host(c, en[1].t);
+      Ere = (ev / nv).real();
+      tp.acc(en[0].id, scalar_seed(c, en[0].t, std::conj(1.0 / nv)));
+      tp.acc(en[1].id, scalar_seed(c, en[1].t, std::conj(-ev / (nv * nv))));
+      c.precision = prec_bw;
+      tp.backward();
+      // every variable is real: the real parts of the cotangents
+      for (int i = 0; i < 4; ++i) {
+        gC[i] = real_of(c, tp.grad(C[i].id));
+        gE[i] = real_of(c, tp.grad(E[i].id));
+      }
+      gAcc = real_of(c, tp.grad(A.id));
+      gAdc = real_of(c, tp.grad(Ad.id));
+    } else {
     AV roh = get_dm_h(p, C[0], C[1], C[2], C[3], E[0], E[0], E[1], E[2], E[2], E[3], A, A, Ad, Ad);
     AV rov = get_dm_v(p, C[0], C[1], C[2], C[3], E[0], E[1], E[1], E[2], E[3], E[3], A, A, Ad, Ad);
     auto t = dm_traces(c, {{roh.t, Hh}, {rov.t, Hv}});
@@ -630,6 +694,7 @@ double energy_grad(Env& e, const Tensor& Hh, const Tensor& Hv, int ad_iters, Ten
     }
     gAcc = tp.grad(A.id);
     gAdc = tp.grad(Ad.id);
+    }
   }
   // reverse over the iterations, recomputing each on a tape
   for (int it = int(ck.size()) - 1; it >= 0; --it) {

@@ -66,7 +66,10 @@ void ad_projector(Tape& tp, const AV& R1, bool t1, const AV& R2, bool t2, const 
 // with A as the variable, evaluate get_gs_energy and return real(E) and
 // dE/dA (real A only).  C/T are checkpointed per iteration and each
 // iteration is recomputed on a tape in the backward pass.
-double energy_grad(Env& e, const Tensor& Hh, const Tensor& Hv, int ad_iters, Tensor* gA);
+// h4 (optional): the plaquette energy get_gs_energy_4x4 (run_gs_h4,
+// optim_gs_h4.jl:113-123) instead of the bond energies; Hh, Hv unused then.
+double energy_grad(Env& e, const Tensor& Hh, const Tensor& Hv, int ad_iters, Tensor* gA,
+                   const std::array<Tensor, 4>* h4 = nullptr);
 
 // Pullback of run_es (optim_es.jl:196-210) with respect to B from the nested
 // environment held by e: runs ad_iters nested iterations, returns

@@ -592,6 +592,24 @@ extern "C" int ipeps_ctm_run_4x4(ipeps_env* env, const ipeps_ctensor_t* H4, int 
   });
 }
 
+extern "C" int ipeps_energy_grad_4x4(ipeps_env* env, const ipeps_ctensor_t* H4, int ad_iters, double* E,
+                                     double* dA) {
+  if (!env) return IPEPS_EINVAL;
+  return guarded(env->owner, [&] {
+    IPEPS_CHECK(ad_iters >= 1, "ad_iters must be >= 1");
+    auto& c = *env->e.ctx;
+    ipeps::H4 h = upload_H4(c, H4);
+    uint64_t m0 = env->e.moves;
+    double s0 = env->e.move_seconds;
+    Tensor g, none;
+    double e = ipeps::energy_grad(env->e, none, none, ad_iters, &g, &h);
+    account(env, m0, s0);
+    if (E) *E = e;
+    if (dA) download(c, dA, g);
+    return IPEPS_OK;
+  });
+}
+
 extern "C" int ipeps_es_energy_grad_4x4(ipeps_env* env, const ipeps_ctensor_t* H4, int ad_iters, double* E,
                                         double* gB) {
   if (!env) return IPEPS_EINVAL;

@@ -679,9 +679,11 @@ int run_ctm(Env& e, int conv_mode, const Tensor* Hh, const Tensor* Hv, double* l
   bool done = false;
   // Mixed form: 3xTF32 contractions while the environment is still moving, then
   // FP64 for the last polish_iters iterations (or from the point where the
-  // change per iteration drops below polish_tol), and convergence is accepted
-  // only after that many FP64 iterations.  The CTMRG map contracts errors, so
-  // the FP32-level errors of the mixed iterations decay in the FP64 ones.
+  // change per iteration drops below polish_tol * rg_tol, i.e. close to the
+  // requested convergence), and convergence is accepted only after that many
+  // FP64 iterations.  The CTMRG map contracts errors, so the FP32-level errors
+  // of the mixed iterations decay in the FP64 ones.  With rg_tol = 0 (a fixed
+  // number of iterations) only the last polish_iters iterations run in FP64.
   Ctx& c = *e.ctx;
   const int prec0 = c.precision;
   const bool polish = (prec0 == kPrecMixed) && e.prm.polish_iters > 0;
@@ -711,7 +713,7 @@ int run_ctm(Env& e, int conv_mode, const Tensor* Hh, const Tensor* Hv, double* l
     };
     int last = 0;
     for (; i <= e.prm.max_iter; ++i) {
-      if (polish && c.precision != kPrecFP64 && (i >= polish_start || diffs.back() < e.prm.polish_tol))
+      if (polish && c.precision != kPrecFP64 && (i >= polish_start || diffs.back() < e.prm.polish_tol * e.prm.rg_tol))
         c.precision = kPrecFP64;
       std::vector<double> s = rg_step(e);
       if (polish && c.precision == kPrecFP64) fp64_done++;
@@ -733,7 +735,7 @@ int run_ctm(Env& e, int conv_mode, const Tensor* Hh, const Tensor* Hv, double* l
     return done ? last : e.prm.max_iter;
   }
   for (; i <= e.prm.max_iter; ++i) {
-    if (polish && c.precision != kPrecFP64 && (i >= polish_start || diffs.back() < e.prm.polish_tol))
+    if (polish && c.precision != kPrecFP64 && (i >= polish_start || diffs.back() < e.prm.polish_tol * e.prm.rg_tol))
       c.precision = kPrecFP64;
     std::vector<double> s = rg_step(e);
     if (polish && c.precision == kPrecFP64) fp64_done++;

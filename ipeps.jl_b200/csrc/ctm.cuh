@@ -31,9 +31,10 @@ struct CtmParams {
   int max_iter = 20;
   int ad_max_iter = 4;
   double rg_tol = 1e-6;
-  // mixed form: FP64 for the last polish_iters iterations (0 = stay mixed)
+  // mixed form: FP64 for the last polish_iters iterations (0 = stay mixed), or
+  // from the iteration whose change drops below polish_tol * rg_tol
   int polish_iters = 4;
-  double polish_tol = 1e-6;
+  double polish_tol = 100.0;
   SvdParams svd;
 };
 

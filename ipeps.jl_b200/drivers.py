@@ -357,6 +357,13 @@ def prepare_basis_h4(h: np.ndarray, A, cfg: Dict[str, Any], engine: Optional[hos
     return ts, H4, basis
 
 
+def optim_gs_h4(h: np.ndarray, A0, cfg, engine: Optional[host.Engine] = None, **kw):
+    """optim_gs_h4 (optim_gs_h4.jl:14-98): optim_gs with the plaquette
+    Hamiltonian h (d^2, d^2, d^2, d^2), split into its MPO by get_local_h, and
+    the plaquette E+grad unit (host.fg_h4)."""
+    return optim_gs(get_local_h(h), A0, cfg, engine=engine, fg_fn=host.fg_h4, **kw)
+
+
 def es_column_h4(px: float, py: float, ts: host.CTMTensors, H4, basis: np.ndarray, i: int, C=None):
     """One basis vector of optim_es_h4 (optim_es_h4.jl:92-108): (effH[:, i], effN[:, i])."""
     C = C if C is not None else [ts.get_CT(k) for k in range(1, 5)]

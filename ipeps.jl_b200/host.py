@@ -41,7 +41,7 @@ EXPORTED = [
     "ipeps_ctm_log", "ipeps_energy", "ipeps_gs_norm", "ipeps_nested_set_B", "ipeps_es_energy",
     "ipeps_all_norm", "ipeps_tcon", "ipeps_projector", "ipeps_projector_c", "ipeps_ctx_stream", "ipeps_prof_enable",
     "ipeps_prof_query", "ipeps_energy_grad", "ipeps_env_set_mixed", "ipeps_es_energy_grad",
-    "ipeps_single_dm_Ad", "ipeps_energy_4x4", "ipeps_ctm_run_4x4", "ipeps_es_energy_grad_4x4", "ipeps_gemm_f64", "ipeps_gemm_tf32x3", "ipeps_gemm_bf16", "ipeps_mlp_create", "ipeps_mlp_destroy", "ipeps_mlp_num_params",
+    "ipeps_single_dm_Ad", "ipeps_energy_4x4", "ipeps_ctm_run_4x4", "ipeps_energy_grad_4x4", "ipeps_es_energy_grad_4x4", "ipeps_gemm_f64", "ipeps_gemm_tf32x3", "ipeps_gemm_bf16", "ipeps_mlp_create", "ipeps_mlp_destroy", "ipeps_mlp_num_params",
     "ipeps_mlp_get_params", "ipeps_mlp_set_params", "ipeps_mlp_forward", "ipeps_mlp_grad", "ipeps_mlp_train_step",
 ]
 
@@ -125,6 +125,7 @@ def load_library(path: str = LIB_PATH) -> ct.CDLL:
         "ipeps_es_energy_grad": [P, dp, dp, I, I, dp, dp],
         "ipeps_energy_4x4": [P, ct.POINTER(CTensor), I, dp],
         "ipeps_ctm_run_4x4": [P, ct.POINTER(CTensor), I, ip, dp, ip],
+        "ipeps_energy_grad_4x4": [P, ct.POINTER(CTensor), I, dp, dp],
         "ipeps_es_energy_grad_4x4": [P, ct.POINTER(CTensor), I, dp, dp],
         "ipeps_single_dm_Ad": [P, dp],
         "ipeps_gemm_f64": [P, ct.c_char, ct.c_char, ct.c_int64, ct.c_int64, ct.c_int64, D, dp, ct.c_int64, dp,
@@ -352,7 +353,7 @@ class CTMTensors:
             int(bool(p.get("svd_seed_older", True)))))
         self.engine.check(self.lib.ipeps_env_set_parallel(self.h, int(bool(p.get("parallel_moves", True)))))
         self.engine.check(self.lib.ipeps_env_set_mixed(
-            self.h, int(p.get("mixed_polish_iters", 4)), float(p.get("mixed_polish_tol", 1e-6))))
+            self.h, int(p.get("mixed_polish_iters", 4)), float(p.get("mixed_polish_tol", 100.0))))
 
     def get_CT(self, k: int):
         """(C_k, E_k) as column-major numpy arrays, k = 1..4."""
@@ -533,6 +534,32 @@ def run_ctm_4x4(ts: CTMTensors, H4, nested: bool = False):
     ts.engine.check(ts.lib.ipeps_ctm_run_4x4(ts.h, h.c, int(bool(nested)), ct.byref(iters), ct.byref(diff),
                                              ct.byref(conv)))
     return ts, _run_info(ts, iters, diff, conv)
+
+
+def energy_grad_4x4(ts: CTMTensors, H4, ad_iters: Optional[int] = None):
+    """Pullback of run_gs_h4 (optim_gs_h4.jl:113-123) from the environment held
+    by ts: returns (real(E), dE/dA) with dE/dA a real (D,D,D,D,d) array."""
+    h = _H4(H4)
+    n = int(ts.Params.get("ad_max_iter", 4) if ad_iters is None else ad_iters)
+    ts._push_params()
+    E = np.zeros(1)
+    g = np.empty(ts.A.shape, dtype=np.float64, order="F")
+    ts.engine.check(ts.lib.ipeps_energy_grad_4x4(ts.h, h.c, n, _dp(E), _dp(g)))
+    return float(E[0]), g
+
+
+def fg_h4(x, H4, cfg, engine: Optional[Engine] = None):
+    """E+grad unit of optim_gs_h4 (fg!, optim_gs_h4.jl:53-91): x renormalised
+    (max-abs), CTMRG converged from init_ctm1 with the plaquette energy
+    (get_conv_boundary_h4), then the pullback of ad_max_iter iterations.
+    H4 is the MPO [s1, s2, s3, s4] of get_local_h.  Returns (E, g, info)."""
+    x = np.asarray(x, dtype=np.float64)
+    x = x / np.abs(x).max()
+    ts = CTMTensors(x, cfg, engine=engine)
+    ts, info = run_ctm_4x4(ts, H4, nested=False)
+    E, g = energy_grad_4x4(ts, H4)
+    ts.close()
+    return E, g, info
 
 
 def es_energy_grad_4x4(ts: CTMTensors, H4, ad_iters: Optional[int] = None):

@@ -865,6 +865,33 @@ def correlation_TM(ts, direction="h", N=10):
     return es1[:N], TM
 
 
+def run_gs_h4(ts, H, A):
+    """optim_gs_h4.jl:113-123: ad_max_iter iterations with the plaquette energy
+    as convergence value, then get_gs_energy_4x4."""
+    ts1 = ts.replace(A=A, Ad=conj(A))
+    ts1, _ = run_ctm(ts1, conv_fun=lambda t: get_gs_energy_4x4(t, H))
+    return get_gs_energy_4x4(ts1, H)
+
+
+def energy_and_grad_h4(x, H, cfg):
+    """The fg! of optim_gs_h4 (optim_gs_h4.jl:53-91): converge with the
+    plaquette criterion (get_conv_boundary_h4, :100-110), then the pullback of
+    run_gs_h4.  Returns (real(E), dE/dx)."""
+    x = renormalize(x.detach())
+    with torch.no_grad():
+        ts = make_ctm_tensors(x, cfg)
+        ts, _ = run_ctm(ts, conv_fun=lambda t: get_gs_energy_4x4(t, H))
+    ts = _detach_ts(ts)
+    p = dict(ts.Params)
+    p["max_iter"] = p.get("ad_max_iter", 4)
+    ts = ts.replace(Params=p)
+    xv = x.clone().requires_grad_(True)
+    y = run_gs_h4(ts, H, xv)
+    yr = y.real if torch.is_complex(y) else y
+    (g,) = torch.autograd.grad(yr, xv)
+    return float(yr.item()), g.detach(), ts
+
+
 def get_gs_norm(ts):
     """evaluation.jl:47-59"""
     n_dm = get_single_dm(*ts.Cs, *ts.Es)

@@ -53,3 +53,18 @@ def test_plaquette_energies_match_oracle(engine, pkg):
     Ee = pkg.get_es_energy_4x4(ts, H4)
     assert abs(Ee - Eeo) <= 1e-12 * max(1.0, abs(Eeo)), (Ee, Eeo)
     ts.close()
+
+
+def test_plaquette_energy_grad_matches_oracle(engine, pkg):
+    """fg! of optim_gs_h4 (optim_gs_h4.jl:53-91): the plaquette energy and its
+    gradient against the oracle's autograd, 1e-10 / 1e-6 relative."""
+    A = O.random_A(2, 2, seed=13)
+    h = _h4(5)
+    H4 = pkg.drivers.get_local_h(h)
+    cfg = O.default_config()
+    cfg.update(chi=8, min_iter=4, max_iter=40, rg_tol=1e-11, ad_max_iter=4)
+    Eo, go, _ = O.energy_and_grad_h4(A, [torch.tensor(x) for x in H4], cfg)
+    E, g, info = pkg.host.fg_h4(A.numpy(), H4, cfg, engine=engine)
+    go = go.numpy()
+    assert abs(E - Eo) <= 1e-10 * max(1.0, abs(Eo)), (E, Eo)
+    assert np.linalg.norm(g - go) <= 1e-6 * np.linalg.norm(go), np.linalg.norm(g - go) / np.linalg.norm(go)
