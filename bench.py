@@ -603,6 +603,40 @@ def run_tf32_shapes():
     return 0
 
 
+def run_projector_shapes():
+    """The truncated-SVD projector alone (ipeps_projector, host buffers; device
+    time from the engine's per-family profile) on synthetic enlarged corners of
+    the workload's size: R1, R2 of N x N, N = chi D^2, with a decaying spectrum;
+    the kernel-level aid behind the projector's ncu captures."""
+    pkg = load_pkg()
+    D, chi = WORKLOAD["D"], WORKLOAD["chi"]
+    N = chi * D * D
+    rng = np.random.default_rng(0)
+    s = np.exp(-0.02 * np.arange(N))
+    U, _ = np.linalg.qr(rng.standard_normal((N, N)))
+    R1 = (U * np.sqrt(s)) @ rng.standard_normal((N, N)) / np.sqrt(N)
+    R2 = np.linalg.solve(rng.standard_normal((N, N)) / np.sqrt(N), (np.sqrt(s)[:, None] * U.T))
+    for prec in ("fp64", "mixed"):
+        eng = pkg.Engine(0, precision=prec)
+        pkg.get_projector(R1, R2, chi, engine=eng)  # warm-up (kernel loads, pool)
+        eng.prof_enable(True)
+        reps = 3
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            P1, P2, S = pkg.get_projector(R1, R2, chi, engine=eng)
+        wall = (time.perf_counter() - t0) / reps
+        prof = eng.prof_query()
+        eng.prof_enable(False)
+        st = eng.stats()
+        print(json.dumps({"projector": f"N={N} chi={chi}", "precision": prec, "wall_ms_per_call": round(1e3 * wall, 2),
+                          "device_ms_per_call": {k: round(v["ms"] / reps, 3) for k, v in prof.items() if v["ms"] > 0},
+                          "launches_per_call": {k: v["launches"] // reps for k, v in prof.items() if v["launches"]},
+                          "jacobi_sweeps": st["jacobi_sweeps"], "extra_passes": st["extra_passes"],
+                          "s_head": [float(x) for x in S[:3]]}), flush=True)
+        eng.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -620,12 +654,17 @@ def main():
                          "projector's and the contractions' shapes, one JSON line per shape")
     ap.add_argument("--tf32-shapes", action="store_true",
                     help="kernel aid: 3xTF32 tcgen05 GEMM throughput (splits included) on the engine's shapes")
+    ap.add_argument("--projector-shapes", action="store_true",
+                    help="kernel aid: the projector alone on synthetic enlarged corners of the workload's size")
     args = ap.parse_args()
+    global WORKLOAD, WORKLOAD_NAME
+    if args.projector_shapes:
+        WORKLOAD = WORKLOADS[args.workload]
+        return run_projector_shapes()
     if args.gemm_shapes:
         return run_gemm_shapes()
     if args.tf32_shapes:
         return run_tf32_shapes()
-    global WORKLOAD, WORKLOAD_NAME
     WORKLOAD = WORKLOADS[args.workload]
     WORKLOAD_NAME = workload_name(WORKLOAD)
     if args.impl == "reference":

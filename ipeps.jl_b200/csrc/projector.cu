@@ -446,6 +446,7 @@ ProjResult projector_impl(Ctx& c, Ops& o, int chi, const SvdParams& sp, ProjCach
     IPEPS_CHECK(dt == DType::F64, "get_projector: the projector adjoint is real-only");
     r.r = rr;
     r.sr_host.assign(all.begin(), all.begin() + rr);
+    r.s_next = (rr < k) ? all[rr] : all[k - 1];
     Tensor Uxr = c.alloc(dt, {k, rr});
     gather_cols(c, sk.X.f64(), k, k, d_perm, rr, sk.Ss.f64(), 2, Uxr.f64(), k);
     r.Ur = c.alloc(dt, {N1, rr});

@@ -65,6 +65,10 @@ struct ProjResult {
   int r = 0;
   Tensor Ur, Vr, Sr;  // N x r, N x r, r
   std::vector<double> sr_host;
+  // upper estimate of the largest singular value outside the resolved set
+  // (the next sketch value, or the smallest resolved one when the sketch is
+  // exhausted): bounds the spectrum the adjoint's resolvent expansion sees
+  double s_next = 0;
 };
 
 // Returns P1 = R2 V S^-1/2, P2 = S^-1/2 U^T R1 with (U,S,V) the truncated
