@@ -491,18 +491,15 @@ void projector_backward(Ctx& c, const Tensor& R1t, bool t1, const Tensor& R2t, b
       Xu = c.zeros(DType::F64, {N1, n});
       Xv = c.zeros(DType::F64, {N2, n});
     }
+    // M = R1 R2 formed once (N1 x N2): each application of M M^T or M^T M is
+    // then two products instead of four
+    Tensor Mx = c.alloc(DType::F64, {N1, N2});
+    gemm(c, DType::F64, t1 ? 'T' : 'N', t2 ? 'T' : 'N', N1, N2, K1, cplx(1), R1t.data(), R1t.dims[0], R2t.data(),
+         R2t.dims[0], cplx(0), Mx.data(), N1);
     // B T = (2/b) P M M^T P T - T on the u side, (2/b) P' M^T M P' T - T on the v side
     auto apply_B = [&](const Tensor& Tu, const Tensor& Tv, Tensor* Bu, Tensor* Bv) {
-      Tensor t = Rapply(c, R1t, t1, 'T', Tu);
-      t = Rapply(c, R2t, t2, 'T', t);
-      t = Rapply(c, R2t, t2, 'N', t);
-      t = Rapply(c, R1t, t1, 'N', t);
-      *Bu = project_out(c, Ur, t);
-      t = Rapply(c, R2t, t2, 'N', Tv);
-      t = Rapply(c, R1t, t1, 'N', t);
-      t = Rapply(c, R1t, t1, 'T', t);
-      t = Rapply(c, R2t, t2, 'T', t);
-      *Bv = project_out(c, Vr, t);
+      *Bu = project_out(c, Ur, mm(c, Mx, 'N', mm(c, Mx, 'T', Tu, 'N'), 'N'));
+      *Bv = project_out(c, Vr, mm(c, Mx, 'T', mm(c, Mx, 'N', Tv, 'N'), 'N'));
       axpby_kernel<<<gridn(c, Bu->numel()), 256, 0, c.stream>>>(-1.0, Tu.f64(), 2.0 / b, Bu->f64(), Bu->numel());
       axpby_kernel<<<gridn(c, Bv->numel()), 256, 0, c.stream>>>(-1.0, Tv.f64(), 2.0 / b, Bv->f64(), Bv->numel());
       IPEPS_LAUNCH_CHECK();
@@ -553,9 +550,9 @@ void projector_backward(Ctx& c, const Tensor& R1t, bool t1, const Tensor& R2t, b
       flag_status(c, 16);
     }
     // Acol += M^T X_u ; Bcol += M X_v ; and the s_t-scaled terms
-    Tensor MtXu = Rapply(c, R2t, t2, 'T', Rapply(c, R1t, t1, 'T', Xu));
+    Tensor MtXu = mm(c, Mx, 'T', Xu, 'N');
     axpy(c, cplx(1), MtXu, W1);
-    Tensor MXv = Rapply(c, R1t, t1, 'N', Rapply(c, R2t, t2, 'N', Xv));
+    Tensor MXv = mm(c, Mx, 'N', Xv, 'N');
     axpy(c, cplx(1), MXv, Bcol);
     axpy(c, cplx(1), Xv, VinGv_plus_Xv);
     axpy(c, cplx(1), Xu, UinGu_plus_Xu);

@@ -147,6 +147,16 @@ Tensor orth(Ctx& c, const Tensor& Y0, int passes, Tensor* Rout) {
 
 namespace {
 
+// out[j] = ||X[:, j]|| for j < nc (FP64, one warp per column)
+__global__ void colnorms_kernel(const double* X, int64_t m, int nc, double* out) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (warp >= nc) return;
+  double s = 0;
+  for (int64_t i = lane; i < m; i += 32) s = fma(X[i + warp * m], X[i + warp * m], s);
+  for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (lane == 0) out[warp] = sqrt(s);
+}
+
 // max over columns j < nc of ||X[:, j]|| (FP64, one warp per column)
 __global__ void colnorm_max_kernel(const double* X, int64_t m, int nc, unsigned long long* out) {
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
@@ -444,6 +454,28 @@ ProjResult projector_impl(Ctx& c, Ops& o, int chi, const SvdParams& sp, ProjCach
   }
   if (keep_factors) {
     IPEPS_CHECK(dt == DType::F64, "get_projector: the projector adjoint is real-only");
+    // The adjoint sums the resolved triplets exactly and expands the rest of the
+    // spectrum on their complement, which is exact only if the resolved vectors
+    // span an invariant subspace: keep just the leading triplets whose residual
+    // ||M v_a - s_a u_a|| is at most 1e-10 s_1 (the sketch's oversampled tail is
+    // less accurate and goes to the expansion instead).
+    if (rr > n) {
+      Tensor Vall = c.alloc(dt, {N2, rr});
+      copy_cols(c, Vall, Vk, N2, rr, w);
+      Tensor Res = o.M(Vall);
+      Tensor Wall = c.alloc(dt, {k, rr});
+      gather_cols(c, sk.X.f64(), k, k, d_perm, rr, nullptr, 0, Wall.f64(), k);
+      gemm(c, dt, 'N', 'N', N1, rr, k, cplx(-1), sk.Q.data(), N1, Wall.data(), k, cplx(1), Res.data(), N1, true);
+      Tensor rn = c.alloc(DType::F64, {rr});
+      colnorms_kernel<<<(rr * 32 + 255) / 256, 256, 0, c.stream>>>(Res.f64(), N1, rr, rn.f64());
+      IPEPS_LAUNCH_CHECK();
+      std::vector<double> rh(rr);
+      IPEPS_CUDA(cudaMemcpyAsync(rh.data(), rn.data(), size_t(rr) * 8, cudaMemcpyDeviceToHost, c.stream));
+      c.sync();
+      int acc = n;
+      while (acc < rr && rh[acc] <= 1e-10 * all[0]) ++acc;
+      rr = acc;
+    }
     r.r = rr;
     r.sr_host.assign(all.begin(), all.begin() + rr);
     r.s_next = (rr < k) ? all[rr] : all[k - 1];
