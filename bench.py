@@ -519,7 +519,8 @@ def run_ours(args):
             "roofline": roofline(forms[0]),
             "projector": {"calls": st["projector_calls"], "jacobi_sweeps_per_call":
                           st["jacobi_sweeps"] / max(1, st["projector_calls"]),
-                          "extra_passes": st["extra_passes"], "series_cap_hits": st["series_cap_hits"]},
+                          "extra_passes": st["extra_passes"], "series_cap_hits": st["series_cap_hits"],
+                          "adjoint_series_terms": st["series_terms"], "adjoint_series_retries": st["series_retries"]},
             "accuracy": acc,
             "cpu_baseline": cpu,
             "clocks": clocks,

@@ -59,8 +59,14 @@ typedef struct {
   uint64_t projector_calls; /* truncated-SVD projectors computed */
   uint64_t jacobi_sweeps;   /* one-sided Jacobi sweeps summed over those projectors */
   uint64_t extra_passes;    /* extra power iterations triggered by the residual check */
-  uint64_t series_cap_hits; /* projector adjoints whose resolvent series hit its 16-term cap
-                               before the 1e-15 tolerance (gradient possibly inexact) */
+  uint64_t series_cap_hits; /* projector adjoints whose Chebyshev expansion of the broadened
+                               resolvent hit its 160-term cap before its 1e-13 tolerance
+                               (gradient possibly inexact) */
+  uint64_t series_terms;    /* Chebyshev terms summed over all projector adjoints */
+  uint64_t series_retries;  /* expansions redone over a wider interval because the resolvent
+                               check ((x^2 + eta) f(x) = x on the result) failed */
+  uint64_t resid_misses;    /* projectors whose kept triplets stayed above the residual tolerance
+                               (the extra power iterations stopped converging or ran out) */
 } ipeps_stats_t;
 
 /* ---- context (no reference counterpart: the reference is one CPU process) */

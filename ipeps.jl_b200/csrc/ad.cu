@@ -138,8 +138,6 @@ __global__ void fin_kernel(int nin, int n, const double* C, const double* s_in, 
   }
 }
 
-// X[:, i] += Re[(s_i^2 - i sqrt(eta))^-(m+1)] Y[:, i]  (Taylor coefficient of the
-// broadened resolvent f(s_i^2 - t) = Re[1/(s_i^2 - i sqrt(eta) - t)] in t)
 // Chebyshev coefficient a_m(i) of the broadened resolvent on [0, b]:
 // Re[1 / (s_i^2 - i sqrt(eta) - t)] = Re[(2/b) / (z - x)], x = 2t/b - 1,
 // z = 2 (s_i^2 - i sqrt(eta)) / b - 1, and 1/(z - x) = sum_m e_m w^m T_m(x) / q
@@ -184,6 +182,29 @@ __global__ void cheb_coef_max_kernel(const double* s, int n, double eta, double 
   for (int i = threadIdx.x; i < n; i += blockDim.x) mx = fmax(mx, fabs(cheb_coef(s[i], eta, b, m)));
   for (int o = 16; o; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
   if (threadIdx.x == 0) *out = mx;
+}
+
+// Check of X[:, i] = f(s_i^2 - B) Y[:, i] through (x^2 + eta) f(x) = x:
+//   rhs = s_i^2 Y - BY,   res = (s_i^4 + eta) X - 2 s_i^2 BX + B^2 X - rhs
+__global__ void resolvent_check_kernel(const double* X, const double* BX, const double* BBX, const double* Y,
+                                       const double* BY, const double* s, double eta, int64_t N, int n, double* res,
+                                       double* rhs) {
+  const int64_t tot = N * n;
+  for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < tot; t += int64_t(gridDim.x) * blockDim.x) {
+    const double s2 = s[t / N] * s[t / N];
+    const double r = fma(s2, Y[t], -BY[t]);
+    rhs[t] = r;
+    res[t] = fma(fma(s2, s2, eta), X[t], fma(-2.0 * s2, BX[t], BBX[t])) - r;
+  }
+}
+
+// out[i] = sum_j X[i + j N]
+__global__ void rowsum_kernel(const double* X, int64_t N, int n, double* out) {
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < N; i += int64_t(gridDim.x) * blockDim.x) {
+    double a = 0;
+    for (int j = 0; j < n; ++j) a += X[i + j * N];
+    out[i] = a;
+  }
 }
 
 // y = alpha * x + beta * y (elementwise over n doubles)
@@ -466,85 +487,125 @@ void projector_backward(Ctx& c, const Tensor& R1t, bool t1, const Tensor& R2t, b
   }
   // complement of the resolved vectors: Chebyshev expansion of the broadened
   // resolvent f_i(t) = Re[1 / (s_i^2 - i sqrt(eta) - t)] over the unresolved
-  // spectrum t in [0, b] of M M^T (resp. M^T M), b = 1.25 s_next^2.  The
-  // coefficients decay like |w_i|^m with w_i set by s_i^2 / b alone, much
-  // faster than the Taylor series in t / s_i^2 when the unresolved spectrum
-  // comes close to the kept one; the recursion T_{m+1} = 2 B T_m - T_{m-1}
-  // (B = (2/b) P M M^T P - 1) keeps |T_m| <= |T_0| while the spectrum lies in
-  // [0, b], and b is doubled if it does not.
+  // spectrum t in [0, b] of B = P M M^T P (resp. P' M^T M P').  The
+  // coefficients decay like |w_i|^m with w_i set by s_i^2 / b alone; the
+  // recursion T_{m+1} = 2 B~ T_m - T_{m-1} (B~ = (2/b) B - 1) keeps
+  // |T_m| <= |T_0| while the spectrum lies in [0, b].  b must bound the
+  // spectrum: the sketch's estimate of the first unresolved singular value is a
+  // Ritz value, i.e. a lower bound, so b also covers a power-iteration estimate
+  // of the top of B, and every result is checked through the identity
+  // (x^2 + eta) f(x) = x, i.e. ((s_i^2 - B)^2 + eta) X_i = (s_i^2 - B) Y_i;
+  // a failed check redoes the expansion over a wider interval.
   {
     Tensor Ur = pr.Ur, Vr = pr.Vr;
     const Tensor Yu0 = project_out(c, Ur, dUt), Yv0 = project_out(c, Vr, dVt);
     double* d_cmax = reinterpret_cast<double*>(c.scal->p) + 40;
     constexpr int kMaxTerms = 160;
     constexpr double kTol = 1e-13;
+    constexpr double kCheckTol = 1e-10;
     const double ny0 = std::sqrt(dot_host(c, Yu0, Yu0) + dot_host(c, Yv0, Yv0));
-    // b bounds the unresolved spectrum (s_next^2) with a margin, kept below the
-    // smallest kept s_n^2 so that every resolvent's pole lies outside [0, b]
-    const double lam = pr.s_next * pr.s_next, sn2 = pr.sr_host[n - 1] * pr.sr_host[n - 1];
-    double b = 1.25 * lam;
-    if (b >= sn2) b = (lam < sn2) ? 0.5 * (lam + sn2) : lam;
-    if (!(b > 0)) b = sn2 > 0 ? 0.5 * sn2 : 1.0;
-    Tensor Xu, Xv;
-    bool series_done = (ny0 == 0.0);
-    if (series_done) {
-      Xu = c.zeros(DType::F64, {N1, n});
-      Xv = c.zeros(DType::F64, {N2, n});
-    }
+    Tensor Xu = c.zeros(DType::F64, {N1, n}), Xv = c.zeros(DType::F64, {N2, n});
     // M = R1 R2 formed once (N1 x N2): each application of M M^T or M^T M is
     // then two products instead of four
     Tensor Mx = c.alloc(DType::F64, {N1, N2});
     gemm(c, DType::F64, t1 ? 'T' : 'N', t2 ? 'T' : 'N', N1, N2, K1, cplx(1), R1t.data(), R1t.dims[0], R2t.data(),
          R2t.dims[0], cplx(0), Mx.data(), N1);
-    // B T = (2/b) P M M^T P T - T on the u side, (2/b) P' M^T M P' T - T on the v side
-    auto apply_B = [&](const Tensor& Tu, const Tensor& Tv, Tensor* Bu, Tensor* Bv) {
-      *Bu = project_out(c, Ur, mm(c, Mx, 'N', mm(c, Mx, 'T', Tu, 'N'), 'N'));
-      *Bv = project_out(c, Vr, mm(c, Mx, 'T', mm(c, Mx, 'N', Tv, 'N'), 'N'));
-      axpby_kernel<<<gridn(c, Bu->numel()), 256, 0, c.stream>>>(-1.0, Tu.f64(), 2.0 / b, Bu->f64(), Bu->numel());
-      axpby_kernel<<<gridn(c, Bv->numel()), 256, 0, c.stream>>>(-1.0, Tv.f64(), 2.0 / b, Bv->f64(), Bv->numel());
-      IPEPS_LAUNCH_CHECK();
-    };
-    for (int attempt = 0; !series_done && attempt < 4; ++attempt, b *= 2.0) {
-      Xu = c.zeros(DType::F64, {N1, n});
-      Xv = c.zeros(DType::F64, {N2, n});
-      Tensor Pu = Yu0, Pv = Yv0;  // T_{m-1}
-      Tensor Tu = Yu0, Tv = Yv0;  // T_m
-      bool blew_up = false;
-      for (int m = 0; m < kMaxTerms; ++m) {
-        cheb_acc_kernel<<<gridn(c, N1 * n), 256, 0, c.stream>>>(Xu.f64(), Tu.f64(), N1, n, s.f64(), kSvdEta, b, m);
-        cheb_acc_kernel<<<gridn(c, N2 * n), 256, 0, c.stream>>>(Xv.f64(), Tv.f64(), N2, n, s.f64(), kSvdEta, b, m);
-        cheb_coef_max_kernel<<<1, 32, 0, c.stream>>>(s.f64(), n, kSvdEta, b, m + 1, d_cmax);
+    auto Bu_of = [&](const Tensor& T) { return project_out(c, Ur, mm(c, Mx, 'N', mm(c, Mx, 'T', T, 'N'), 'N')); };
+    auto Bv_of = [&](const Tensor& T) { return project_out(c, Vr, mm(c, Mx, 'T', mm(c, Mx, 'N', T, 'N'), 'N')); };
+    bool series_done = (ny0 == 0.0);
+    if (!series_done) {
+      // b: above the sketch's s_next^2 and a power-iteration estimate of the
+      // top of B (six steps on the sum of the u-side cotangent columns), kept
+      // below the smallest kept s_n^2 so that every resolvent's pole lies outside [0, b]
+      const double lam = pr.s_next * pr.s_next, sn2 = pr.sr_host[n - 1] * pr.sr_host[n - 1];
+      double est = 0;
+      {
+        Tensor t = c.alloc(DType::F64, {N1, 1});
+        rowsum_kernel<<<gridn(c, N1), 256, 0, c.stream>>>(Yu0.f64(), N1, n, t.f64());
         IPEPS_LAUNCH_CHECK();
-        double cnext = 0;
-        IPEPS_CUDA(cudaMemcpyAsync(&cnext, d_cmax, 8, cudaMemcpyDeviceToHost, c.stream));
-        const double nt = std::sqrt(dot_host(c, Tu, Tu) + dot_host(c, Tv, Tv));
-        if (nt > 8.0 * ny0) {
-          blew_up = true;  // spectrum beyond b
-          break;
+        double nt = std::sqrt(dot_host(c, t, t));
+        for (int it = 0; it < 6 && nt > 0; ++it) {
+          Tensor bt = Bu_of(t);
+          const double nb = std::sqrt(dot_host(c, bt, bt));
+          est = nb / nt;
+          t = bt;
+          nt = nb;
         }
-        const double nx = std::sqrt(dot_host(c, Xu, Xu) + dot_host(c, Xv, Xv));
-        // |T_m| <= |T_0| on [0, b]: the remaining terms are bounded by the coefficient tail
-        if (cnext * ny0 <= kTol * nx) {
+      }
+      double b = std::max(1.25 * lam, 1.2 * est);
+      if (b >= sn2) b = (std::max(lam, est) < sn2) ? 0.5 * (std::max(lam, est) + sn2) : std::max(lam, est);
+      if (!(b > 0)) b = sn2 > 0 ? 0.5 * sn2 : 1.0;
+      // B~ T = (2/b) B T - T on both sides
+      auto apply_B = [&](const Tensor& Tu, const Tensor& Tv, Tensor* Bu, Tensor* Bv) {
+        *Bu = Bu_of(Tu);
+        *Bv = Bv_of(Tv);
+        axpby_kernel<<<gridn(c, Bu->numel()), 256, 0, c.stream>>>(-1.0, Tu.f64(), 2.0 / b, Bu->f64(), Bu->numel());
+        axpby_kernel<<<gridn(c, Bv->numel()), 256, 0, c.stream>>>(-1.0, Tv.f64(), 2.0 / b, Bv->f64(), Bv->numel());
+        IPEPS_LAUNCH_CHECK();
+      };
+      // relative residual of ((s_i^2 - B)^2 + eta) X_i = (s_i^2 - B) Y_i over all columns of one side
+      auto check = [&](const Tensor& X, const Tensor& Y, bool u_side) {
+        auto B = [&](const Tensor& T) { return u_side ? Bu_of(T) : Bv_of(T); };
+        const Tensor BX = B(X), BBX = B(BX), BY = B(Y);
+        Tensor res = c.alloc(DType::F64, X.shape()), rhs = c.alloc(DType::F64, X.shape());
+        resolvent_check_kernel<<<gridn(c, X.numel()), 256, 0, c.stream>>>(
+            X.f64(), BX.f64(), BBX.f64(), Y.f64(), BY.f64(), s.f64(), kSvdEta, X.dims[0], n, res.f64(), rhs.f64());
+        IPEPS_LAUNCH_CHECK();
+        const double nr = dot_host(c, rhs, rhs);
+        return nr > 0 ? std::sqrt(dot_host(c, res, res) / nr) : 0.0;
+      };
+      for (int attempt = 0; attempt < 6; ++attempt) {
+        Xu = c.zeros(DType::F64, {N1, n});
+        Xv = c.zeros(DType::F64, {N2, n});
+        Tensor Pu = Yu0, Pv = Yv0;  // T_{m-1}
+        Tensor Tu = Yu0, Tv = Yv0;  // T_m
+        bool blew_up = false, converged = false;
+        for (int m = 0; m < kMaxTerms; ++m) {
+          cheb_acc_kernel<<<gridn(c, N1 * n), 256, 0, c.stream>>>(Xu.f64(), Tu.f64(), N1, n, s.f64(), kSvdEta, b, m);
+          cheb_acc_kernel<<<gridn(c, N2 * n), 256, 0, c.stream>>>(Xv.f64(), Tv.f64(), N2, n, s.f64(), kSvdEta, b, m);
+          cheb_coef_max_kernel<<<1, 32, 0, c.stream>>>(s.f64(), n, kSvdEta, b, m + 1, d_cmax);
+          IPEPS_LAUNCH_CHECK();
+          c.series_terms++;
+          double cnext = 0;
+          IPEPS_CUDA(cudaMemcpyAsync(&cnext, d_cmax, 8, cudaMemcpyDeviceToHost, c.stream));
+          const double nt = std::sqrt(dot_host(c, Tu, Tu) + dot_host(c, Tv, Tv));
+          if (nt > 8.0 * ny0) {
+            blew_up = true;  // spectrum beyond b
+            break;
+          }
+          const double nx = std::sqrt(dot_host(c, Xu, Xu) + dot_host(c, Xv, Xv));
+          // |T_m| <= |T_0| on [0, b]: the remaining terms are bounded by the coefficient tail
+          if (cnext * ny0 <= kTol * nx) {
+            converged = true;
+            break;
+          }
+          Tensor Bu, Bv;
+          apply_B(Tu, Tv, &Bu, &Bv);
+          if (m > 0) {
+            // T_{m+1} = 2 B~ T_m - T_{m-1}
+            axpby_kernel<<<gridn(c, Bu.numel()), 256, 0, c.stream>>>(-1.0, Pu.f64(), 2.0, Bu.f64(), Bu.numel());
+            axpby_kernel<<<gridn(c, Bv.numel()), 256, 0, c.stream>>>(-1.0, Pv.f64(), 2.0, Bv.f64(), Bv.numel());
+            IPEPS_LAUNCH_CHECK();
+          }
+          Pu = Tu;
+          Pv = Tv;
+          Tu = Bu;
+          Tv = Bv;
+        }
+        if (converged && std::max(check(Xu, Yu0, true), check(Xv, Yv0, false)) <= kCheckTol) {
           series_done = true;
           break;
         }
-        Tensor Bu, Bv;
-        apply_B(Tu, Tv, &Bu, &Bv);
-        if (m > 0) {
-          // T_{m+1} = 2 B T_m - T_{m-1}
-          axpby_kernel<<<gridn(c, Bu.numel()), 256, 0, c.stream>>>(-1.0, Pu.f64(), 2.0, Bu.f64(), Bu.numel());
-          axpby_kernel<<<gridn(c, Bv.numel()), 256, 0, c.stream>>>(-1.0, Pv.f64(), 2.0, Bv.f64(), Bv.numel());
-          IPEPS_LAUNCH_CHECK();
-        }
-        Pu = Tu;
-        Pv = Tv;
-        Tu = Bu;
-        Tv = Bv;
+        if (!converged && !blew_up) break;  // term cap: counted below
+        // the spectrum reaches beyond b: widen the interval, still below s_n^2
+        c.series_retries++;
+        const double sn2w = sn2 > b ? sn2 : 2.0 * b;
+        b = (2.0 * b < sn2w) ? 2.0 * b : 0.5 * (b + sn2w);
       }
-      if (!blew_up) break;
     }
-    // the expansion stopped at its term cap: the discarded spectrum's share of
-    // the gradient is truncated (counted in ipeps_stats_t, bit 16 of the status word)
+    // the expansion stopped at its term cap or never passed its check: the
+    // discarded spectrum's share of the gradient is inexact (counted in
+    // ipeps_stats_t, bit 16 of the status word)
     if (!series_done) {
       c.series_cap_hits++;
       flag_status(c, 16);

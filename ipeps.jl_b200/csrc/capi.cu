@@ -139,6 +139,9 @@ int ipeps_stats(ipeps_ctx* ctx, ipeps_stats_t* out) {
     out->jacobi_sweeps = ctx->c->jacobi_sweeps;
     out->extra_passes = ctx->c->projector_extra_passes;
     out->series_cap_hits = ctx->c->series_cap_hits;
+    out->series_terms = ctx->c->series_terms;
+    out->series_retries = ctx->c->series_retries;
+    out->resid_misses = ctx->c->resid_misses;
     return IPEPS_OK;
   });
 }
@@ -152,6 +155,9 @@ int ipeps_stats_reset(ipeps_ctx* ctx) {
     ctx->c->jacobi_sweeps = 0;
     ctx->c->projector_extra_passes = 0;
     ctx->c->series_cap_hits = 0;
+    ctx->c->series_terms = 0;
+    ctx->c->series_retries = 0;
+    ctx->c->resid_misses = 0;
     return IPEPS_OK;
   });
 }

@@ -297,7 +297,11 @@ std::vector<double> move_pair(Env& e, int da, int db, ProjResult* ka, ProjResult
   c1.projector_calls += c2.projector_calls;
   c1.projector_extra_passes += c2.projector_extra_passes;
   c1.series_cap_hits += c2.series_cap_hits;
+  c1.series_terms += c2.series_terms;
+  c1.series_retries += c2.series_retries;
+  c1.resid_misses += c2.resid_misses;
   c2.jacobi_sweeps = c2.projector_calls = c2.projector_extra_passes = c2.series_cap_hits = 0;
+  c2.series_terms = c2.series_retries = c2.resid_misses = 0;
   for (auto& r : c2.prof_rec) c1.prof_rec.push_back(r);
   c2.prof_rec.clear();
   if (err_a) std::rethrow_exception(err_a);
@@ -559,7 +563,11 @@ void merge_stats(Ctx& to, Ctx& from) {
   to.projector_calls += from.projector_calls;
   to.projector_extra_passes += from.projector_extra_passes;
   to.series_cap_hits += from.series_cap_hits;
+  to.series_terms += from.series_terms;
+  to.series_retries += from.series_retries;
+  to.resid_misses += from.resid_misses;
   from.jacobi_sweeps = from.projector_calls = from.projector_extra_passes = from.series_cap_hits = 0;
+  from.series_terms = from.series_retries = from.resid_misses = 0;
   for (auto& r : from.prof_rec) to.prof_rec.push_back(r);
   from.prof_rec.clear();
 }

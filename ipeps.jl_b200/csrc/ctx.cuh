@@ -44,9 +44,16 @@ struct Ctx {
   uint64_t jacobi_sweeps = 0;
   uint64_t projector_calls = 0;
   uint64_t projector_extra_passes = 0;
-  // projector adjoints whose resolvent series stopped at its term cap before
-  // reaching the 1e-15 relative tolerance (the gradient may be inexact)
+  // projector adjoints whose resolvent expansion stopped at its term cap before
+  // reaching its tolerance (the gradient may be inexact)
   uint64_t series_cap_hits = 0;
+  // Chebyshev terms summed over all projector adjoints, and expansions redone
+  // over a wider interval after the resolvent check failed
+  uint64_t series_terms = 0;
+  uint64_t series_retries = 0;
+  // projectors whose kept triplets ended above the residual tolerance (the
+  // extra passes stopped converging or ran out)
+  uint64_t resid_misses = 0;
   // split-K partial sums live here (grown on demand, stream ordered)
   std::shared_ptr<DBuf> ws;
   // small device scalars (max-abs, traces, status words)

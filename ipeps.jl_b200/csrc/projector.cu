@@ -401,7 +401,6 @@ ProjResult projector_impl(Ctx& c, Ops& o, int chi, const SvdParams& sp, ProjCach
     Vk = c.alloc(dt, {N2, k});
     gemm(c, dt, 'N', 'N', N2, k, k, cplx(1), sk.Q2.data(), N2, Js.data(), k, cplx(0), Vk.data(), N2, true);
     if (q == 0 && k == Nmin) break;  // the sketch spans a whole side of M: exact
-    if (attempt >= sp.max_extra_passes) break;
     // residual of the kept triplets: ||M v_i - s_i u_i|| <= resid_tol * s_1
     Tensor Vc = c.alloc(dt, {N2, nc});
     copy_cols(c, Vc, Vk, N2, nc, w);
@@ -420,7 +419,11 @@ ProjResult projector_impl(Ctx& c, Ops& o, int chi, const SvdParams& sp, ProjCach
     // R1 (R2 v), ~eps ||R1|| ||R2||, can sit above resid_tol * s_1)
     const double rtol = (c.precision == kPrecMixed && dt == DType::F64) ? std::max(sp.resid_tol, sp.resid_tol_mixed)
                                                                          : sp.resid_tol;
-    if (res <= rtol * smax || res > 0.5 * prev_res) break;
+    if (res <= rtol * smax) break;
+    if (res > 0.5 * prev_res || attempt >= sp.max_extra_passes) {
+      c.resid_misses++;
+      break;
+    }
     prev_res = res;
     // not converged: one more power iteration from the current right vectors
     Om = Vk;

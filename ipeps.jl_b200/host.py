@@ -60,7 +60,8 @@ class CTensor(ct.Structure):
 class Stats(ct.Structure):
     _fields_ = [("launches", ct.c_uint64 * 8), ("flops", ct.c_double * 8), ("bytes", ct.c_double * 8),
                 ("moves", ct.c_uint64), ("move_seconds", ct.c_double), ("projector_calls", ct.c_uint64),
-                ("jacobi_sweeps", ct.c_uint64), ("extra_passes", ct.c_uint64), ("series_cap_hits", ct.c_uint64)]
+                ("jacobi_sweeps", ct.c_uint64), ("extra_passes", ct.c_uint64), ("series_cap_hits", ct.c_uint64),
+                ("series_terms", ct.c_uint64), ("series_retries", ct.c_uint64), ("resid_misses", ct.c_uint64)]
 
     FAMILIES = ["permute", "gemm_f64", "gemm_tf32x3", "reduce", "elementwise", "small_linalg", "jacobi"]
 
@@ -69,7 +70,9 @@ class Stats(ct.Structure):
                for i, n in enumerate(self.FAMILIES)}
         return {"families": fam, "moves": int(self.moves), "move_seconds": float(self.move_seconds),
                 "projector_calls": int(self.projector_calls), "jacobi_sweeps": int(self.jacobi_sweeps),
-                "extra_passes": int(self.extra_passes), "series_cap_hits": int(self.series_cap_hits)}
+                "extra_passes": int(self.extra_passes), "series_cap_hits": int(self.series_cap_hits),
+                "series_terms": int(self.series_terms), "series_retries": int(self.series_retries),
+                "resid_misses": int(self.resid_misses)}
 
 
 _lib = None

@@ -126,10 +126,29 @@ def test_tfim_chi30_last_spectrum(engines, pkg):
 
 
 # ------------------------------------------------------------------ Heisenberg D=4 chi=64
+def _oracle_pullback(A, H, CT, ad_iters):
+    """The oracle's run_gs pullback (optim_gs.jl:133-143) from the given C/T:
+    ad_iters CTMRG iterations and the energy, differentiated w.r.t. A."""
+    import torch
+    At = torch.tensor(A)
+    cfg = O.default_config()
+    cfg.update(chi=64, min_iter=ad_iters + 1, max_iter=ad_iters, rg_tol=0.0, ad_max_iter=ad_iters)
+    ts = O.make_ctm_tensors(At, cfg)
+    ts = ts.replace(Cs=[torch.tensor(np.asarray(C)) for C, _ in CT], Es=[torch.tensor(np.asarray(E)) for _, E in CT])
+    p = dict(ts.Params)
+    p["max_iter"] = ad_iters
+    ts = ts.replace(Params=p)
+    x = At.clone().requires_grad_(True)
+    y = O.run_gs(ts, [torch.tensor(h) for h in H], x)
+    (gx,) = torch.autograd.grad(y.real if torch.is_complex(y) else y, x)
+    return float((y.real if torch.is_complex(y) else y).item()), O.freshape(gx.detach(), -1).numpy()
+
+
 @pytest.fixture(scope="module")
 def d4_runs(engines, pkg):
     """30 iterations of the D=4 chi=64 workload in each form: energies, last
-    spectrum, E+grad, and the converged C/T (for finite differences)."""
+    spectrum, E+grad, the converged C/T (for finite differences), and the
+    oracle's E+grad from the same C/T."""
     g = _gold("config2")
     A = O.random_A(4, 2, seed=g["seed"]).numpy()
     H = [h.numpy() for h in O.heisenberg(1.0)]
@@ -143,27 +162,37 @@ def d4_runs(engines, pkg):
         E30, _ = pkg.get_gs_energy(ts, H)
         C = [ts.get_CT(k) for k in range(1, 5)]
         Ead, grad = pkg.energy_grad(ts, H)
+        Eo, go = _oracle_pullback(A, H, C, 4)
         out[form] = dict(traj=[l["obj"].real for l in info["log"]] + [E30.real], s=s, Ead=Ead,
-                         grad=grad.ravel(order="F"), C=C, cfg=cfg)
+                         grad=grad.ravel(order="F"), C=C, cfg=cfg, Eo=Eo, go=go)
         ts.close()
     return A, H, g, out
 
 
-# The D=4 chi=64 workload does not converge: after ~20 iterations it cycles
-# with period 2, so differences are carried along instead of damped.  The FP64
-# form keeps its bars; for the mixed form the FP32-level errors of its 26
-# mixed iterations are not removed by 4 FP64 ones in a cycle, and its errors
-# are checked at the level they settle at (energy 1e-6, singular values
-# 3e-5 relative or 1e-6 s_1 absolute, gradient 2e-2).  The FP64 singular
-# values are checked to 1e-12 s_1 absolute below their relative bar.
-D4_BARS = {"fp64": (1e-10, 1e-10, 1e-6, 1e-12, 1e-6), "mixed": (1e-6, 3e-5, 3e-5, 1e-6, 2e-2)}
+# The D=4 chi=64 workload does not converge: from ~iteration 20 it sits on a
+# period-2 cycle that is unstable, in the oracle as much as here.  Started from
+# this engine's 30-iteration environment (energy within 1e-13..5e-11 of the
+# oracle's), the oracle's own iterations 31..36 leave the cycle by a factor
+# ~3.5 per iteration (energy deviations 2.5e-11, 9.5e-11, 1.6e-10, 6e-10, 1e-9,
+# 3.7e-9 in one measured case); the fixture's trajectory stays on the cycle only
+# because its rounding is deterministic.  So the pullback (4 more iterations)
+# is checked against the oracle's pullback from the same environment, where
+# the E+grad unit itself is compared: energy 1e-12, gradient 1e-8 relative
+# (measured 7e-11), in both forms (the pullback runs in FP64 in both).  Against
+# the fixture's own pullback the energy agrees within 1e-8 and the gradient
+# within 1e-3 (measured up to 5e-9 and 3e-4 over repeated runs).
+# The mixed form's trajectory carries the FP32-level errors of its 26 mixed
+# iterations, which 4 FP64 ones in an unstable cycle do not remove: energy
+# 1e-6, singular values 3e-5 relative or 1e-6 s_1 absolute.  The FP64
+# singular values are checked to 1e-12 s_1 absolute below their relative bar.
+D4_BARS = {"fp64": (1e-10, 1e-10, 1e-6, 1e-12), "mixed": (1e-6, 3e-5, 3e-5, 1e-6)}
 
 
 @pytest.mark.parametrize("form", ["fp64", "mixed"])
 def test_heisenberg_d4_chi64_energy_spectrum_gradient(d4_runs, form):
     A, H, g, out = d4_runs
     r = out[form]
-    ebar, srel, sall, sabs, gbar = D4_BARS[form]
+    ebar, srel, sall, sabs = D4_BARS[form]
     traj = np.asarray(r["traj"])
     eo = np.asarray(g["energies"])
     # the mixed form runs its last iterations in FP64 (polish); compare the end of the run
@@ -175,10 +204,15 @@ def test_heisenberg_d4_chi64_energy_spectrum_gradient(d4_runs, form):
     assert np.allclose(r["s"][:16], so[:16], rtol=srel), np.abs(r["s"][:16] / so[:16] - 1).max()
     ds = np.abs(np.asarray(r["s"]) - so)
     assert np.all(ds <= sall * so + sabs * so[0]), ((ds / so).max(), ds.max() / so[0])
-    assert abs(r["Ead"] - g["E_ad"]) <= ebar, (r["Ead"], g["E_ad"])
+    # the E+grad unit against the oracle's from the same environment
+    assert abs(r["Ead"] - r["Eo"]) <= 1e-12, (r["Ead"], r["Eo"])
+    rel = np.linalg.norm(r["grad"] - r["go"]) / np.linalg.norm(r["go"])
+    assert rel <= 1e-8, rel
+    # and against the fixture's pullback, through the unstable cycle
     go = np.asarray(g["grad"])
-    rel = np.linalg.norm(r["grad"] - go) / np.linalg.norm(go)
-    assert rel <= gbar, rel
+    if form == "fp64":
+        assert abs(r["Ead"] - g["E_ad"]) <= 1e-8, (r["Ead"], g["E_ad"])
+        assert np.linalg.norm(r["grad"] - go) / np.linalg.norm(go) <= 1e-3
 
 
 def test_heisenberg_d4_chi64_finite_differences(engines, pkg, d4_runs):
