@@ -101,6 +101,13 @@ IPEPS_API int ipeps_projector(ipeps_ctx* ctx, const double* R1, const double* R2
 IPEPS_API int ipeps_projector_c(ipeps_ctx* ctx, const double* R1, const double* R2, int64_t N1, int64_t K1,
                       int64_t N2, int chi, double* P1, double* P2, double* s, int* n);
 
+/* ---- orthonormal basis of range(Y) for Y (N x k, column-major, real, N >= k): the
+ * projector's range-finder step (it stands in for the Q factor of the reference's full SVD,
+ * ctmrg.jl:257).  passes CholeskyQR passes, the first one shifted (passes = 3: sCholQR3):
+ * Q (N x k) with Q^T Q = I, and, when R is not NULL, R (k x k upper triangular, column-major)
+ * with Q R = Y. */
+IPEPS_API int ipeps_orth(ipeps_ctx* ctx, const double* Y, int64_t N, int k, int passes, double* Q, double* R);
+
 /* ---- environment state: CTMTensors (src/ctm/ctm_tensor.jl:3-18, ctors :57-69) */
 IPEPS_API int ipeps_env_create(ipeps_ctx* ctx, int D, int d, int chi, int is_complex, ipeps_env** out);
 IPEPS_API int ipeps_env_destroy(ipeps_env* env);

@@ -245,6 +245,19 @@ int ipeps_projector_c(ipeps_ctx* ctx, const double* R1, const double* R2, int64_
   });
 }
 
+int ipeps_orth(ipeps_ctx* ctx, const double* Y, int64_t N, int k, int passes, double* Q, double* R) {
+  return guarded(ctx, [&] {
+    IPEPS_CHECK(Y && Q && N > 0 && k > 0 && N >= k && passes >= 1, "bad orth arguments");
+    auto& c = *ctx->c;
+    Tensor y = upload(c, Y, DType::F64, {N, k});
+    Tensor r;
+    Tensor q = ipeps::orth(c, y, passes, R ? &r : nullptr);
+    download(c, Q, q);
+    if (R) download(c, R, r);
+    return IPEPS_OK;
+  });
+}
+
 int ipeps_env_create(ipeps_ctx* ctx, int D, int d, int chi, int is_complex, ipeps_env** out) {
   return guarded(ctx, [&] {
     IPEPS_CHECK(out && D > 0 && d > 0 && chi > 0, "bad env arguments");

@@ -3,8 +3,10 @@
 //   chol_blocked      G = R^T R in one CTA, 32-column panels: one warp factors the
 //                     diagonal block in registers, the block's rows of R are solved
 //                     column-parallel, the trailing update is a register-tiled SYRK.
-//   trsm_right_upper  Q = Y R^-1, one warp per row of Y across the whole GPU (the rows
-//                     are independent), R staged row-major in each CTA's shared memory.
+//   chol_ldl          the same for k <= 160 with the upper triangle in registers: one
+//                     barrier per elimination step.
+//   trsm_right_upper  Q = Y R^-1, two rows of Y per warp (the rows are independent), at
+//                     most one CTA per SM, R staged row-major in each CTA's shared memory.
 //   jacobi_svd_auto   one-sided Jacobi with only X in shared memory; every rotation is
 //                     logged, and J = product of the rotations is formed afterwards by a
 //                     row-parallel kernel (each row of J sees the same rotation sequence).
@@ -203,22 +205,168 @@ __global__ void __launch_bounds__(kCholThreads) chol_blocked_kernel(double* G, i
       for (int jj = lane; jj < k - i; jj += 32) Rrow[rowoff(i, k) + jj] = P[pku(i, i + jj)];
 }
 
-constexpr int kTrsmRows = 8;  // rows of Y per CTA, one warp each
+// Register-resident Cholesky for k <= 32 NBB (NBB <= 5), same contract as
+// chol_blocked_kernel.  The right-looking elimination is written as
+// G = U^T D U (U unit upper): step j subtracts a[j][r] a[j][c] / a[j][j] from
+// every a[r][c] with c >= r > j, and R = D^1/2 U at the end.  512 threads
+// hold the upper triangle in registers, thread (w, l) of warp w and lane l the
+// entries (w + 16 a, l + 32 b) (slots a <= 2b + 1 can reach the triangle), so a
+// step costs one barrier: the warp owning row j publishes the row and the row
+// divided by the pivot in shared memory (double-buffered by the parity of j),
+// and every thread updates its slots from two broadcast loads per row and
+// one load per column block.
+constexpr int kLdlThreads = 512;
+
+size_t chol_ldl_smem_doubles(int k) {
+  const size_t npk = (size_t(k) * (k + 1) / 2 + 1) & ~size_t(1);
+  return npk + 4 * 160 + 2 * 160 + 8;
+}
+
+template <int NBB>
+__global__ void __launch_bounds__(kLdlThreads, 1) chol_ldl_kernel(double* G, int k, int64_t ldg, double shift_factor,
+                                                                double* Rrow) {
+  constexpr int NBA = 2 * NBB, KP = 32 * NBB;
+  extern __shared__ __align__(16) double sm[];
+  const int npk = ((k * (k + 1)) / 2 + 1) & ~1;
+  double* P = sm;             // packed upper triangle, column by column
+  double* raw = P + npk;      // [2][KP]: row j of the eliminated matrix
+  double* scl = raw + 2 * KP; // [2][KP]: the same divided by the pivot (0 for a failed pivot)
+  double* dd = scl + 2 * KP;  // pivots (0: failed)
+  double* rs = dd + KP;       // 1 / sqrt(pivot), 0 for a failed pivot
+  __shared__ double s_red[kLdlThreads / 32];
+  __shared__ double s_tr;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+  {
+    const int kk2 = k * k;
+    for (int t0 = tid; t0 < kk2; t0 += 4 * kLdlThreads) {
+      double v[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int t = t0 + u * kLdlThreads, i = t % k, j = t / k;
+        v[u] = (t < kk2 && i <= j) ? G[i + int64_t(j) * ldg] : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int t = t0 + u * kLdlThreads, i = t % k, j = t / k;
+        if (t < kk2 && i <= j) P[pku(i, j)] = v[u];
+      }
+    }
+    for (int t = tid; t < 4 * KP; t += kLdlThreads) raw[t] = 0.0;  // raw and scl, rows >= k stay 0
+  }
+  __syncthreads();
+  double t = 0;
+  for (int i = tid; i < k; i += kLdlThreads) t += fabs(P[pku(i, i)]);
+  for (int o = 16; o; o >>= 1) t += __shfl_xor_sync(kFull, t, o);
+  if (lane == 0) s_red[warp] = t;
+  __syncthreads();
+  if (tid == 0) {
+    double s = 0;
+    for (int w = 0; w < kLdlThreads / 32; ++w) s += s_red[w];
+    s_tr = s;
+  }
+  __syncthreads();
+  const double shift = shift_factor > 0 ? shift_factor * s_tr : 0.0;
+  const double tiny = 1e-300 + 1e-32 * (s_tr + shift * k);
+
+  double v[NBA][NBB];
+#pragma unroll
+  for (int a = 0; a < NBA; ++a)
+#pragma unroll
+    for (int b = 0; b < NBB; ++b) {
+      if (a > 2 * b + 1) continue;
+      const int r = warp + 16 * a, c = lane + 32 * b;
+      double x = (r <= c && c < k) ? P[pku(r, c)] : 0.0;
+      if (r == c) x += shift;
+      v[a][b] = x;
+    }
+
+  for (int j = 0; j < k; ++j) {
+    const int p = j & 1;
+    double* rw = raw + p * KP;
+    double* sc = scl + p * KP;
+    if (warp == (j & 15)) {
+      // this warp holds row j: publish a[j][c] (c >= j), then a[j][c] / a[j][j]
+      const int aj = j >> 4;
+#pragma unroll
+      for (int a = 0; a < NBA; ++a) {
+        if (a != aj) continue;
+#pragma unroll
+        for (int b = 0; b < NBB; ++b) {
+          if (a > 2 * b + 1) continue;
+          const int c = lane + 32 * b;
+          if (c >= j && c < k) rw[c] = v[a][b];
+        }
+      }
+      __syncwarp();
+      const double d = rw[j];
+      const bool ok = d > tiny;
+      const double inv = ok ? __drcp_rn(d) : 0.0;
+#pragma unroll
+      for (int b = 0; b < NBB; ++b) {
+        const int c = lane + 32 * b;
+        if (c > j && c < k) sc[c] = rw[c] * inv;
+      }
+      if (lane == 0) dd[j] = ok ? d : 0.0;
+    }
+    __syncthreads();
+    // a[r][c] -= a[j][r] * (a[j][c] / a[j][j]) for r > j; slots left of the
+    // diagonal take garbage that is never read
+    double s[NBB];
+#pragma unroll
+    for (int b = 0; b < NBB; ++b) s[b] = (32 * b + 31 > j) ? sc[lane + 32 * b] : 0.0;
+#pragma unroll
+    for (int a = 0; a < NBA; ++a) {
+      const int r = warp + 16 * a;
+      if (r <= j) continue;
+      const double ra = rw[r];
+#pragma unroll
+      for (int b = 0; b < NBB; ++b) {
+        if (a > 2 * b + 1) continue;
+        v[a][b] = fma(-ra, s[b], v[a][b]);
+      }
+    }
+  }
+  for (int i = tid; i < k; i += kLdlThreads) rs[i] = dd[i] > 0.0 ? rsqrt(dd[i]) : 0.0;
+  __syncthreads();
+  // R = D^1/2 U into P; a failed pivot gives R[j][j] = 1 and row j zero
+#pragma unroll
+  for (int a = 0; a < NBA; ++a)
+#pragma unroll
+    for (int b = 0; b < NBB; ++b) {
+      if (a > 2 * b + 1) continue;
+      const int r = warp + 16 * a, c = lane + 32 * b;
+      if (r <= c && c < k) {
+        const double q = rs[r];
+        P[pku(r, c)] = (r == c) ? (q > 0.0 ? dd[r] * q : 1.0) : v[a][b] * q;
+      }
+    }
+  __syncthreads();
+  for (int j = warp; j < k; j += kLdlThreads / 32)
+    for (int i = lane; i < k; i += 32) G[i + int64_t(j) * ldg] = (i <= j) ? P[pku(i, j)] : 0.0;
+  if (Rrow)
+    for (int i = warp; i < k; i += kLdlThreads / 32)
+      for (int jj = lane; jj < k - i; jj += 32) Rrow[rowoff(i, k) + jj] = P[pku(i, i + jj)];
+}
 
 // Q = Y R^-1 for R (k x k) upper triangular: row y of Y solves x R = y by
-// forward substitution, x_j = (y_j - sum_{l<j} x_l R[l][j]) / R[j][j].
+// forward substitution, x_j = (y_j - sum_{l<j} x_l R[l][j]) / R[j][j].  Each
+// warp carries two rows at once (two independent substitution chains), a CTA
+// takes 2 x warps rows per pass over a grid of at most one CTA per SM, so R is
+// staged into shared memory once per SM rather than once per handful of rows.
+constexpr int kTrsmRPW = 2;  // rows per warp and pass
+
 template <int NS>
-__global__ void __launch_bounds__(kTrsmRows * 32) trsm_rows_kernel(const double* Y, int64_t ldy, int64_t N, int k,
-                                                                  const double* R, int64_t ldr, const double* Rrow,
-                                                                  double* Q, int64_t ldq) {
+__global__ void __launch_bounds__(512, 1) trsm_rows_kernel(const double* Y, int64_t ldy, int64_t N, int k,
+                                                           const double* R, int64_t ldr, const double* Rrow,
+                                                           double* Q, int64_t ldq) {
   extern __shared__ __align__(16) double sm[];
   const int kp = k | 1;
-  double* Rs = sm;                       // k(k+1)/2, row-major packed
-  double* rinv = Rs + (k * (k + 1)) / 2; // k
-  double* Yt = rinv + k;                 // kTrsmRows x kp
+  const int nthr = blockDim.x, nwarp = nthr >> 5, rows = nwarp * kTrsmRPW;
+  double* Rs = sm;                        // k(k+1)/2, row-major packed
+  double* rinv = Rs + (k * (k + 1)) / 2;  // k
+  double* Yt = rinv + k;                  // rows x kp
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  constexpr int nthr = kTrsmRows * 32;
-  const int64_t i0 = int64_t(blockIdx.x) * kTrsmRows;
   const int npk = (k * (k + 1)) / 2;
   if (Rrow) {
     // R already packed row by row: contiguous 16-byte copies (both bases are 16-byte aligned)
@@ -229,50 +377,74 @@ __global__ void __launch_bounds__(kTrsmRows * 32) trsm_rows_kernel(const double*
     __syncthreads();
     for (int j = tid; j < k; j += nthr) rinv[j] = 1.0 / Rs[rowoff(j, k)];
   } else {
-    for (int l = warp; l < k; l += kTrsmRows)
+    for (int l = warp; l < k; l += nwarp)
       for (int j = lane; j <= l; j += 32) Rs[rowoff(j, k) + (l - j)] = R[j + int64_t(l) * ldr];
     for (int j = tid; j < k; j += nthr) rinv[j] = 1.0 / R[j + int64_t(j) * ldr];
   }
-  for (int t = tid; t < kTrsmRows * k; t += nthr) {
-    const int r = t % kTrsmRows, l = t / kTrsmRows;
-    Yt[r * kp + l] = (i0 + r < N) ? Y[(i0 + r) + int64_t(l) * ldy] : 0.0;
-  }
-  __syncthreads();
-  double b[NS];
+  for (int64_t i0 = int64_t(blockIdx.x) * rows; i0 < N; i0 += int64_t(gridDim.x) * rows) {
+    __syncthreads();  // R staged; the previous pass's Yt written out
+    for (int t = tid; t < rows * k; t += nthr) {
+      const int r = t % rows, l = t / rows;
+      Yt[r * kp + l] = (i0 + r < N) ? Y[(i0 + r) + int64_t(l) * ldy] : 0.0;
+    }
+    __syncthreads();
+    double b0[NS], b1[NS];
+    const double* y0 = Yt + (kTrsmRPW * warp) * kp;
+    const double* y1 = y0 + kp;
 #pragma unroll
-  for (int s = 0; s < NS; ++s) {
-    const int l = 32 * s + lane;
-    b[s] = l < k ? Yt[warp * kp + l] : 0.0;
-  }
+    for (int s = 0; s < NS; ++s) {
+      const int l = 32 * s + lane;
+      b0[s] = l < k ? y0[l] : 0.0;
+      b1[s] = l < k ? y1[l] : 0.0;
+    }
 #pragma unroll
-  for (int s = 0; s < NS; ++s) {
-    for (int o = 0; o < 32; ++o) {
-      const int j = 32 * s + o;
-      if (j >= k) break;
-      const double xj = __shfl_sync(kFull, b[s], o) * rinv[j];
-      const double* rj = Rs + rowoff(j, k) - j;  // rj[l] = R[j][l], l >= j
+    for (int s = 0; s < NS; ++s) {
+#pragma unroll 8
+      for (int o = 0; o < 32; ++o) {
+        const int j = 32 * s + o;
+        if (j >= k) break;
+        const double rj_inv = rinv[j];
+        const double x0 = __shfl_sync(kFull, b0[s], o) * rj_inv;
+        const double x1 = __shfl_sync(kFull, b1[s], o) * rj_inv;
+        const double* rj = Rs + rowoff(j, k) - j;  // rj[l] = R[j][l], l >= j
 #pragma unroll
-      for (int t = 0; t < NS; ++t) {
-        if (t < s) continue;
-        const int l = 32 * t + lane;
-        if (l > j && l < k) b[t] = fma(-xj, rj[l], b[t]);
+        for (int t = 0; t < NS; ++t) {
+          if (t < s) continue;
+          const int l = 32 * t + lane;
+          if (l > j && l < k) {
+            const double rv = rj[l];
+            b0[t] = fma(-x0, rv, b0[t]);
+            b1[t] = fma(-x1, rv, b1[t]);
+          }
+        }
       }
     }
-  }
+    __syncthreads();  // every warp has read its rows of Yt
 #pragma unroll
-  for (int s = 0; s < NS; ++s) {
-    const int l = 32 * s + lane;
-    if (l < k) Yt[warp * kp + l] = b[s] * rinv[l];
-  }
-  __syncthreads();
-  for (int t = tid; t < kTrsmRows * k; t += nthr) {
-    const int r = t % kTrsmRows, l = t / kTrsmRows;
-    if (i0 + r < N) Q[(i0 + r) + int64_t(l) * ldq] = Yt[r * kp + l];
+    for (int s = 0; s < NS; ++s) {
+      const int l = 32 * s + lane;
+      if (l < k) {
+        Yt[(kTrsmRPW * warp) * kp + l] = b0[s] * rinv[l];
+        Yt[(kTrsmRPW * warp + 1) * kp + l] = b1[s] * rinv[l];
+      }
+    }
+    __syncthreads();
+    for (int t = tid; t < rows * k; t += nthr) {
+      const int r = t % rows, l = t / rows;
+      if (i0 + r < N) Q[(i0 + r) + int64_t(l) * ldq] = Yt[r * kp + l];
+    }
   }
 }
 
-size_t trsm_smem_bytes(int k) { return (size_t(k) * (k + 1) / 2 + size_t(k) + size_t(kTrsmRows) * (k | 1)) * 8; }
-
+size_t trsm_smem_bytes(int k, int warps) {
+  return (size_t(k) * (k + 1) / 2 + size_t(k) + size_t(kTrsmRPW) * warps * (k | 1)) * 8;
+}
+// warps per CTA: 16 when their rows fit next to R, else fewer (at least 4)
+int trsm_warps(int k) {
+  int w = 16;
+  while (w > 4 && trsm_smem_bytes(k, w) > kSmemMax) w /= 2;
+  return w;
+}
 
 // round-robin pair pi of round r over kk (even) slots; p < q, valid when both < k.
 // Both sums are below 2 (kk - 1), so one conditional subtraction replaces the modulo.
@@ -480,7 +652,14 @@ __global__ void __launch_bounds__(kApplyRows * 32) jacobi_apply_kernel(const dou
 }
 
 // shared-memory opt-in, once per kernel and device
-SmemAttrOnce g_chol_attr, g_trsm_attr[9], g_jlog_attr[11], g_apply_attr;
+SmemAttrOnce g_chol_attr, g_ldl_attr[6], g_trsm_attr[9], g_jlog_attr[11], g_apply_attr;
+
+template <int NBB>
+void launch_ldl(Ctx& c, double* G, int k, int64_t ldg, double shift_factor, double* Rrow) {
+  const size_t smem = chol_ldl_smem_doubles(k) * 8;
+  g_ldl_attr[NBB].ensure(chol_ldl_kernel<NBB>, int(kSmemMax));
+  chol_ldl_kernel<NBB><<<1, kLdlThreads, smem, c.stream>>>(G, k, ldg, shift_factor, Rrow);
+}
 
 template <int NV>
 void launch_jacobi(Ctx& c, double* X, int m, int k, int64_t ldx, double2* rot, int max_sweeps, double tol, double* S,
@@ -493,10 +672,12 @@ void launch_jacobi(Ctx& c, double* X, int m, int k, int64_t ldx, double2* rot, i
 template <int NS>
 void launch_trsm(Ctx& c, const double* Y, int64_t ldy, int64_t N, int k, const double* R, int64_t ldr,
                  const double* Rrow, double* Q, int64_t ldq) {
-  const size_t smem = trsm_smem_bytes(k);
+  const int warps = trsm_warps(k);
+  const size_t smem = trsm_smem_bytes(k, warps);
   g_trsm_attr[NS].ensure(trsm_rows_kernel<NS>, int(kSmemMax));
-  const unsigned grid = unsigned((N + kTrsmRows - 1) / kTrsmRows);
-  trsm_rows_kernel<NS><<<grid, kTrsmRows * 32, smem, c.stream>>>(Y, ldy, N, k, R, ldr, Rrow, Q, ldq);
+  const int64_t rows = int64_t(warps) * kTrsmRPW;
+  const unsigned grid = unsigned(std::min<int64_t>((N + rows - 1) / rows, std::max(c.sm_count, 1)));
+  trsm_rows_kernel<NS><<<grid, warps * 32, smem, c.stream>>>(Y, ldy, N, k, R, ldr, Rrow, Q, ldq);
   IPEPS_LAUNCH_CHECK();
 }
 
@@ -506,14 +687,24 @@ bool chol_fits(int k) { return k >= 1 && chol_smem_doubles(k) * 8 <= kSmemMax; }
 
 void chol_blocked(Ctx& c, double* G, int k, int64_t ldg, double shift_factor, double* Rrow) {
   IPEPS_CHECK(chol_fits(k), "chol_blocked: k too large for shared memory");
-  g_chol_attr.ensure(chol_blocked_kernel, int(kSmemMax));
   ProfScope ps(c, KFam::SmallLinalg);
-  chol_blocked_kernel<<<1, kCholThreads, chol_smem_doubles(k) * 8, c.stream>>>(G, k, ldg, shift_factor, Rrow);
+  if (k <= 160 && chol_ldl_smem_doubles(k) * 8 <= kSmemMax) {
+    switch ((k + 31) / 32) {
+      case 1: launch_ldl<1>(c, G, k, ldg, shift_factor, Rrow); break;
+      case 2: launch_ldl<2>(c, G, k, ldg, shift_factor, Rrow); break;
+      case 3: launch_ldl<3>(c, G, k, ldg, shift_factor, Rrow); break;
+      case 4: launch_ldl<4>(c, G, k, ldg, shift_factor, Rrow); break;
+      default: launch_ldl<5>(c, G, k, ldg, shift_factor, Rrow); break;
+    }
+  } else {
+    g_chol_attr.ensure(chol_blocked_kernel, int(kSmemMax));
+    chol_blocked_kernel<<<1, kCholThreads, chol_smem_doubles(k) * 8, c.stream>>>(G, k, ldg, shift_factor, Rrow);
+  }
   IPEPS_LAUNCH_CHECK();
   c.count(KFam::SmallLinalg, double(k) * k * k / 3.0);
 }
 
-bool trsm_fits(int k) { return k >= 1 && k <= 256 && trsm_smem_bytes(k) <= kSmemMax; }
+bool trsm_fits(int k) { return k >= 1 && k <= 256 && trsm_smem_bytes(k, trsm_warps(k)) <= kSmemMax; }
 
 void trsm_right_upper(Ctx& c, const double* Y, int64_t ldy, int64_t N, int k, const double* R, int64_t ldr, double* Q,
                       int64_t ldq, const double* Rrow) {

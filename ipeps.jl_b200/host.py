@@ -41,7 +41,7 @@ EXPORTED = [
     "ipeps_ctm_log", "ipeps_energy", "ipeps_gs_norm", "ipeps_nested_set_B", "ipeps_es_energy",
     "ipeps_all_norm", "ipeps_tcon", "ipeps_projector", "ipeps_projector_c", "ipeps_ctx_stream", "ipeps_prof_enable",
     "ipeps_prof_query", "ipeps_energy_grad", "ipeps_env_set_mixed", "ipeps_es_energy_grad",
-    "ipeps_single_dm_Ad", "ipeps_energy_4x4", "ipeps_ctm_run_4x4", "ipeps_energy_grad_4x4", "ipeps_es_energy_grad_4x4", "ipeps_gemm_f64", "ipeps_gemm_tf32x3", "ipeps_gemm_bf16", "ipeps_mlp_create", "ipeps_mlp_destroy", "ipeps_mlp_num_params",
+    "ipeps_single_dm_Ad", "ipeps_energy_4x4", "ipeps_ctm_run_4x4", "ipeps_energy_grad_4x4", "ipeps_es_energy_grad_4x4", "ipeps_gemm_f64", "ipeps_gemm_tf32x3", "ipeps_orth", "ipeps_gemm_bf16", "ipeps_mlp_create", "ipeps_mlp_destroy", "ipeps_mlp_num_params",
     "ipeps_mlp_get_params", "ipeps_mlp_set_params", "ipeps_mlp_forward", "ipeps_mlp_grad", "ipeps_mlp_train_step",
 ]
 
@@ -135,8 +135,7 @@ def load_library(path: str = LIB_PATH) -> ct.CDLL:
                            ct.c_int64, D, dp, ct.c_int64, I],
         "ipeps_gemm_tf32x3": [P, ct.c_char, ct.c_char, ct.c_int64, ct.c_int64, ct.c_int64, D, dp, ct.c_int64, dp,
                               ct.c_int64, D, dp, ct.c_int64, I, dp],
-        "ipeps_gemm_tf32x3": [P, ct.c_char, ct.c_char, ct.c_int64, ct.c_int64, ct.c_int64, D, dp, ct.c_int64, dp,
-                              ct.c_int64, D, dp, ct.c_int64, I, dp],
+        "ipeps_orth": [P, dp, ct.c_int64, I, I, dp, dp],
         "ipeps_gemm_bf16": [P, ct.c_char, ct.c_char, ct.c_int64, ct.c_int64, ct.c_int64, ct.c_float, fp,
                             ct.c_int64, fp, ct.c_int64, ct.c_float, fp, ct.c_int64],
         "ipeps_mlp_create": [P, I, I, I, I, U64, ct.POINTER(P)],
@@ -750,22 +749,16 @@ def gemm_f64(opA: str, opB: str, A, B, alpha: float = 1.0, beta: float = 0.0, C=
     return C
 
 
-def gemm_tf32x3(opA: str, opB: str, A, B, alpha: float = 1.0, beta: float = 0.0, C=None,
-                engine: Optional[Engine] = None, reps: int = 1, timing: bool = False):
-    """C = alpha op(A) op(B) + beta C on the engine's 3xTF32 tcgen05 GEMM; host
-    arrays.  With timing=True returns (C, device ms of one product)."""
+def orth(Y, passes: int = 3, engine: Optional[Engine] = None):
+    """Orthonormal basis of range(Y) by the projector's CholeskyQR (first pass
+    shifted; passes = 3 is sCholQR3): returns (Q, R) with Q^T Q = I, Q R = Y."""
     eng = engine or default_engine()
-    A = _fortran(A, np.float64)
-    B = _fortran(B, np.float64)
-    m = A.shape[0] if opA == "N" else A.shape[1]
-    k = A.shape[1] if opA == "N" else A.shape[0]
-    n = B.shape[1] if opB == "N" else B.shape[0]
-    C = np.zeros((m, n), order="F") if C is None else _fortran(C, np.float64).copy(order="F")
-    ms = np.zeros(1)
-    eng.check(eng.lib.ipeps_gemm_tf32x3(eng.h, opA.encode(), opB.encode(), m, n, k, float(alpha), _dp(A),
-                                        A.shape[0], _dp(B), B.shape[0], float(beta), _dp(C), C.shape[0], int(reps),
-                                        _dp(ms)))
-    return (C, float(ms[0])) if timing else C
+    Y = _fortran(Y, np.float64)
+    N, k = Y.shape
+    Q = np.empty((N, k), order="F")
+    R = np.empty((k, k), order="F")
+    eng.check(eng.lib.ipeps_orth(eng.h, _dp(Y), N, k, int(passes), _dp(Q), _dp(R)))
+    return Q, R
 
 
 def gemm_tf32x3(opA: str, opB: str, A, B, alpha: float = 1.0, beta: float = 0.0, C=None,
