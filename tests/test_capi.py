@@ -44,3 +44,17 @@ def test_missing_library_fails_loudly(tmp_path, pkg):
             host.load_library(str(tmp_path / "nope.so"))
         finally:
             host._lib = saved
+
+
+def test_package_exports_what_the_gpu_tests_call(pkg):
+    """Every ``pkg.<name>`` the GPU tests use exists on the package (checked
+    here, without a GPU, so a missing export does not first show on a B200)."""
+    import re
+    here = os.path.dirname(os.path.abspath(__file__))
+    names = set()
+    for f in os.listdir(here):
+        if f.endswith("_gpu.py") or f == "test_zz_no_alloc.py":
+            with open(os.path.join(here, f)) as fh:
+                names |= set(re.findall(r"\bpkg\.([A-Za-z_]\w*)", fh.read()))
+    missing = sorted(n for n in names if not hasattr(pkg, n))
+    assert not missing, missing
