@@ -5,7 +5,7 @@ register-resident Cholesky (k <= 160), the blocked Cholesky (larger k) and the
 row-parallel triangular solve directly, against numpy's QR:
 
 * Q^T Q = I to 1e-14 and Q R = Y to 1e-14 relative (sCholQR3 on a
-  well-conditioned Y; one and two passes on the same Y);
+  well-conditioned Y); one pass (shifted) orthogonal to 1e-6, two to 1e-14;
 * R equals numpy's R up to the signs of its rows, to 1e-12 relative (R has a
   positive diagonal);
 * ill-conditioned Y (singular values 1 .. 1e-12; the first pass is shifted):
@@ -31,9 +31,12 @@ def test_orth_matches_numpy_qr(engine, pkg, N, k):
     _, Rn = np.linalg.qr(Y)
     Rn = Rn * np.sign(np.diag(Rn))[:, None]
     assert np.linalg.norm(R - Rn) <= 1e-12 * np.linalg.norm(Rn)
-    for passes in (1, 2):
+    # one shifted pass is orthogonal only to the shift's level, ~11 (N k + k^2) u
+    # trace(G) / s_min(Y)^2 (a CPU restatement: 1e-11 at k = 5 .. 1e-7 at k = 160);
+    # the unshifted second pass restores the rounding level
+    for passes, bar in ((1, 1e-6), (2, 1e-14 * k ** 0.5)):
         Qp, Rp = pkg.orth(Y, passes, engine=engine)
-        assert np.abs(Qp.T @ Qp - np.eye(k)).max() <= 1e-12
+        assert np.abs(Qp.T @ Qp - np.eye(k)).max() <= bar, passes
         assert np.linalg.norm(Qp @ Rp - Y) <= 1e-13 * np.linalg.norm(Y)
 
 
