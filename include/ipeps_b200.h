@@ -215,6 +215,15 @@ IPEPS_API int ipeps_energy_grad_4x4(ipeps_env* env, const ipeps_ctensor_t* H4, i
                                     double* dA);
 /* Pullback of run_es_h4 w.r.t. B (get_es_grad_h4, optim_es_h4.jl:133-168): as
  * ipeps_es_energy_grad with the plaquette energy; E = real(get_es_energy_4x4). */
+/* The unit of optim_wp (get_wp_grad / run_wp, optim_wp.jl:195-238): in the environment held
+ * by env (no CTMRG), the plaquette operator given as the MPO wp4 = [s1, s2, s3, s4] of
+ * get_local_h and the norm of the 2x2 cluster whose site `site` (Params["wp"], 1..4) holds
+ * B (ComplexF64, the shape of A) and the others A (energy_norm_4x4, evaluation.jl:435-441).
+ * wp_norm[4] = (re, im) of the operator value, then of the norm; gH, gN (ComplexF64, the
+ * shape of A): the gradients of their real parts w.r.t. B (Zygote's back((1, nothing)) and
+ * back((nothing, 1))). */
+IPEPS_API int ipeps_wp_grad(ipeps_env* env, const ipeps_ctensor_t* wp4, int site, const double* B, double* wp_norm,
+                            double* gH, double* gN);
 IPEPS_API int ipeps_es_energy_grad_4x4(ipeps_env* env, const ipeps_ctensor_t* H4, int ad_iters, double* E,
                                        double* gB);
 

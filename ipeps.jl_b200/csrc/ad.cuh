@@ -79,4 +79,15 @@ double energy_grad(Env& e, const Tensor& Hh, const Tensor& Hv, int ad_iters, Ten
 double es_energy_grad(Env& e, const Tensor& Hh, const Tensor& Hv, int ad_iters, Tensor* gB,
                       const std::array<Tensor, 4>* h4 = nullptr);
 
+// The unit of optim_wp (get_wp_grad / run_wp, optim_wp.jl:195-238): in the
+// environment held by e (no CTMRG iterations), the plaquette operator given
+// as the MPO wp = [s1, s2, s3, s4] (get_local_h) and the norm of the 2x2
+// cluster whose site `site` (1..4, Params["wp"]) holds B and the other three
+// A (energy_norm_4x4, evaluation.jl:435-441).  Returns both values and their
+// gradients w.r.t. B, gH of the real part of the operator value and gN of the
+// real part of the norm (Zygote's back((1, nothing)) / back((nothing, 1)):
+// dRe/dRe(B) + i dRe/dIm(B)); complex.
+void wp_grad(Env& e, const std::array<Tensor, 4>& wp, int site, const Tensor& B, std::complex<double>* wp_value,
+             std::complex<double>* norm, Tensor* gH, Tensor* gN);
+
 }  // namespace ipeps

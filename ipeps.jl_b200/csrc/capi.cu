@@ -647,6 +647,29 @@ extern "C" int ipeps_es_energy_grad_4x4(ipeps_env* env, const ipeps_ctensor_t* H
   });
 }
 
+extern "C" int ipeps_wp_grad(ipeps_env* env, const ipeps_ctensor_t* wp4, int site, const double* B,
+                             double* wp_norm, double* gH, double* gN) {
+  if (!env) return IPEPS_EINVAL;
+  return guarded(env->owner, [&] {
+    IPEPS_CHECK(B && site >= 1 && site <= 4, "ipeps_wp_grad: B and site 1..4 required");
+    auto& c = *env->e.ctx;
+    ipeps::H4 h = upload_H4(c, wp4);
+    Tensor b = upload(c, B, DType::C128, env->e.A.shape());
+    std::complex<double> w, n;
+    Tensor gh, gn;
+    ipeps::wp_grad(env->e, h, site, b, &w, &n, &gh, &gn);
+    if (wp_norm) {
+      wp_norm[0] = w.real();
+      wp_norm[1] = w.imag();
+      wp_norm[2] = n.real();
+      wp_norm[3] = n.imag();
+    }
+    if (gH) download(c, gH, gh);
+    if (gN) download(c, gN, gn);
+    return IPEPS_OK;
+  });
+}
+
 extern "C" int ipeps_single_dm_Ad(ipeps_env* env, double* out) {
   if (!env) return IPEPS_EINVAL;
   return guarded(env->owner, [&] {

@@ -379,4 +379,56 @@ double es_energy_grad(Env& e, const Tensor& Hh, const Tensor& Hv, int ad_iters, 
   return Eres;
 }
 
+void wp_grad(Env& e, const std::array<Tensor, 4>& wp, int site, const Tensor& B, std::complex<double>* wp_value,
+             std::complex<double>* norm, Tensor* gH, Tensor* gN) {
+  Ctx& c = *e.ctx;
+  IPEPS_CHECK(site >= 1 && site <= 4, "wp_grad: site must be 1..4");
+  IPEPS_CHECK(B.shape() == e.A.shape(), "wp_grad: B must have the shape of A");
+  Fp64Scope fp64(c);
+  auto cx = [&](const Tensor& t) { return t.dt == DType::C128 ? t : to_complex(c, t); };
+  const Tensor Ac = cx(e.A), Adc = conj(c, Ac), Bc = cx(B), Bdc = conj(c, Bc);
+  std::array<Tensor, 4> Cc, Ec, sc;
+  for (int k = 0; k < 4; ++k) {
+    Cc[k] = cx(e.Cs[k]);
+    Ec[k] = cx(e.Es[k]);
+    sc[k] = cx(wp[k]);
+  }
+  // one tape per seed: the operator value (gH), then the norm (gN)
+  for (int pass = 0; pass < 2; ++pass) {
+    Tape tp(c);
+    ADPolicy p{tp};
+    AV Bl = tp.leaf(Bc), Bdl = tp.leaf(Bdc);
+    Arr4<ADPolicy> As, Ads, sv;
+    for (int k = 0; k < 4; ++k) {
+      As[k] = tp.constant(Ac);
+      Ads[k] = tp.constant(Adc);
+      sv[k] = tp.constant(sc[k]);
+    }
+    As[site - 1] = Bl;
+    Ads[site - 1] = Bdl;
+    AV C[4], E[4];
+    for (int k = 0; k < 4; ++k) {
+      C[k] = tp.constant(Cc[k]);
+      E[k] = tp.constant(Ec[k]);
+    }
+    Arr4<ADPolicy> op = get_op_Ad4(p, sv, Ads);
+    auto en = energy_norm_4x4(p, C[0], C[1], C[2], C[3], E[0], E[0], E[1], E[1], E[2], E[2], E[3], E[3], As, Ads, op);
+    if (pass == 0) {
+      if (wp_value) *wp_value = host_scalar(c, en[0].t);
+      if (norm) *norm = host_scalar(c, en[1].t);
+    }
+    // L = Re(y): the cotangent of y is 1
+    Tensor sd = c.alloc(DType::C128, en[pass].t.shape());
+    const double one[2] = {1.0, 0.0};
+    IPEPS_CUDA(cudaMemcpyAsync(sd.data(), one, 16, cudaMemcpyHostToDevice, c.stream));
+    c.sync();
+    tp.acc(en[pass].id, as_dtype(c, sd, en[pass].t.dt));
+    tp.backward();
+    // B enters as B and conj(B): the gradient is g_B + conj(g_Bd)
+    Tensor g = tp.grad(Bl.id).empty() ? c.zeros(DType::C128, B.shape()) : clone(c, cx(tp.grad(Bl.id)));
+    if (!tp.grad(Bdl.id).empty()) axpy(c, cplx(1), conj(c, cx(tp.grad(Bdl.id))), g);
+    (pass == 0 ? *gH : *gN) = g;
+  }
+}
+
 }  // namespace ipeps

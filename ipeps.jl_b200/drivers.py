@@ -396,6 +396,87 @@ def shard_indices(n: int, rank: int, world: int) -> List[int]:
     return list(range(rank, n, world))
 
 
+# ---------------------------------------------------------------- optim_wp
+_SIGX = np.array([[0, 1], [1, 0]], dtype=np.complex128)
+_SIGY = np.array([[0, -1j], [1j, 0]], dtype=np.complex128)
+_SIGZ = np.array([[1, 0], [0, -1]], dtype=np.complex128)
+_SI = np.eye(2, dtype=np.complex128)
+
+
+def tout(a: np.ndarray, b: np.ndarray) -> np.ndarray:
+    """tout (basis.jl:16-21): c[i,k,j,l] = a[i,j] b[k,l] reshaped to (d1 d2, d3 d4)."""
+    c = np.einsum("ij,kl->ikjl", a, b)
+    s = c.shape
+    return c.reshape(s[0] * s[1], s[2] * s[3], order="F")
+
+
+def get_w_op() -> np.ndarray:
+    """get_w_op (honeycomb.jl:82-101): the XX plaquette operator of the
+    honeycomb model, shape (d^2, d^2, d^2, d^2) with d = 4."""
+    Ix, yz = tout(_SI, _SIGX), tout(_SIGY, _SIGZ)
+    xI, zy = tout(_SIGX, _SI), tout(_SIGZ, _SIGY)
+    wp = tout_site(tout_site(Ix, yz), tout_site(xI, zy))
+    return wp.reshape(16, 16, 16, 16, order="F")
+
+
+def optim_wp(ts: host.CTMTensors, wp_op: np.ndarray, basis: np.ndarray, site: Optional[int] = None,
+             es_resume: int = 1, es_num: int = 0, effH: Optional[np.ndarray] = None,
+             effN: Optional[np.ndarray] = None):
+    """optim_wp (optim_wp.jl:133-193) in the fixed environment held by ts (the
+    reference loads ts and the basis from basis.jld2): for every basis vector,
+    get_wp_grad at plaquette site ``site`` (Params["wp"], default 1) on the
+    device, effH[:, i] = basis' gH / 2, effN[:, i] = basis' gN / 2.  As the
+    reference: vectors before es_resume (1-based) are skipped, and with
+    es_num > 0 the loop stops after es_num vectors; effH/effN of an earlier
+    partial run can be passed in to continue it.  Returns (effH, effN)."""
+    basis = np.asarray(basis, dtype=np.complex128)
+    nb = basis.shape[1]
+    effH = np.zeros((nb, nb), dtype=np.complex128) if effH is None else np.array(effH, dtype=np.complex128)
+    effN = np.zeros((nb, nb), dtype=np.complex128) if effN is None else np.array(effN, dtype=np.complex128)
+    wp4 = get_local_h(wp_op)
+    bh = basis.conj().T
+    for i in range(1, nb + 1):
+        if i < es_resume:
+            continue
+        if es_num > 0 and i >= es_resume + es_num:
+            break
+        gH, gN, _, _ = host.get_wp_grad(ts, wp4, basis[:, i - 1], site)
+        effH[:, i - 1] = bh @ gH / 2
+        effN[:, i - 1] = bh @ gN / 2
+    return effH, effN
+
+
+def _eig_sorted(H2, N2):
+    import scipy.linalg as sl
+    es, vecs = sl.eig(H2, N2)
+    ix = np.argsort(es.real, kind="stable")
+    return es[ix], vecs[:, ix]
+
+
+def get_wp_basis(effH: np.ndarray, effN: np.ndarray, basis: np.ndarray):
+    """get_wp_basis (optim_wp.jl:25-72): effH, effN hermitised, the metric
+    diagonalised (eigenvalues descending), eigen(H2, N2) in that frame, and the
+    basis split by the sign of the eigenvalues.  Returns (es, basis_p,
+    basis_m): the new bases basis P vecs of the positive and negative sectors
+    (the reference saves them as <basis>_<wp>p.jld2 and _<wp>m.jld2)."""
+    H = (effH + effH.conj().T) / 2
+    N = (effN + effN.conj().T) / 2
+    ev, P = np.linalg.eigh(N)
+    P = P[:, np.argsort(ev)[::-1]]
+    N2 = P.conj().T @ N @ P
+    H2 = P.conj().T @ H @ P
+    es, vecs = _eig_sorted((H2 + H2.conj().T) / 2, (N2 + N2.conj().T) / 2)
+    exci = np.asarray(basis, dtype=np.complex128) @ P @ vecs
+    return es, exci[:, es.real > 0.0], exci[:, es.real < 0.0]
+
+
+def evaluate_wp(effH: np.ndarray, effN: np.ndarray, nrmB_cut=1e-3):
+    """evaluate_wp (optim_wp.jl:86-119): as compute_es, the generalised
+    eigenproblem on the metric's leading subspace (nrmB_cut relative, or an
+    integer count).  Returns (es, vecs, P)."""
+    return compute_es(effH, effN, nrmB_cut)
+
+
 def optim_es_sharded(px: float, py: float, ts: Optional[host.CTMTensors], H, basis: np.ndarray, group=None,
                      column_fn=None):
     """optim_es over the ranks of a torch.distributed job (one process per GPU).

@@ -41,7 +41,7 @@ EXPORTED = [
     "ipeps_ctm_log", "ipeps_energy", "ipeps_gs_norm", "ipeps_nested_set_B", "ipeps_es_energy",
     "ipeps_all_norm", "ipeps_tcon", "ipeps_projector", "ipeps_projector_c", "ipeps_ctx_stream", "ipeps_prof_enable",
     "ipeps_prof_query", "ipeps_energy_grad", "ipeps_env_set_mixed", "ipeps_es_energy_grad",
-    "ipeps_single_dm_Ad", "ipeps_energy_4x4", "ipeps_ctm_run_4x4", "ipeps_energy_grad_4x4", "ipeps_es_energy_grad_4x4", "ipeps_gemm_f64", "ipeps_gemm_tf32x3", "ipeps_orth", "ipeps_gemm_bf16", "ipeps_mlp_create", "ipeps_mlp_destroy", "ipeps_mlp_num_params",
+    "ipeps_single_dm_Ad", "ipeps_wp_grad", "ipeps_energy_4x4", "ipeps_ctm_run_4x4", "ipeps_energy_grad_4x4", "ipeps_es_energy_grad_4x4", "ipeps_gemm_f64", "ipeps_gemm_tf32x3", "ipeps_orth", "ipeps_gemm_bf16", "ipeps_mlp_create", "ipeps_mlp_destroy", "ipeps_mlp_num_params",
     "ipeps_mlp_get_params", "ipeps_mlp_set_params", "ipeps_mlp_forward", "ipeps_mlp_grad", "ipeps_mlp_train_step",
 ]
 
@@ -130,6 +130,7 @@ def load_library(path: str = LIB_PATH) -> ct.CDLL:
         "ipeps_ctm_run_4x4": [P, ct.POINTER(CTensor), I, ip, dp, ip],
         "ipeps_energy_grad_4x4": [P, ct.POINTER(CTensor), I, dp, dp],
         "ipeps_es_energy_grad_4x4": [P, ct.POINTER(CTensor), I, dp, dp],
+        "ipeps_wp_grad": [P, ct.POINTER(CTensor), I, dp, dp, dp, dp],
         "ipeps_single_dm_Ad": [P, dp],
         "ipeps_gemm_f64": [P, ct.c_char, ct.c_char, ct.c_int64, ct.c_int64, ct.c_int64, D, dp, ct.c_int64, dp,
                            ct.c_int64, D, dp, ct.c_int64, I],
@@ -585,6 +586,22 @@ def get_es_grad_h4(ts: CTMTensors, H4, Bi):
     E, gH = es_energy_grad_4x4(ts, H4)
     Nb, gN = get_all_norm(ts)
     return gH.reshape(-1, order="F"), gN.reshape(-1, order="F")
+
+
+def get_wp_grad(ts: CTMTensors, wp4, Bi, site: Optional[int] = None):
+    """get_wp_grad (optim_wp.jl:195-220) on the device, in the environment held
+    by ts (no CTMRG): the basis tensor Bi at plaquette site ``site`` (default
+    ts.Params["wp"], else 1), the plaquette operator as the MPO wp4 = [s1, s2,
+    s3, s4] (get_local_h of the operator).  Returns (gH, gN) flat complex
+    (column-major) and the operator value and norm (run_wp, :222-238)."""
+    site = int(ts.Params.get("wp", 1) if site is None else site)
+    h = _H4(wp4)
+    B = np.asarray(Bi, dtype=np.complex128).reshape(ts.A.shape, order="F").copy(order="F")
+    out = np.zeros(4)
+    gH = np.empty(ts.A.shape, dtype=np.complex128, order="F")
+    gN = np.empty(ts.A.shape, dtype=np.complex128, order="F")
+    ts.engine.check(ts.lib.ipeps_wp_grad(ts.h, h.c, site, _dp(B), _dp(out), _dp(gH), _dp(gN)))
+    return gH.reshape(-1, order="F"), gN.reshape(-1, order="F"), complex(out[0], out[1]), complex(out[2], out[3])
 
 
 def _run_info(ts, iters, diff, conv):

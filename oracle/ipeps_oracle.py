@@ -28,6 +28,7 @@ import math
 from dataclasses import dataclass, field
 from typing import Any, Dict, List, Optional
 
+import numpy as np
 import torch
 
 _F64 = torch.float64
@@ -847,6 +848,108 @@ def get_es_grad_h4(ts, H, Bi):
     with torch.no_grad():
         Nb, gN = get_all_norm(_detach_ts(ts2))
     return freshape(gH.detach(), -1), freshape(gN.detach(), -1)
+
+
+def tout_site(a, b):
+    """honeycomb.jl:37-42: c[i,j,k,l] = a[i,j] b[k,l], reshaped to (d1 d2, d3 d4)."""
+    a, b = _promote(a, b)
+    c = tcon([a, b], [[-1, -2], [-3, -4]])
+    s = c.shape
+    return freshape(c, s[0] * s[1], s[2] * s[3])
+
+
+def get_w_op():
+    """honeycomb.jl:82-101 (the XX plaquette operator): (d^2, d^2, d^2, d^2), d = 4."""
+    Ix, yz = tout(sI, sigmax), tout(sigmay, sigmaz)
+    xI, zy = tout(sigmax, sI), tout(sigmaz, sigmay)
+    wp = tout_site(tout_site(Ix, yz), tout_site(xI, zy))
+    d = 4
+    return freshape(wp, d * d, d * d, d * d, d * d)
+
+
+def get_local_h(h):
+    """local_h.jl:1-31: the plaquette operator h (d^2, d^2, d^2, d^2) as the MPO
+    [s1, s2, s3, s4] by successive truncated SVDs (wrap_svd)."""
+    h = h.to(_C128)
+    dims = tuple(h.shape)
+    d = int(round(math.sqrt(dims[0])))
+    sl = []
+    u, s, v = wrap_svd(freshape(h, dims[0], -1))
+    sl.append(freshape(u * torch.sqrt(s).to(u.dtype), d, d, -1))
+    sdots = torch.sqrt(s).to(v.dtype)[:, None] * v.mH
+    for i in range(len(dims) - 2):
+        dl = sdots.shape[0]
+        sdots = freshape(sdots, dl * dims[i], -1)
+        u, s, v = wrap_svd(sdots)
+        sl.append(freshape(u * torch.sqrt(s).to(u.dtype), dl, d, d, -1))
+        sdots = torch.sqrt(s).to(v.dtype)[:, None] * v.mH
+    sl.append(freshape(sdots, sdots.shape[0], d, d))
+    return sl
+
+
+def run_wp(ts, wp, A1, A2, A3, A4):
+    """optim_wp.jl:222-238: the plaquette operator and the norm of the 2x2
+    cluster with its four sites A1..A4 (one of them the basis tensor B) in the
+    fixed environment of ts (energy_norm_4x4, evaluation.jl:435-441)."""
+    C1, C2, C3, C4 = ts.Cs
+    E1, E2, E3, E4 = ts.Es
+    s1, s2, s3, s4 = wp
+    Ad = [conj(a) for a in (A1, A2, A3, A4)]
+    ops = get_op_Ad4(s1, s2, s3, s4, *Ad)
+    return energy_norm_4x4(C1, C2, C3, C4, E1, E1, E2, E2, E3, E3, E4, E4, A1, A2, A3, A4, *Ad, *ops)
+
+
+def get_wp_grad(ts, wp_op, Bi, site=1):
+    """optim_wp.jl:195-220: (gH, gN) of the plaquette operator and of the norm
+    w.r.t. the basis tensor B placed at plaquette site ``site`` (Params["wp"]),
+    as flat complex vectors (column-major).  Zygote's back((1, nothing)) of the
+    complex pair is the gradient of the real part (dL/dRe + i dL/dIm), which is
+    what torch returns for a real scalar."""
+    A = ts.A.to(_C128)
+    B = freshape(Bi.to(_C128), *A.shape).detach().clone().requires_grad_(True)
+    wp = get_local_h(wp_op)
+    Cs = [c.to(_C128) for c in ts.Cs]
+    Es = [e.to(_C128) for e in ts.Es]
+    t = ts.replace(Cs=Cs, Es=Es)
+    sites = [A, A, A, A]
+    sites[site - 1] = B
+    e, n = run_wp(t, wp, *sites)
+    (gH,) = torch.autograd.grad(e.real, B, retain_graph=True)
+    (gN,) = torch.autograd.grad(n.real, B)
+    return freshape(gH.detach(), -1), freshape(gN.detach(), -1), complex(e.detach()), complex(n.detach())
+
+
+def optim_wp_columns(ts, wp_op, basis, cols, site=1):
+    """The effH, effN columns of optim_wp (optim_wp.jl:164-166):
+    effH[:, i] = basis' gH / 2, effN[:, i] = basis' gN / 2."""
+    basis = basis.to(_C128)
+    out = []
+    for i in cols:
+        gH, gN, _, _ = get_wp_grad(ts, wp_op, basis[:, i], site)
+        out.append((basis.mH @ gH / 2, basis.mH @ gN / 2))
+    return out
+
+
+def get_wp_basis(effH, effN, basis):
+    """optim_wp.jl:25-72: diagonalise the (hermitised) effH in the metric effN
+    and split the basis into the positive- and negative-eigenvalue sectors
+    (new basis = basis P vecs).  Returns (es, basis_p, basis_m)."""
+    H = (effH + effH.mH) / 2
+    N = (effN + effN.mH) / 2
+    ev_N, P = torch.linalg.eigh(N)
+    idx = torch.argsort(ev_N, descending=True)
+    P = P[:, idx]
+    N2 = P.mH @ N @ P
+    H2 = P.mH @ H @ P
+    H2 = (H2 + H2.mH) / 2
+    N2 = (N2 + N2.mH) / 2
+    # eigen(H2, N2) on plain matrices: the generalised (QZ) problem, as LAPACK ggev
+    import scipy.linalg as sla
+    es, vecs = sla.eig(H2.numpy(), N2.numpy())
+    ixs = np.argsort(es.real, kind="stable")
+    es, vecs = es[ixs], vecs[:, ixs]
+    exci = basis.to(_C128).numpy() @ P.numpy() @ vecs
+    return es, exci[:, es.real > 0.0], exci[:, es.real < 0.0]
 
 
 def correlation_TM(ts, direction="h", N=10):

@@ -94,3 +94,45 @@ def test_jld2_reader_matches_committed_pins(pkg):
     assert np.array_equal(e["effN"], p["effN_1_1"])
     # effN is Hermitian up to the columns' separate CTMRG convergence (rg_tol 1e-6)
     assert np.abs(e["effN"] - e["effN"].conj().T).max() <= 1e-6 * np.abs(e["effN"]).max()
+
+
+def wp_ts(p):
+    T = torch.tensor
+    return O.CTMTensors(A=T(p["wp_A"]), Ad=T(p["wp_A"].conj()), Cs=[T(p[f"wp_C{k}"]) for k in range(1, 5)],
+                        Es=[T(p[f"wp_E{k}"]) for k in range(1, 5)], Params=dict(O.default_config()))
+
+
+@pytest.mark.parametrize("site,basis_key,effH_key,effN_key,cols", [
+    (1, "wp_basis", "wp_effH", "wp_effN", [0, 31, 62]),
+    (2, "wp_basis_1m", "wp2_effH_1_10", "wp2_effN_1_10", [0, 9]),
+])
+def test_oracle_reproduces_reference_optim_wp(site, basis_key, effH_key, effN_key, cols):
+    """optim_wp (optim_wp.jl:133-193, get_wp_grad :195-220) with the honeycomb
+    XX plaquette operator (get_w_op, honeycomb.jl:82-101) in the saved
+    environment: the effH and effN columns the reference saved (wp/HN.jld2 at
+    site 1, wp/HN_1m/1_10.jld2 at site 2 on the basis_1m sector), 1e-12 relative
+    (measured ~1e-15)."""
+    p = pins()
+    ts = wp_ts(p)
+    basis = torch.tensor(p[basis_key])
+    out = O.optim_wp_columns(ts, O.get_w_op(), basis, cols, site=site)
+    for (h, n), i in zip(out, cols):
+        eh, en = p[effH_key][:, i], p[effN_key][:, i]
+        assert np.linalg.norm(h.numpy() - eh) <= 1e-12 * np.linalg.norm(eh), (i, "effH")
+        assert np.linalg.norm(n.numpy() - en) <= 1e-12 * np.linalg.norm(en), (i, "effN")
+
+
+def _range_projector(X):
+    Q, _ = np.linalg.qr(X)
+    return Q @ Q.conj().T
+
+
+def test_oracle_get_wp_basis_reproduces_reference_sectors():
+    """get_wp_basis (optim_wp.jl:25-72) on the saved effH/effN: the positive and
+    negative sectors span the reference's basis_1p and basis_1m (projectors
+    within 1e-10; the eigenvectors themselves are defined up to normalisation)."""
+    p = pins()
+    es, bp, bm = O.get_wp_basis(torch.tensor(p["wp_effH"]), torch.tensor(p["wp_effN"]), torch.tensor(p["wp_basis"]))
+    assert bp.shape == p["wp_basis_1p"].shape and bm.shape == p["wp_basis_1m"].shape
+    assert np.linalg.norm(_range_projector(bp) - _range_projector(p["wp_basis_1p"])) <= 1e-10
+    assert np.linalg.norm(_range_projector(bm) - _range_projector(p["wp_basis_1m"])) <= 1e-10
