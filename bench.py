@@ -578,6 +578,76 @@ def run_gemm_shapes():
     return 0
 
 
+def run_pullback_profile(args):
+    """The E+grad pullback alone (energy_grad: ad_iters checkpointed iterations
+    from a converged environment, the energy on a tape, the backward with the
+    projector adjoints) of the workload, in one precision form: converge once,
+    one warm-up pullback, then one pullback bracketed by cudaProfilerStart /
+    cudaProfilerStop (ncu --profile-from-start off captures only it), timed by
+    CUDA events, with the per-family device profile of a second one and the
+    projector/adjoint counters.  Also times the checkpoint iterations alone
+    (ad_iters CTMRG steps at the pullback's residual tolerance)."""
+    import torch
+    pkg = load_pkg()
+    form = "fp64" if args.precision == "both" else args.precision
+    D, d, chi, iters, ad_iters = (WORKLOAD[k] for k in ("D", "d", "chi", "iters", "ad_iters"))
+    cfg = workload_cfg(pkg, chi, iters, ad_iters)
+    H = heisenberg(1.0)
+    A = random_A(D, d, seed=1000)
+    eng = pkg.Engine(0, precision=form)
+    ext = torch.cuda.ExternalStream(eng.stream_ptr())
+    ts = pkg.CTMTensors(A, cfg, engine=eng)
+    pkg.run_ctm(ts, conv_fun="energy", H=H)
+    C = [ts.get_CT(k) for k in range(1, 5)]
+    ts.close()
+
+    def fresh():
+        t = pkg.CTMTensors(A, cfg, engine=eng, init=False)
+        for k in range(4):
+            t.set_CT(k + 1, *C[k])
+        return t
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(ext)
+        fn()
+        e.record(ext)
+        e.synchronize()
+        return s.elapsed_time(e)
+
+    t = fresh()
+    pkg.energy_grad(t, H, ad_iters)
+    t.close()
+    t = fresh()
+    eng.reset_stats()
+    torch.cuda.profiler.start()
+    ms = timed(lambda: pkg.energy_grad(t, H, ad_iters))
+    torch.cuda.profiler.stop()
+    st = eng.stats()
+    t.close()
+    t = fresh()
+    eng.prof_enable(True)
+    pkg.energy_grad(t, H, ad_iters)
+    prof = eng.prof_query()
+    eng.prof_enable(False)
+    t.close()
+    t = fresh()
+    t.Params["svd_resid_tol"] = 1e-12
+    t._push_params()
+    ms_ck = timed(lambda: [pkg.rg_step(t) for _ in range(ad_iters)])
+    t.close()
+    print(json.dumps({"pullback": WORKLOAD_NAME, "precision": form, "pullback_ms": round(ms, 2),
+                      "checkpoint_iterations_ms": round(ms_ck, 2),
+                      "launches": int(sum(f["launches"] for f in st["families"].values())),
+                      "projector": {k: st[k] for k in ("projector_calls", "extra_passes", "resid_misses",
+                                                       "series_terms", "series_retries", "series_cap_hits")},
+                      "families_ms_serialised": {k: round(v["ms"], 3) for k, v in prof.items() if v["ms"] > 0}}),
+          flush=True)
+    eng.close()
+    return 0
+
+
 def run_tf32_shapes():
     """ipeps_gemm_tf32x3 (3xTF32 on tcgen05: operand splits + GEMM, device time
     by CUDA events, mean over 10 repetitions) on the engine's shapes; credited
@@ -657,11 +727,17 @@ def main():
                     help="kernel aid: 3xTF32 tcgen05 GEMM throughput (splits included) on the engine's shapes")
     ap.add_argument("--projector-shapes", action="store_true",
                     help="kernel aid: the projector alone on synthetic enlarged corners of the workload's size")
+    ap.add_argument("--pullback-profile", action="store_true",
+                    help="profiling aid: one E+grad pullback of the workload alone, between cudaProfilerStart/Stop")
     args = ap.parse_args()
     global WORKLOAD, WORKLOAD_NAME
     if args.projector_shapes:
         WORKLOAD = WORKLOADS[args.workload]
         return run_projector_shapes()
+    if args.pullback_profile:
+        WORKLOAD = WORKLOADS[args.workload]
+        WORKLOAD_NAME = workload_name(WORKLOAD)
+        return run_pullback_profile(args)
     if args.gemm_shapes:
         return run_gemm_shapes()
     if args.tf32_shapes:
