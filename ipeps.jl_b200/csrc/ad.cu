@@ -233,6 +233,17 @@ double dot_host(Ctx& c, const Tensor& x, const Tensor& y) {
   return h;
 }
 
+// *out = sum x*y on the device (stream ordered, no host round trip)
+void dot_dev(Ctx& c, const Tensor& x, const Tensor& y, double* out) {
+  const int64_t n = x.numel();
+  const int blocks = int(std::min<int64_t>((n + 255) / 256, 1024));
+  double* part = static_cast<double*>(c.workspace(size_t(std::max(blocks, 1)) * 8 + 64));
+  dot_partial_kernel<<<std::max(blocks, 1), 256, 0, c.stream>>>(x.f64(), y.f64(), n, part);
+  sum_kernel<<<1, 256, 0, c.stream>>>(part, std::max(blocks, 1), out);
+  IPEPS_LAUNCH_CHECK();
+  c.count(KFam::Reduce, 2.0 * n, 16.0 * n);
+}
+
 void colscale(Ctx& c, Tensor& X, const double* s, int ncols, int mode) {
   colscale_kernel<<<gridn(c, X.dims[0] * ncols), 256, 0, c.stream>>>(X.f64(), X.dims[0], X.dims[0], ncols, s, mode);
   IPEPS_LAUNCH_CHECK();
@@ -503,6 +514,7 @@ void projector_backward(Ctx& c, const Tensor& R1t, bool t1, const Tensor& R2t, b
     constexpr int kMaxTerms = 160;
     constexpr double kTol = 1e-13;
     constexpr double kCheckTol = 1e-10;
+    constexpr int kCheckEvery = 4;
     const double ny0 = std::sqrt(dot_host(c, Yu0, Yu0) + dot_host(c, Yv0, Yv0));
     Tensor Xu = c.zeros(DType::F64, {N1, n}), Xv = c.zeros(DType::F64, {N2, n});
     // M = R1 R2 formed once (N1 x N2): each application of M M^T or M^T M is
@@ -563,21 +575,29 @@ void projector_backward(Ctx& c, const Tensor& R1t, bool t1, const Tensor& R2t, b
         for (int m = 0; m < kMaxTerms; ++m) {
           cheb_acc_kernel<<<gridn(c, N1 * n), 256, 0, c.stream>>>(Xu.f64(), Tu.f64(), N1, n, s.f64(), kSvdEta, b, m);
           cheb_acc_kernel<<<gridn(c, N2 * n), 256, 0, c.stream>>>(Xv.f64(), Tv.f64(), N2, n, s.f64(), kSvdEta, b, m);
-          cheb_coef_max_kernel<<<1, 32, 0, c.stream>>>(s.f64(), n, kSvdEta, b, m + 1, d_cmax);
           IPEPS_LAUNCH_CHECK();
           c.series_terms++;
-          double cnext = 0;
-          IPEPS_CUDA(cudaMemcpyAsync(&cnext, d_cmax, 8, cudaMemcpyDeviceToHost, c.stream));
-          const double nt = std::sqrt(dot_host(c, Tu, Tu) + dot_host(c, Tv, Tv));
-          if (nt > 8.0 * ny0) {
-            blew_up = true;  // spectrum beyond b
-            break;
-          }
-          const double nx = std::sqrt(dot_host(c, Xu, Xu) + dot_host(c, Xv, Xv));
-          // |T_m| <= |T_0| on [0, b]: the remaining terms are bounded by the coefficient tail
-          if (cnext * ny0 <= kTol * nx) {
-            converged = true;
-            break;
+          // the stopping tests read back five device scalars every kCheckEvery terms
+          // (one host round trip instead of five per term)
+          if (m % kCheckEvery == kCheckEvery - 1 || m == kMaxTerms - 1) {
+            cheb_coef_max_kernel<<<1, 32, 0, c.stream>>>(s.f64(), n, kSvdEta, b, m + 1, d_cmax);
+            IPEPS_LAUNCH_CHECK();
+            dot_dev(c, Tu, Tu, d_cmax + 1);
+            dot_dev(c, Tv, Tv, d_cmax + 2);
+            dot_dev(c, Xu, Xu, d_cmax + 3);
+            dot_dev(c, Xv, Xv, d_cmax + 4);
+            double h[5];
+            IPEPS_CUDA(cudaMemcpyAsync(h, d_cmax, sizeof(h), cudaMemcpyDeviceToHost, c.stream));
+            c.sync();
+            if (std::sqrt(h[1] + h[2]) > 8.0 * ny0) {
+              blew_up = true;  // spectrum beyond b
+              break;
+            }
+            // |T_m| <= |T_0| on [0, b]: the remaining terms are bounded by the coefficient tail
+            if (h[0] * ny0 <= kTol * std::sqrt(h[3] + h[4])) {
+              converged = true;
+              break;
+            }
           }
           Tensor Bu, Bv;
           apply_B(Tu, Tv, &Bu, &Bv);
