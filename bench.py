@@ -581,12 +581,14 @@ def run_gemm_shapes():
 def run_pullback_profile(args):
     """The E+grad pullback alone (energy_grad: ad_iters checkpointed iterations
     from a converged environment, the energy on a tape, the backward with the
-    projector adjoints) of the workload, in one precision form: converge once,
-    one warm-up pullback, then one pullback bracketed by cudaProfilerStart /
+    projector adjoints) of the workload, in one precision form.  Each pullback
+    follows the forward iterations on the same environment, as in an E+grad
+    step; one warm-up, then one pullback bracketed by cudaProfilerStart /
     cudaProfilerStop (ncu --profile-from-start off captures only it), timed by
-    CUDA events, with the per-family device profile of a second one and the
+    CUDA events, with the per-family device profile of a third one and the
     projector/adjoint counters.  Also times the checkpoint iterations alone
-    (ad_iters CTMRG steps at the pullback's residual tolerance)."""
+    (ad_iters CTMRG steps at the pullback's residual tolerance, from a copy of
+    the converged environment without sketch seeds)."""
     import torch
     pkg = load_pkg()
     form = "fp64" if args.precision == "both" else args.precision
@@ -616,17 +618,20 @@ def run_pullback_profile(args):
         e.synchronize()
         return s.elapsed_time(e)
 
-    t = fresh()
+    # as in an E+grad step, the pullback follows the forward iterations on the
+    # same environment (its projectors' sketches are seeded from them)
+    t = pkg.CTMTensors(A, cfg, engine=eng)
+    pkg.run_ctm(t, conv_fun="energy", H=H)
     pkg.energy_grad(t, H, ad_iters)
-    t.close()
-    t = fresh()
+    eng.check(eng.lib.ipeps_env_init(t.h))
+    pkg.run_ctm(t, conv_fun="energy", H=H)
     eng.reset_stats()
     torch.cuda.profiler.start()
     ms = timed(lambda: pkg.energy_grad(t, H, ad_iters))
     torch.cuda.profiler.stop()
     st = eng.stats()
-    t.close()
-    t = fresh()
+    eng.check(eng.lib.ipeps_env_init(t.h))
+    pkg.run_ctm(t, conv_fun="energy", H=H)
     eng.prof_enable(True)
     pkg.energy_grad(t, H, ad_iters)
     prof = eng.prof_query()

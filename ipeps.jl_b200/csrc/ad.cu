@@ -544,9 +544,14 @@ void projector_backward(Ctx& c, const Tensor& R1t, bool t1, const Tensor& R2t, b
           nt = nb;
         }
       }
-      double b = std::max(1.25 * lam, 1.2 * est);
-      if (b >= sn2) b = (std::max(lam, est) < sn2) ? 0.5 * (std::max(lam, est) + sn2) : std::max(lam, est);
-      if (!(b > 0)) b = sn2 > 0 ? 0.5 * sn2 : 1.0;
+      // b is at least the rounding level of B (~eps s_1^2): below it the
+      // recursion would amplify rounding noise.  Kept s_n^2 under that floor
+      // are far inside the broadening (f(x) ~ x / eta there, the pole
+      // sqrt(eta) off the real axis), so the expansion converges all the same.
+      const double s1 = pr.sr_host[0], bfloor = 1e-14 * s1 * s1;
+      const double top = std::max(lam, est);
+      double b = std::max({1.25 * lam, 1.2 * est, bfloor});
+      if (b >= sn2 && sn2 > bfloor) b = std::max(top < sn2 ? 0.5 * (top + sn2) : top, bfloor);
       // B~ T = (2/b) B T - T on both sides
       auto apply_B = [&](const Tensor& Tu, const Tensor& Tv, Tensor* Bu, Tensor* Bv) {
         *Bu = Bu_of(Tu);
@@ -624,11 +629,14 @@ void projector_backward(Ctx& c, const Tensor& R1t, bool t1, const Tensor& R2t, b
       }
     }
     // the expansion stopped at its term cap or never passed its check: the
-    // discarded spectrum's share of the gradient is inexact (counted in
-    // ipeps_stats_t, bit 16 of the status word)
+    // discarded spectrum's share of the gradient is left out (counted in
+    // ipeps_stats_t, bit 16 of the status word) rather than taken from a
+    // diverging partial sum
     if (!series_done) {
       c.series_cap_hits++;
       flag_status(c, 16);
+      Xu = c.zeros(DType::F64, {N1, n});
+      Xv = c.zeros(DType::F64, {N2, n});
     }
     // Acol += M^T X_u ; Bcol += M X_v ; and the s_t-scaled terms
     Tensor MtXu = mm(c, Mx, 'T', Xu, 'N');
@@ -759,6 +767,13 @@ double energy_grad(Env& e, const Tensor& Hh, const Tensor& Hv, int ad_iters, Ten
     ~RestoreTol() { e.prm.svd.resid_tol = v; }
   } restore_tol{e, resid_tol0};
   e.prm.svd.resid_tol = std::min(resid_tol0, 1e-12);
+  const int max_extra0 = e.prm.svd.max_extra_passes;
+  struct RestoreExtra {
+    Env& e;
+    int v;
+    ~RestoreExtra() { e.prm.svd.max_extra_passes = v; }
+  } restore_extra{e, max_extra0};
+  e.prm.svd.max_extra_passes = std::max(max_extra0, 12);
   {
     std::complex<double> conv = 1.0;
     for (int i = 1; i <= ad_iters; ++i) {
@@ -785,6 +800,7 @@ double energy_grad(Env& e, const Tensor& Hh, const Tensor& Hv, int ad_iters, Ten
     }
   }
   e.prm.svd.resid_tol = resid_tol0;
+  e.prm.svd.max_extra_passes = max_extra0;
   // energy on a tape (evaluation.jl:15-29)
   std::array<Tensor, 4> gC, gE;
   Tensor gAcc, gAdc;

@@ -401,15 +401,22 @@ ProjResult projector_impl(Ctx& c, Ops& o, int chi, const SvdParams& sp, ProjCach
     Vk = c.alloc(dt, {N2, k});
     gemm(c, dt, 'N', 'N', N2, k, k, cplx(1), sk.Q2.data(), N2, Js.data(), k, cplx(0), Vk.data(), N2, true);
     if (q == 0 && k == Nmin) break;  // the sketch spans a whole side of M: exact
-    // residual of the kept triplets: ||M v_i - s_i u_i|| <= resid_tol * s_1
-    Tensor Vc = c.alloc(dt, {N2, nc});
-    copy_cols(c, Vc, Vk, N2, nc, w);
+    // residual of the kept triplets and the next one: ||M v_i - s_i u_i|| <= resid_tol * s_1.
+    // For the adjoint (keep_factors) also the tail down to 0.8 s_n: the adjoint
+    // sums those triplets exactly, and the interval of its expansion of the
+    // rest of the spectrum, and with it the number of terms, is set by the
+    // first triplet it does not resolve.
+    int nr = nc;
+    if (keep_factors)
+      while (nr < k && all[nr] >= 0.8 * all[n - 1]) ++nr;
+    Tensor Vc = c.alloc(dt, {N2, nr});
+    copy_cols(c, Vc, Vk, N2, nr, w);
     Tensor Res = o.M(Vc);
-    Tensor Us = c.alloc(dt, {k, nc});
-    gather_cols(c, sk.X.f64(), w * k, w * k, d_perm, nc, nullptr, 0, Us.f64(), w * k);  // W = Ux S
-    gemm(c, dt, 'N', 'N', N1, nc, k, cplx(-1), sk.Q.data(), N1, Us.data(), k, cplx(1), Res.data(), N1, true);
+    Tensor Us = c.alloc(dt, {k, nr});
+    gather_cols(c, sk.X.f64(), w * k, w * k, d_perm, nr, nullptr, 0, Us.f64(), w * k);  // W = Ux S
+    gemm(c, dt, 'N', 'N', N1, nr, k, cplx(-1), sk.Q.data(), N1, Us.data(), k, cplx(1), Res.data(), N1, true);
     IPEPS_CUDA(cudaMemsetAsync(d_res, 0, 8, c.stream));
-    colnorm_max_kernel<<<(nc * 32 + 255) / 256, 256, 0, c.stream>>>(Res.f64(), w * N1, nc,
+    colnorm_max_kernel<<<(nr * 32 + 255) / 256, 256, 0, c.stream>>>(Res.f64(), w * N1, nr,
                                                                     reinterpret_cast<unsigned long long*>(d_res));
     IPEPS_LAUNCH_CHECK();
     double res = 0;
