@@ -552,13 +552,30 @@ void projector_backward(Ctx& c, const Tensor& R1t, bool t1, const Tensor& R2t, b
       const double top = std::max(lam, est);
       double b = std::max({1.25 * lam, 1.2 * est, bfloor});
       if (b >= sn2 && sn2 > bfloor) b = std::max(top < sn2 ? 0.5 * (top + sn2) : top, bfloor);
-      // B~ T = (2/b) B T - T on both sides
-      auto apply_B = [&](const Tensor& Tu, const Tensor& Tv, Tensor* Bu, Tensor* Bv) {
-        *Bu = Bu_of(Tu);
-        *Bv = Bv_of(Tv);
-        axpby_kernel<<<gridn(c, Bu->numel()), 256, 0, c.stream>>>(-1.0, Tu.f64(), 2.0 / b, Bu->f64(), Bu->numel());
-        axpby_kernel<<<gridn(c, Bv->numel()), 256, 0, c.stream>>>(-1.0, Tv.f64(), 2.0 / b, Bv->f64(), Bv->numel());
+      // One term's products with M, the u and v sides batched into two GEMMs of
+      // 2n columns: W1 = M^T [T_u | M T_v] = [M^T T_u | M^T M T_v], then, with the
+      // next v-side vector T_v' formed from the second half,
+      // W2 = M [M^T T_u | T_v'] = [M M^T T_u | M T_v'], whose second half feeds the
+      // next term.  B~ T = (2/b) P (...) - T, T_{m+1} = 2 B~ T_m - T_{m-1}.
+      Tensor W1 = c.alloc(DType::F64, {N2, 2 * int64_t(n)}), W2 = c.alloc(DType::F64, {N1, 2 * int64_t(n)});
+      auto next_T = [&](Tensor& B, const Tensor& T, const Tensor& Tprev, int m) {
+        axpby_kernel<<<gridn(c, B.numel()), 256, 0, c.stream>>>(-1.0, T.f64(), 2.0 / b, B.f64(), B.numel());
+        if (m > 0) axpby_kernel<<<gridn(c, B.numel()), 256, 0, c.stream>>>(-1.0, Tprev.f64(), 2.0, B.f64(), B.numel());
         IPEPS_LAUNCH_CHECK();
+      };
+      auto apply_B = [&](const Tensor& Tu, const Tensor& Tv, const Tensor& Pu, const Tensor& Pv, int m, Tensor* Bu,
+                         Tensor* Bv) {
+        IPEPS_CUDA(cudaMemcpyAsync(W2.data(), Tu.data(), size_t(N1) * n * 8, cudaMemcpyDeviceToDevice, c.stream));
+        gemm(c, DType::F64, 'T', 'N', N2, 2 * n, N1, cplx(1), Mx.data(), N1, W2.data(), N1, cplx(0), W1.data(), N2,
+             true);
+        *Bv = project_out(c, Vr, cols(W1, n, n));
+        next_T(*Bv, Tv, Pv, m);
+        IPEPS_CUDA(cudaMemcpyAsync(cols(W1, n, n).data(), Bv->data(), size_t(N2) * n * 8, cudaMemcpyDeviceToDevice,
+                                   c.stream));
+        gemm(c, DType::F64, 'N', 'N', N1, 2 * n, N2, cplx(1), Mx.data(), N1, W1.data(), N2, cplx(0), W2.data(), N1,
+             true);
+        *Bu = project_out(c, Ur, cols(W2, 0, n));
+        next_T(*Bu, Tu, Pu, m);
       };
       // relative residual of ((s_i^2 - B)^2 + eta) X_i = (s_i^2 - B) Y_i over all columns of one side
       auto check = [&](const Tensor& X, const Tensor& Y, bool u_side) {
@@ -577,6 +594,9 @@ void projector_backward(Ctx& c, const Tensor& R1t, bool t1, const Tensor& R2t, b
         Tensor Pu = Yu0, Pv = Yv0;  // T_{m-1}
         Tensor Tu = Yu0, Tv = Yv0;  // T_m
         bool blew_up = false, converged = false;
+        // M T_v of the first term, in the second half of W2
+        gemm(c, DType::F64, 'N', 'N', N1, n, N2, cplx(1), Mx.data(), N1, Tv.data(), N2, cplx(0),
+             cols(W2, n, n).data(), N1, true);
         for (int m = 0; m < kMaxTerms; ++m) {
           cheb_acc_kernel<<<gridn(c, N1 * n), 256, 0, c.stream>>>(Xu.f64(), Tu.f64(), N1, n, s.f64(), kSvdEta, b, m);
           cheb_acc_kernel<<<gridn(c, N2 * n), 256, 0, c.stream>>>(Xv.f64(), Tv.f64(), N2, n, s.f64(), kSvdEta, b, m);
@@ -605,13 +625,7 @@ void projector_backward(Ctx& c, const Tensor& R1t, bool t1, const Tensor& R2t, b
             }
           }
           Tensor Bu, Bv;
-          apply_B(Tu, Tv, &Bu, &Bv);
-          if (m > 0) {
-            // T_{m+1} = 2 B~ T_m - T_{m-1}
-            axpby_kernel<<<gridn(c, Bu.numel()), 256, 0, c.stream>>>(-1.0, Pu.f64(), 2.0, Bu.f64(), Bu.numel());
-            axpby_kernel<<<gridn(c, Bv.numel()), 256, 0, c.stream>>>(-1.0, Pv.f64(), 2.0, Bv.f64(), Bv.numel());
-            IPEPS_LAUNCH_CHECK();
-          }
+          apply_B(Tu, Tv, Pu, Pv, m, &Bu, &Bv);
           Pu = Tu;
           Pv = Tv;
           Tu = Bu;
