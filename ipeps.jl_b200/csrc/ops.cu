@@ -149,38 +149,28 @@ struct RowArgs {
   int64_t istride[kMaxDims];  // their input strides
 };
 
-// Each warp copies kPermRows rows at a time, all their loads issued before the
-// stores, so that enough bytes are in flight to keep HBM busy (one row per
-// warp left a short row's single load round trip exposed).
-constexpr int kPermRows = 4;
+// A warp copies one chunk of up to kPermChunk consecutive elements of one
+// row, so that a few very long rows still spread over the whole GPU and many
+// short rows take one warp each.
+constexpr int64_t kPermChunk = 2048;
 
 template <typename T>
-__global__ void permute_rows(RowArgs a, int64_t rows, const T* __restrict__ in, T* __restrict__ out) {
+__global__ void permute_rows(RowArgs a, int64_t rows, int64_t nchunk, const T* __restrict__ in, T* __restrict__ out) {
   const int lane = threadIdx.x & 31;
   const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
-  for (int64_t r0 = ((int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5) * kPermRows; r0 < rows;
-       r0 += nwarps * kPermRows) {
-    const T* src[kPermRows];
-    T* dst[kPermRows];
-#pragma unroll
-    for (int j = 0; j < kPermRows; ++j) {
-      const int64_t r = min(r0 + j, rows - 1);  // rows past the end repeat the last one (same values)
-      int64_t q = r, off = 0;
-      for (int i = 0; i < a.nd; ++i) {
-        const int64_t t = q / a.odims[i];
-        off += (q - t * a.odims[i]) * a.istride[i];
-        q = t;
-      }
-      src[j] = in + off;
-      dst[j] = out + r * a.n0;
+  const int64_t units = rows * nchunk;
+  for (int64_t u = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; u < units; u += nwarps) {
+    const int64_t r = u / nchunk, c0 = (u - r * nchunk) * kPermChunk;
+    int64_t q = r, off = 0;
+    for (int i = 0; i < a.nd; ++i) {
+      const int64_t t = q / a.odims[i];
+      off += (q - t * a.odims[i]) * a.istride[i];
+      q = t;
     }
-    for (int64_t i = lane; i < a.n0; i += 32) {
-      T v[kPermRows];
-#pragma unroll
-      for (int j = 0; j < kPermRows; ++j) v[j] = src[j][i];
-#pragma unroll
-      for (int j = 0; j < kPermRows; ++j) dst[j][i] = v[j];
-    }
+    const T* src = in + off;
+    T* dst = out + r * a.n0;
+    const int64_t c1 = min(a.n0, c0 + kPermChunk);
+    for (int64_t i = c0 + lane; i < c1; i += 32) dst[i] = src[i];
   }
 }
 
@@ -244,8 +234,9 @@ void permute_impl(Ctx& c, const Tensor& in, const std::vector<int>& perm, Tensor
       a.istride[i - 1] = istr[perm[i]];
     }
     const int64_t rows = total / a.n0;
-    const int64_t blocks = std::min<int64_t>((rows + 8 * kPermRows - 1) / (8 * kPermRows), int64_t(c.sm_count) * 16);
-    permute_rows<T><<<unsigned(std::max<int64_t>(blocks, 1)), 256, 0, c.stream>>>(a, rows, ip, op);
+    const int64_t nchunk = (a.n0 + kPermChunk - 1) / kPermChunk;
+    const int64_t blocks = std::min<int64_t>((rows * nchunk + 7) / 8, int64_t(c.sm_count) * 16);
+    permute_rows<T><<<unsigned(std::max<int64_t>(blocks, 1)), 256, 0, c.stream>>>(a, rows, nchunk, ip, op);
   } else if (perm[0] == 0 || in.dims[0] == 1 || out.dims[0] == 1) {
     PermArgs a{};
     a.nd = nd;
