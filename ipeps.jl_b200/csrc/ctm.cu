@@ -692,6 +692,16 @@ int run_ctm(Env& e, int conv_mode, const Tensor* Hh, const Tensor* Hv, double* l
   // FP64 iterations.  The CTMRG map contracts errors, so the FP32-level errors
   // of the mixed iterations decay in the FP64 ones.  With rg_tol = 0 (a fixed
   // number of iterations) only the last polish_iters iterations run in FP64.
+  // With a tolerance, the switch also happens when the mixed iterations stall
+  // close to convergence: the change per iteration is below 1e-6 of the
+  // objective and has not halved against either of the two iterations before
+  // (the FP32-level floor of the 3xTF32 products can sit above
+  // polish_tol * rg_tol, and the run would reach max_iter unconverged).
+  auto stalled = [&]() {
+    const size_t n = diffs.size();
+    return e.prm.rg_tol > 0 && n >= 4 && diffs[n - 1] < 1e-6 * std::max(std::abs(conv), 1e-12) &&
+           diffs[n - 1] > 0.5 * std::min(diffs[n - 2], diffs[n - 3]);
+  };
   Ctx& c = *e.ctx;
   const int prec0 = c.precision;
   const bool polish = (prec0 == kPrecMixed) && e.prm.polish_iters > 0;
@@ -721,7 +731,8 @@ int run_ctm(Env& e, int conv_mode, const Tensor* Hh, const Tensor* Hv, double* l
     };
     int last = 0;
     for (; i <= e.prm.max_iter; ++i) {
-      if (polish && c.precision != kPrecFP64 && (i >= polish_start || diffs.back() < e.prm.polish_tol * e.prm.rg_tol))
+      if (polish && c.precision != kPrecFP64 &&
+          (i >= polish_start || diffs.back() < e.prm.polish_tol * e.prm.rg_tol || stalled()))
         c.precision = kPrecFP64;
       std::vector<double> s = rg_step(e);
       if (polish && c.precision == kPrecFP64) fp64_done++;
@@ -743,7 +754,8 @@ int run_ctm(Env& e, int conv_mode, const Tensor* Hh, const Tensor* Hv, double* l
     return done ? last : e.prm.max_iter;
   }
   for (; i <= e.prm.max_iter; ++i) {
-    if (polish && c.precision != kPrecFP64 && (i >= polish_start || diffs.back() < e.prm.polish_tol * e.prm.rg_tol))
+    if (polish && c.precision != kPrecFP64 &&
+        (i >= polish_start || diffs.back() < e.prm.polish_tol * e.prm.rg_tol || (by_value && stalled())))
       c.precision = kPrecFP64;
     std::vector<double> s = rg_step(e);
     if (polish && c.precision == kPrecFP64) fp64_done++;

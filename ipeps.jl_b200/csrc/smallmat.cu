@@ -3,8 +3,8 @@
 //   chol_blocked      G = R^T R in one CTA, 32-column panels: one warp factors the
 //                     diagonal block in registers, the block's rows of R are solved
 //                     column-parallel, the trailing update is a register-tiled SYRK.
-//   chol_ldl          the same for k <= 160 with the upper triangle in registers,
-//                     eliminated in panels of 8 rows: two barriers per panel.
+//   chol_ldl          the same for k <= 160 with the upper triangle in registers: one
+//                     barrier per elimination step.
 //   trsm_right_upper  Q = Y R^-1, two rows of Y per warp (the rows are independent), at
 //                     most one CTA per SM, R staged row-major in each CTA's shared memory.
 //   jacobi_svd_auto   one-sided Jacobi with only X in shared memory; every rotation is
@@ -206,35 +206,33 @@ __global__ void __launch_bounds__(kCholThreads) chol_blocked_kernel(double* G, i
 }
 
 // Register-resident Cholesky for k <= 32 NBB (NBB <= 5), same contract as
-// chol_blocked_kernel.  512 threads hold the upper triangle in registers,
-// thread (w, l) of warp w and lane l the entries (w + 16 a, l + 32 b) (slots
-// a <= 2b + 1 can reach the triangle).  The elimination runs in panels of
-// kPW rows with two barriers each:
-//   A  the warps owning the panel's rows publish them in shared memory
-//      (double-buffered by panel parity);
-//   B  warp 0 eliminates within the panel (kPW pivots, each row divided by its
-//      pivot with __drcp_rn) and writes the panel's rows of R = D^1/2 U;
-//   C  every thread applies the panel's kPW rank-1 updates
-//      a[r][c] -= a[j][r] (a[j][c] / a[j][j]) to its slots below the panel.
-// Slots left of the diagonal take garbage that is never read.
+// chol_blocked_kernel.  The right-looking elimination is written as
+// G = U^T D U (U unit upper): step j subtracts a[j][r] a[j][c] / a[j][j] from
+// every a[r][c] with c >= r > j, and R = D^1/2 U at the end.  512 threads
+// hold the upper triangle in registers, thread (w, l) of warp w and lane l the
+// entries (w + 16 a, l + 32 b) (slots a <= 2b + 1 can reach the triangle), so a
+// step costs one barrier: the warp owning row j publishes the row and the row
+// divided by the pivot in shared memory (double-buffered by the parity of j),
+// and every thread updates its slots from two broadcast loads per row and
+// one load per column block.
 constexpr int kLdlThreads = 512;
-constexpr int kPW = 8;
 
 size_t chol_ldl_smem_doubles(int k) {
   const size_t npk = (size_t(k) * (k + 1) / 2 + 1) & ~size_t(1);
-  return npk + 4 * size_t(kPW) * 160 + 160 + 8;
+  return npk + 4 * 160 + 2 * 160 + 8;
 }
 
 template <int NBB>
 __global__ void __launch_bounds__(kLdlThreads, 1) chol_ldl_kernel(double* G, int k, int64_t ldg, double shift_factor,
-                                                                   double* Rrow) {
+                                                                double* Rrow) {
   constexpr int NBA = 2 * NBB, KP = 32 * NBB;
   extern __shared__ __align__(16) double sm[];
   const int npk = ((k * (k + 1)) / 2 + 1) & ~1;
-  double* P = sm;                   // R, packed upper triangle, column by column
-  double* PB = P + npk;             // [2][kPW][KP]: the panel's rows as eliminated
-  double* Wd = PB + 2 * kPW * KP;   // [2][kPW][KP]: the same divided by their pivots
-  double* dd = Wd + 2 * kPW * KP;   // pivots (0: failed)
+  double* P = sm;             // packed upper triangle, column by column
+  double* raw = P + npk;      // [2][KP]: row j of the eliminated matrix
+  double* scl = raw + 2 * KP; // [2][KP]: the same divided by the pivot (0 for a failed pivot)
+  double* dd = scl + 2 * KP;  // pivots (0: failed)
+  double* rs = dd + KP;       // 1 / sqrt(pivot), 0 for a failed pivot
   __shared__ double s_red[kLdlThreads / 32];
   __shared__ double s_tr;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -254,8 +252,7 @@ __global__ void __launch_bounds__(kLdlThreads, 1) chol_ldl_kernel(double* G, int
         if (t < kk2 && i <= j) P[pku(i, j)] = v[u];
       }
     }
-    // panel buffers: columns >= k stay 0 (rows below k read them as zeros)
-    for (int t = tid; t < 4 * kPW * KP; t += kLdlThreads) PB[t] = 0.0;
+    for (int t = tid; t < 4 * KP; t += kLdlThreads) raw[t] = 0.0;  // raw and scl, rows >= k stay 0
   }
   __syncthreads();
   double t = 0;
@@ -284,68 +281,66 @@ __global__ void __launch_bounds__(kLdlThreads, 1) chol_ldl_kernel(double* G, int
       v[a][b] = x;
     }
 
-  for (int p0 = 0; p0 < k; p0 += kPW) {
-    double* pb = PB + ((p0 / kPW) & 1) * kPW * KP;
-    double* wd = Wd + ((p0 / kPW) & 1) * kPW * KP;
-    // (A) rows p0 .. p0 + kPW - 1 sit in warps (p0 mod 16) .. + kPW - 1, slot a = p0 / 16
-    {
-      const int jj = warp - (p0 & 15), r = p0 + jj;
-      if (jj >= 0 && jj < kPW && r < k) {
-        const int ar = r >> 4;
-#pragma unroll
-        for (int a = 0; a < NBA; ++a) {
-          if (a != ar) continue;
-#pragma unroll
-          for (int b = 0; b < NBB; ++b) {
-            if (a > 2 * b + 1) continue;
-            const int c = lane + 32 * b;
-            if (c >= p0 && c < k) pb[jj * KP + c] = v[a][b];
-          }
-        }
-      }
-    }
-    __syncthreads();
-    // (B) warp 0: the panel's pivots in order
-    if (warp == 0) {
-      for (int jj = 0; jj < kPW && p0 + jj < k; ++jj) {
-        const int r = p0 + jj;
-        const double d = pb[jj * KP + r];
-        const bool ok = d > tiny;
-        const double inv = ok ? __drcp_rn(d) : 0.0, rs = ok ? rsqrt(d) : 0.0;
-        for (int c = lane; c < k; c += 32) {
-          const double x = pb[jj * KP + c];
-          if (c > r) wd[jj * KP + c] = x * inv;
-          if (c >= r) P[pku(r, c)] = (c == r) ? (ok ? d * rs : 1.0) : x * rs;
-        }
-        if (lane == 0) dd[r] = ok ? d : 0.0;
-        __syncwarp();
-        for (int ii = jj + 1; ii < kPW && p0 + ii < k; ++ii) {
-          const double m = pb[jj * KP + p0 + ii] * inv;
-          for (int c = p0 + ii + lane; c < k; c += 32) pb[ii * KP + c] = fma(-m, pb[jj * KP + c], pb[ii * KP + c]);
-        }
-        __syncwarp();
-      }
-    }
-    __syncthreads();
-    // (C) the panel's rank-1 updates of the rows below it
-    const int pe = p0 + kPW;
-    for (int jj = 0; jj < kPW && p0 + jj < k; ++jj) {
-      double s[NBB];
-#pragma unroll
-      for (int b = 0; b < NBB; ++b) s[b] = (32 * b + 31 >= pe) ? wd[jj * KP + lane + 32 * b] : 0.0;
+  for (int j = 0; j < k; ++j) {
+    const int p = j & 1;
+    double* rw = raw + p * KP;
+    double* sc = scl + p * KP;
+    if (warp == (j & 15)) {
+      // this warp holds row j: publish a[j][c] (c >= j), then a[j][c] / a[j][j]
+      const int aj = j >> 4;
 #pragma unroll
       for (int a = 0; a < NBA; ++a) {
-        const int r = warp + 16 * a;
-        if (r < pe) continue;
-        const double ra = pb[jj * KP + r];
+        if (a != aj) continue;
 #pragma unroll
         for (int b = 0; b < NBB; ++b) {
           if (a > 2 * b + 1) continue;
-          v[a][b] = fma(-ra, s[b], v[a][b]);
+          const int c = lane + 32 * b;
+          if (c >= j && c < k) rw[c] = v[a][b];
         }
+      }
+      __syncwarp();
+      const double d = rw[j];
+      const bool ok = d > tiny;
+      const double inv = ok ? __drcp_rn(d) : 0.0;
+#pragma unroll
+      for (int b = 0; b < NBB; ++b) {
+        const int c = lane + 32 * b;
+        if (c > j && c < k) sc[c] = rw[c] * inv;
+      }
+      if (lane == 0) dd[j] = ok ? d : 0.0;
+    }
+    __syncthreads();
+    // a[r][c] -= a[j][r] * (a[j][c] / a[j][j]) for r > j; slots left of the
+    // diagonal take garbage that is never read
+    double s[NBB];
+#pragma unroll
+    for (int b = 0; b < NBB; ++b) s[b] = (32 * b + 31 > j) ? sc[lane + 32 * b] : 0.0;
+#pragma unroll
+    for (int a = 0; a < NBA; ++a) {
+      const int r = warp + 16 * a;
+      if (r <= j) continue;
+      const double ra = rw[r];
+#pragma unroll
+      for (int b = 0; b < NBB; ++b) {
+        if (a > 2 * b + 1) continue;
+        v[a][b] = fma(-ra, s[b], v[a][b]);
       }
     }
   }
+  for (int i = tid; i < k; i += kLdlThreads) rs[i] = dd[i] > 0.0 ? rsqrt(dd[i]) : 0.0;
+  __syncthreads();
+  // R = D^1/2 U into P; a failed pivot gives R[j][j] = 1 and row j zero
+#pragma unroll
+  for (int a = 0; a < NBA; ++a)
+#pragma unroll
+    for (int b = 0; b < NBB; ++b) {
+      if (a > 2 * b + 1) continue;
+      const int r = warp + 16 * a, c = lane + 32 * b;
+      if (r <= c && c < k) {
+        const double q = rs[r];
+        P[pku(r, c)] = (r == c) ? (q > 0.0 ? dd[r] * q : 1.0) : v[a][b] * q;
+      }
+    }
   __syncthreads();
   for (int j = warp; j < k; j += kLdlThreads / 32)
     for (int i = lane; i < k; i += 32) G[i + int64_t(j) * ldg] = (i <= j) ? P[pku(i, j)] : 0.0;
