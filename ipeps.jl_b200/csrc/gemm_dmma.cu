@@ -282,14 +282,6 @@ void gemm_f64_dmma(Ctx& c, char opA, char opB, int64_t m, int64_t n, int64_t k, 
       launch_ops<128, 64, 4, 2, 2>(c, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
     else
       launch_ops<128, 64, 4, 2, 1>(c, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
-  } else if (m >= 1024 && n >= 128 && k >= 1024 && big_tiles < c.sm_count) {
-    // mid-size products with a long K (the projector adjoint's 2500 x 200 x 2500,
-    // the range finder's N x 160 x N): 128x64 tiles with split-K over two waves
-    // keep 16 warps per SM instead of 8 with 64x64 tiles
-    if (vec)
-      launch_ops<128, 64, 4, 2, 2>(c, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
-    else
-      launch_ops<128, 64, 4, 2, 1>(c, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
   } else if (big_tiles >= c.sm_count) {
     if (vec)
       launch_ops<128, 128, 2, 4, 2>(c, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
