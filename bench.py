@@ -556,7 +556,8 @@ def run_gemm_shapes():
     eng = pkg.Engine(0)
     shapes = [("N", "N", 2500, 160, 2500), ("T", "N", 2500, 160, 2500), ("T", "N", 160, 160, 2500),
               ("N", "N", 2500, 200, 2500), ("T", "N", 2500, 200, 2500),
-              ("N", "N", 2500, 2500, 100), ("N", "N", 250000, 50, 25), ("N", "T", 4096, 4096, 4096)]
+              ("N", "N", 2500, 2500, 100), ("N", "N", 250000, 50, 25), ("N", "T", 4096, 4096, 4096),
+              ("N", "N", 4096, 4096, 4096)]
     rng = np.random.default_rng(0)
     for oa, ob, m, n, k in shapes:
         A = rng.standard_normal((m, k) if oa == "N" else (k, m))

@@ -195,7 +195,8 @@ struct RealOps {
     return X;
   }
   void jacobi(Tensor& X, Tensor& J, Tensor& S, int k, const SvdParams& sp, int* d_sweeps) {
-    jacobi_svd_auto(c, X.f64(), k, k, k, J.f64(), k, S.f64(), sp.jacobi_max_sweeps, sp.jacobi_tol, d_sweeps);
+    const double tol = (c.precision == kPrecMixed) ? std::max(sp.jacobi_tol, sp.jacobi_tol_mixed) : sp.jacobi_tol;
+    jacobi_svd_auto(c, X.f64(), k, k, k, J.f64(), k, S.f64(), sp.jacobi_max_sweeps, tol, d_sweeps);
   }
   // sketch width: 128 columns when that still oversamples by want/2 (the
   // Jacobi then rotates all of its 64 pairs in one pass of its 8-lane groups),

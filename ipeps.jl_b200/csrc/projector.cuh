@@ -34,6 +34,11 @@ struct SvdParams {
   bool warm_start = true;
   int jacobi_max_sweeps = 40;
   double jacobi_tol = 0.0;  // <= 0: m * eps (rounding level of the column dot products)
+  // the Jacobi SVD's tolerance in the mixed form's 3xTF32 iterations, whose
+  // products carry ~1e-7 relative errors: the last sweep or two that take the
+  // column angles from 1e-10 to the rounding level buy nothing there (the
+  // FP64 iterations at the end of a run use jacobi_tol)
+  double jacobi_tol_mixed = 1e-10;
 };
 
 // Resolved right vectors of the last two calls of one direction (warm start).
