@@ -211,12 +211,10 @@ __global__ void __launch_bounds__(kCholThreads) chol_blocked_kernel(double* G, i
 // every a[r][c] with c >= r > j, and R = D^1/2 U at the end.  512 threads
 // hold the upper triangle in registers, thread (w, l) of warp w and lane l the
 // entries (w + 16 a, l + 32 b) (slots a <= 2b + 1 can reach the triangle), so a
-// step costs one barrier: the warp owning row j has published the row and the
-// row divided by the pivot in shared memory (double-buffered by the parity of
-// j), and every thread updates its slots from two broadcast loads per row and
-// one load per column block.  The warp owning row j + 1 updates that row first
-// and publishes it during step j, so the next step starts without waiting for
-// a publish.
+// step costs one barrier: the warp owning row j publishes the row and the row
+// divided by the pivot in shared memory (double-buffered by the parity of j),
+// and every thread updates its slots from two broadcast loads per row and
+// one load per column block.
 constexpr int kLdlThreads = 512;
 
 size_t chol_ldl_smem_doubles(int k) {
@@ -283,65 +281,44 @@ __global__ void __launch_bounds__(kLdlThreads, 1) chol_ldl_kernel(double* G, int
       v[a][b] = x;
     }
 
-  // publish row j (c >= j) into buffer j & 1: a[j][c], then a[j][c] / a[j][j]
-  // (called by the warp holding row j, with that row's slots up to date)
-  auto publish = [&](int j) {
-    double* rw = raw + (j & 1) * KP;
-    double* sc = scl + (j & 1) * KP;
-    const int aj = j >> 4;
-#pragma unroll
-    for (int a = 0; a < NBA; ++a) {
-      if (a != aj) continue;
-#pragma unroll
-      for (int b = 0; b < NBB; ++b) {
-        if (a > 2 * b + 1) continue;
-        const int c = lane + 32 * b;
-        if (c >= j && c < k) rw[c] = v[a][b];
-      }
-    }
-    __syncwarp();
-    const double d = rw[j];
-    const bool ok = d > tiny;
-    const double inv = ok ? __drcp_rn(d) : 0.0;
-#pragma unroll
-    for (int b = 0; b < NBB; ++b) {
-      const int c = lane + 32 * b;
-      if (c > j && c < k) sc[c] = rw[c] * inv;
-    }
-    if (lane == 0) dd[j] = ok ? d : 0.0;
-  };
-  if (warp == 0) publish(0);
   for (int j = 0; j < k; ++j) {
     const int p = j & 1;
-    const double* rw = raw + p * KP;
-    const double* sc = scl + p * KP;
-    __syncthreads();  // row j published; every read of buffer (j + 1) & 1 of step j - 1 done
+    double* rw = raw + p * KP;
+    double* sc = scl + p * KP;
+    if (warp == (j & 15)) {
+      // this warp holds row j: publish a[j][c] (c >= j), then a[j][c] / a[j][j]
+      const int aj = j >> 4;
+#pragma unroll
+      for (int a = 0; a < NBA; ++a) {
+        if (a != aj) continue;
+#pragma unroll
+        for (int b = 0; b < NBB; ++b) {
+          if (a > 2 * b + 1) continue;
+          const int c = lane + 32 * b;
+          if (c >= j && c < k) rw[c] = v[a][b];
+        }
+      }
+      __syncwarp();
+      const double d = rw[j];
+      const bool ok = d > tiny;
+      const double inv = ok ? __drcp_rn(d) : 0.0;
+#pragma unroll
+      for (int b = 0; b < NBB; ++b) {
+        const int c = lane + 32 * b;
+        if (c > j && c < k) sc[c] = rw[c] * inv;
+      }
+      if (lane == 0) dd[j] = ok ? d : 0.0;
+    }
+    __syncthreads();
     // a[r][c] -= a[j][r] * (a[j][c] / a[j][j]) for r > j; slots left of the
     // diagonal take garbage that is never read
     double s[NBB];
 #pragma unroll
     for (int b = 0; b < NBB; ++b) s[b] = (32 * b + 31 > j) ? sc[lane + 32 * b] : 0.0;
-    // the warp holding row j + 1 updates that row first and publishes it at
-    // once, off the critical path of the next step
-    const int jn = j + 1, an = jn >> 4;
-    const bool next_owner = jn < k && warp == (jn & 15);
-    if (next_owner) {
-      const double ra = rw[jn];
-#pragma unroll
-      for (int a = 0; a < NBA; ++a) {
-        if (a != an) continue;
-#pragma unroll
-        for (int b = 0; b < NBB; ++b) {
-          if (a > 2 * b + 1) continue;
-          v[a][b] = fma(-ra, s[b], v[a][b]);
-        }
-      }
-      publish(jn);
-    }
 #pragma unroll
     for (int a = 0; a < NBA; ++a) {
       const int r = warp + 16 * a;
-      if (r <= j || (next_owner && a == an)) continue;
+      if (r <= j) continue;
       const double ra = rw[r];
 #pragma unroll
       for (int b = 0; b < NBB; ++b) {
@@ -350,7 +327,6 @@ __global__ void __launch_bounds__(kLdlThreads, 1) chol_ldl_kernel(double* G, int
       }
     }
   }
-  __syncthreads();
   for (int i = tid; i < k; i += kLdlThreads) rs[i] = dd[i] > 0.0 ? rsqrt(dd[i]) : 0.0;
   __syncthreads();
   // R = D^1/2 U into P; a failed pivot gives R[j][j] = 1 and row j zero
