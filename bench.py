@@ -664,6 +664,71 @@ def run_pullback_profile(args):
     return 0
 
 
+def run_optim_gs(args):
+    """The full optim_gs of the D=5 chi=100 workload (L-BFGS over A on the unit
+    sphere, optim_gs.jl:14-118) for args.optim_gs steps in each form, from the
+    same seeded A: every step's fg! runs CTMRG from init_ctm1 with the energy
+    criterion (rg_tol 1e-8, at most 30 iterations) and the pullback of 4
+    iterations.  Reports E+grad evals/s per form, the energies after each step
+    and the difference of the final energies."""
+    import torch
+    pkg = load_pkg()
+    D, d, chi = (WORKLOAD[k] for k in ("D", "d", "chi"))
+    H = heisenberg(1.0)
+    A0 = random_A(D, d, seed=1000)
+    cfg = pkg.default_config()
+    cfg.update(chi=chi, min_iter=4, max_iter=30, rg_tol=1e-8, ad_max_iter=4)
+    out = {"optim_gs": WORKLOAD_NAME.split(":")[0], "lbfgs_steps": args.optim_gs,
+           "fg": "CTMRG from init_ctm1, energy criterion rg_tol 1e-8, min 4 / max 30 iterations, pullback of 4"}
+    for form in ("fp64", "mixed"):
+        eng = pkg.Engine(0, precision=form)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = pkg.drivers.optim_gs(H, A0, dict(cfg), iterations=args.optim_gs, engine=eng)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        out[form] = {"seconds": round(dt, 2), "evals": r["evals"], "evals_per_s": r["evals"] / dt,
+                     "steps_done": len(r["energies"]), "E_final": r["energies"][-1],
+                     "energies": [float(e) for e in r["energies"]]}
+        eng.close()
+    out["dE_final_mixed_vs_fp64"] = abs(out["mixed"]["E_final"] - out["fp64"]["E_final"])
+    out["mixed_over_fp64_evals_per_s"] = out["mixed"]["evals_per_s"] / out["fp64"]["evals_per_s"]
+    print(json.dumps(out), flush=True)
+    return 0
+
+
+def run_es_momentum(args):
+    """One momentum of the excited-state workload (Heisenberg D=3 d=2 chi=48):
+    a ground state from args.es_gs_steps L-BFGS steps of optim_gs from a seeded
+    A, prepare_basis (reconverged environment, normalised state, E0/2
+    subtracted, the 161 tangent vectors), then optim_es at (px, py) = (pi, 0)
+    over the whole basis and evaluate_es.  Reports the seconds per momentum
+    (momenta/s) and the lowest four band energies."""
+    import torch
+    pkg = load_pkg()
+    eng = pkg.Engine(0)
+    H = heisenberg(1.0)
+    A0 = random_A(3, 2, seed=21)
+    cfg = pkg.default_config()
+    cfg.update(chi=48, min_iter=4, max_iter=40, rg_tol=1e-8, ad_max_iter=4)
+    r = pkg.drivers.optim_gs(H, A0, dict(cfg), iterations=args.es_gs_steps, engine=eng)
+    ts, H2, basis = pkg.drivers.prepare_basis(H, r["A"], dict(cfg), engine=eng)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    effH, effN = pkg.drivers.optim_es(1.0, 0.0, ts, H2, basis)
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    es = pkg.drivers.evaluate_es(effH, effN, 1e-3)
+    print(json.dumps({"es_momentum": "heisenberg D=3 d=2 chi=48, (px, py) = (pi, 0)", "basis_vectors": int(basis.shape[1]),
+                      "gs_lbfgs_steps": args.es_gs_steps, "E_gs": r["energies"][-1],
+                      "seconds_per_momentum": round(dt, 2), "momenta_per_s": 1.0 / dt,
+                      "get_es_grad_per_s": basis.shape[1] / dt,
+                      "lowest_bands": [float(x) for x in es[:4]]}), flush=True)
+    ts.close()
+    eng.close()
+    return 0
+
+
 def run_tf32_shapes():
     """ipeps_gemm_tf32x3 (3xTF32 on tcgen05: operand splits + GEMM, device time
     by CUDA events, mean over 10 repetitions) on the engine's shapes; credited
@@ -743,6 +808,11 @@ def main():
                     help="kernel aid: 3xTF32 tcgen05 GEMM throughput (splits included) on the engine's shapes")
     ap.add_argument("--projector-shapes", action="store_true",
                     help="kernel aid: the projector alone on synthetic enlarged corners of the workload's size")
+    ap.add_argument("--optim-gs", type=int, default=0, metavar="STEPS",
+                    help="workload aid: optim_gs (L-BFGS) for STEPS steps in each form, evals/s and final energies")
+    ap.add_argument("--es-momentum", action="store_true",
+                    help="workload aid: one excited-state momentum over the whole tangent basis (D=3 chi=48)")
+    ap.add_argument("--es-gs-steps", type=int, default=10, help="L-BFGS steps of the ground state for --es-momentum")
     ap.add_argument("--pullback-profile", action="store_true",
                     help="profiling aid: one E+grad pullback of the workload alone, between cudaProfilerStart/Stop")
     args = ap.parse_args()
@@ -750,6 +820,12 @@ def main():
     if args.projector_shapes:
         WORKLOAD = WORKLOADS[args.workload]
         return run_projector_shapes()
+    if args.optim_gs > 0:
+        WORKLOAD = WORKLOADS[args.workload]
+        WORKLOAD_NAME = workload_name(WORKLOAD)
+        return run_optim_gs(args)
+    if args.es_momentum:
+        return run_es_momentum(args)
     if args.pullback_profile:
         WORKLOAD = WORKLOADS[args.workload]
         WORKLOAD_NAME = workload_name(WORKLOAD)
