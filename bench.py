@@ -713,14 +713,18 @@ def run_es_momentum(args):
     cfg.update(chi=48, min_iter=4, max_iter=40, rg_tol=1e-8, ad_max_iter=4)
     r = pkg.drivers.optim_gs(H, A0, dict(cfg), iterations=args.es_gs_steps, engine=eng)
     ts, H2, basis = pkg.drivers.prepare_basis(H, r["A"], dict(cfg), engine=eng)
+    workers = [pkg.Engine(0) for _ in range(max(args.es_workers, 1) - 1)]
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    effH, effN = pkg.drivers.optim_es(1.0, 0.0, ts, H2, basis)
+    effH, effN = pkg.drivers.optim_es(1.0, 0.0, ts, H2, basis, engines=([eng] + workers) if workers else None)
     torch.cuda.synchronize()
     dt = time.perf_counter() - t0
+    for w in workers:
+        w.close()
     es = pkg.drivers.evaluate_es(effH, effN, 1e-3)
     print(json.dumps({"es_momentum": "heisenberg D=3 d=2 chi=48, (px, py) = (pi, 0)", "basis_vectors": int(basis.shape[1]),
                       "gs_lbfgs_steps": args.es_gs_steps, "E_gs": r["energies"][-1],
+                      "contexts": max(args.es_workers, 1),
                       "seconds_per_momentum": round(dt, 2), "momenta_per_s": 1.0 / dt,
                       "get_es_grad_per_s": basis.shape[1] / dt,
                       "lowest_bands": [float(x) for x in es[:4]]}), flush=True)
@@ -813,6 +817,8 @@ def main():
     ap.add_argument("--es-momentum", action="store_true",
                     help="workload aid: one excited-state momentum over the whole tangent basis (D=3 chi=48)")
     ap.add_argument("--es-gs-steps", type=int, default=10, help="L-BFGS steps of the ground state for --es-momentum")
+    ap.add_argument("--es-workers", type=int, default=4,
+                    help="contexts (streams, host threads) running --es-momentum's basis vectors concurrently")
     ap.add_argument("--pullback-profile", action="store_true",
                     help="profiling aid: one E+grad pullback of the workload alone, between cudaProfilerStart/Stop")
     args = ap.parse_args()

@@ -236,12 +236,14 @@ def evaluate_es(effH: np.ndarray, effN: np.ndarray, nrmB_cut=1e-3):
     return np.sort(es.real)
 
 
-def es_column(px: float, py: float, ts: host.CTMTensors, H, basis: np.ndarray, i: int, C=None):
+def es_column(px: float, py: float, ts: host.CTMTensors, H, basis: np.ndarray, i: int, C=None,
+              engine: Optional[host.Engine] = None):
     """One basis vector of optim_es (optim_es.jl:127-153): a nested
     environment started from the ground-state C/T, the pullback w.r.t. B
-    (get_es_grad), projected on the basis: (effH[:, i], effN[:, i])."""
+    (get_es_grad), projected on the basis: (effH[:, i], effN[:, i]).  engine:
+    the context to run it on (default: the one holding ts)."""
     C = C if C is not None else [ts.get_CT(k) for k in range(1, 5)]
-    t = host.CTMTensors(ts.A, dict(ts.Params), engine=ts.engine, init=False)
+    t = host.CTMTensors(ts.A, dict(ts.Params), engine=engine or ts.engine, init=False)
     try:
         for k in range(4):
             t.set_CT(k + 1, *C[k])
@@ -253,19 +255,53 @@ def es_column(px: float, py: float, ts: host.CTMTensors, H, basis: np.ndarray, i
 
 
 def optim_es(px: float, py: float, ts: host.CTMTensors, H, basis: np.ndarray,
-             indices: Optional[List[int]] = None):
+             indices: Optional[List[int]] = None, engines: Optional[List[host.Engine]] = None):
     """optim_es (optim_es.jl:91-165) for one momentum (px, py in units of pi).
 
     ts: normalised ground-state environment (copied per basis vector from its
     C/T), H: Hamiltonian with E0/2 subtracted, basis: (D^4 d, nb) complex.
-    indices: which basis columns to compute (all by default).  Returns (effH,
-    effN) with those columns filled (others zero)."""
+    indices: which basis columns to compute (all by default).  engines: more
+    contexts on the same GPU (each with its own stream) to run the independent
+    basis vectors concurrently, one host thread per context (the library
+    releases the interpreter lock during its calls); the columns do not depend
+    on which context computed them beyond the projectors' random sketches.
+    Returns (effH, effN) with those columns filled (others zero)."""
     nb = basis.shape[1]
     effH = np.zeros((nb, nb), dtype=np.complex128)
     effN = np.zeros((nb, nb), dtype=np.complex128)
     C = [ts.get_CT(k) for k in range(1, 5)]
-    for i in (range(nb) if indices is None else indices):
-        effH[:, i], effN[:, i] = es_column(px, py, ts, H, basis, i, C)
+    cols = list(range(nb) if indices is None else indices)
+    if not engines:
+        for i in cols:
+            effH[:, i], effN[:, i] = es_column(px, py, ts, H, basis, i, C)
+        return effH, effN
+    import threading
+    lock = threading.Lock()
+    queue = list(cols)
+
+    errors = []
+
+    def worker(eng):
+        while True:
+            with lock:
+                if not queue or errors:
+                    return
+                i = queue.pop(0)
+            try:
+                h, n = es_column(px, py, ts, H, basis, i, C, engine=eng)
+            except BaseException as exc:  # re-raised in the calling thread
+                with lock:
+                    errors.append(exc)
+                return
+            effH[:, i], effN[:, i] = h, n
+
+    threads = [threading.Thread(target=worker, args=(e,)) for e in engines]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    if errors:
+        raise errors[0]
     return effH, effN
 
 

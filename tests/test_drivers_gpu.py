@@ -65,6 +65,30 @@ def test_optim_es_band_energies_match_oracle(engine, pkg):
     ts.close()
 
 
+def test_optim_es_concurrent_contexts_match_oracle(engine, pkg):
+    """optim_es with its basis vectors spread over three contexts (own streams,
+    host threads) on one GPU: the same band energies as the oracle (1e-6)."""
+    with open(os.path.join(GOLD, "es_d2.json")) as f:
+        g = json.load(f)
+    A = O.random_A(g["D"], g["d"], seed=g["seed"]).numpy()
+    H = [h.numpy() for h in O.heisenberg(1.0)]
+    cfg = pkg.default_config()
+    cfg.update(chi=g["chi"], **g["cfg"])
+    ts, H2, basis = pkg.drivers.prepare_basis(H, A, cfg, engine=engine)
+    extra = [pkg.Engine(0), pkg.Engine(0)]
+    try:
+        effH, effN = pkg.drivers.optim_es(g["px"], g["py"], ts, H2, basis, engines=[engine] + extra)
+    finally:
+        for e in extra:
+            e.close()
+    assert np.all(np.abs(effN).sum(axis=0) > 0)  # every column computed
+    es = pkg.drivers.evaluate_es(effH, effN, g["nrmB_cut"])
+    eo = np.asarray(g["es"])
+    assert len(es) == len(eo)
+    assert np.allclose(es, eo, rtol=1e-6, atol=1e-6), (es[:4], eo[:4])
+    ts.close()
+
+
 @pytest.mark.parametrize("direction", ["h", "v"])
 def test_correlation_TM_matches_oracle(engine, pkg, direction):
     """correlation_TM (expectation.jl:193-220): the leading transfer-matrix
