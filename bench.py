@@ -644,8 +644,10 @@ def run_pullback_profile(args):
     eng.check(eng.lib.ipeps_env_init(t.h))
     pkg.run_ctm(t, conv_fun="energy", H=H)
     eng.prof_enable(True)
+    eng.prof_phases()
     pkg.energy_grad(t, H, ad_iters)
     prof = eng.prof_query()
+    phases = eng.prof_phases()
     eng.prof_enable(False)
     t.close()
     t = fresh()
@@ -658,7 +660,8 @@ def run_pullback_profile(args):
                       "launches": int(sum(f["launches"] for f in st["families"].values())),
                       "projector": {k: st[k] for k in ("projector_calls", "extra_passes", "resid_misses",
                                                        "series_terms", "series_retries", "series_cap_hits")},
-                      "families_ms_serialised": {k: round(v["ms"], 3) for k, v in prof.items() if v["ms"] > 0}}),
+                      "families_ms_serialised": {k: round(v["ms"], 3) for k, v in prof.items() if v["ms"] > 0},
+                      "phases_ms_profiled": {k: round(v, 2) for k, v in phases.items()}}),
           flush=True)
     eng.close()
     return 0

@@ -83,6 +83,10 @@ IPEPS_API int ipeps_ctx_stream(ipeps_ctx* ctx, void** stream);
  * credited flops / bytes per family since enabling (query clears the window) */
 IPEPS_API int ipeps_prof_enable(ipeps_ctx* ctx, int on);
 IPEPS_API int ipeps_prof_query(ipeps_ctx* ctx, double* ms, uint64_t* launches, double* flops, double* bytes);
+/* While profiling is enabled: wall ms of the E+grad pullback's phases since the last call
+ * (ms[5]: checkpoint iterations, energy tape, recorded recomputation of the iterations, their
+ * backward, the projector adjoints inside that backward), then cleared. */
+IPEPS_API int ipeps_prof_phases(ipeps_ctx* ctx, double* ms);
 
 /* ---- contraction operator: tcon(ind_xs, ind_y, A, B) (src/utility/wrapper.jl:15-23).
  * la/lb: labels per leg (positive = summed, negative -1..-n = output order).

@@ -5,6 +5,7 @@
 #include "moves.cuh"
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 
 namespace ipeps {
@@ -707,7 +708,14 @@ void ad_projector(Tape& tp, const AV& R1, bool t1, const AV& R2, bool t2, const 
     const Tensor &g1 = tp.grad(o1), &g2 = tp.grad(o2);
     if (g1.empty() && g2.empty()) return;
     Tensor dR1, dR2;
-    projector_backward(tp.ctx(), R1t, t1, R2t, t2, prc, P1t, P2t, g1, g2, &dR1, &dR2);
+    Ctx& cx = tp.ctx();
+    if (cx.prof) cx.sync();
+    const auto t0 = std::chrono::steady_clock::now();
+    projector_backward(cx, R1t, t1, R2t, t2, prc, P1t, P2t, g1, g2, &dR1, &dR2);
+    if (cx.prof) {
+      cx.sync();
+      cx.ad_phase_ms[4] += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
     tp.acc(i1, dR1);
     tp.acc(i2, dR2);
   });
@@ -759,8 +767,29 @@ Tensor scalar_seed(Ctx& c, const Tensor& like, std::complex<double> v) {
 
 }  // namespace
 
+namespace {
+// wall-clock phase timer of the pullback, active only while profiling (it
+// synchronises the stream at each mark)
+struct PhaseClock {
+  Ctx& c;
+  std::chrono::steady_clock::time_point t = std::chrono::steady_clock::now();
+  explicit PhaseClock(Ctx& cc) : c(cc) {
+    if (c.prof) c.sync();
+    t = std::chrono::steady_clock::now();
+  }
+  void mark(int phase) {
+    if (!c.prof) return;
+    c.sync();
+    const auto t1 = std::chrono::steady_clock::now();
+    c.ad_phase_ms[size_t(phase)] += std::chrono::duration<double, std::milli>(t1 - t).count();
+    t = t1;
+  }
+};
+}  // namespace
+
 double energy_grad(Env& e, const Tensor& Hh, const Tensor& Hv, int ad_iters, Tensor* gA, const H4* h4) {
   Ctx& c = *e.ctx;
+  PhaseClock clock(c);
   IPEPS_CHECK(e.dt == DType::F64 && !e.nested, "energy_grad: real single-site A only");
   // The pullback runs in FP64 in both forms.  Measured at Heisenberg D=5
   // chi=100: with 3xTF32 contractions in the tape's backward (checkpoints and
@@ -815,6 +844,7 @@ double energy_grad(Env& e, const Tensor& Hh, const Tensor& Hv, int ad_iters, Ten
   }
   e.prm.svd.resid_tol = resid_tol0;
   e.prm.svd.max_extra_passes = max_extra0;
+  clock.mark(0);
   // energy on a tape (evaluation.jl:15-29)
   std::array<Tensor, 4> gC, gE;
   Tensor gAcc, gAdc;
@@ -883,6 +913,7 @@ double energy_grad(Env& e, const Tensor& Hh, const Tensor& Hv, int ad_iters, Ten
     gAdc = tp.grad(Ad.id);
     }
   }
+  clock.mark(1);
   // reverse over the iterations, recomputing each on a tape
   for (int it = int(ck.size()) - 1; it >= 0; --it) {
     Tape tp(c);
@@ -909,7 +940,9 @@ double energy_grad(Env& e, const Tensor& Hh, const Tensor& Hv, int ad_iters, Ten
       tp.acc(C[i].id, gC[i]);
       tp.acc(E[i].id, gE[i]);
     }
+    clock.mark(2);
     tp.backward();
+    clock.mark(3);
     for (int i = 0; i < 4; ++i) {
       gC[i] = tp.grad(leafC[i].id);
       gE[i] = tp.grad(leafE[i].id);

@@ -193,6 +193,15 @@ int ipeps_prof_query(ipeps_ctx* ctx, double* ms, uint64_t* launches, double* flo
   });
 }
 
+int ipeps_prof_phases(ipeps_ctx* ctx, double* ms) {
+  return guarded(ctx, [&] {
+    IPEPS_CHECK(ms, "null output");
+    for (int i = 0; i < 5; ++i) ms[i] = ctx->c->ad_phase_ms[size_t(i)];
+    ctx->c->ad_phase_ms = {};
+    return IPEPS_OK;
+  });
+}
+
 int ipeps_tcon(ipeps_ctx* ctx, int is_complex, const double* A, int nA, const int64_t* dimsA, const int* la,
                const double* B, int nB, const int64_t* dimsB, const int* lb, double* out, int64_t out_cap,
                int64_t* out_dims, int* out_nd) {

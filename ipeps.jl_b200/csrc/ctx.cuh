@@ -61,6 +61,10 @@ struct Ctx {
   int* d_status = nullptr;
   // per-kernel-family CUDA-event timing (enabled by ipeps_prof_enable)
   bool prof = false;
+  // with prof: wall ms of the E+grad pullback's phases (checkpoint iterations,
+  // energy tape, recorded recomputation of the iterations, their backward,
+  // and the projector adjoints inside that backward), stream-synchronised
+  std::array<double, 5> ad_phase_ms{};
   std::array<KStat, int(KFam::Count)> prof_stats{};
   std::vector<std::tuple<int, cudaEvent_t, cudaEvent_t>> prof_rec;
   std::vector<cudaEvent_t> ev_pool;

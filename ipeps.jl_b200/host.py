@@ -40,7 +40,7 @@ EXPORTED = [
     "ipeps_env_get_CT", "ipeps_env_set_CT", "ipeps_ctm_move", "ipeps_ctm_step", "ipeps_ctm_run",
     "ipeps_ctm_log", "ipeps_energy", "ipeps_gs_norm", "ipeps_nested_set_B", "ipeps_es_energy",
     "ipeps_all_norm", "ipeps_tcon", "ipeps_projector", "ipeps_projector_c", "ipeps_ctx_stream", "ipeps_prof_enable",
-    "ipeps_prof_query", "ipeps_energy_grad", "ipeps_env_set_mixed", "ipeps_es_energy_grad",
+    "ipeps_prof_query", "ipeps_prof_phases", "ipeps_energy_grad", "ipeps_env_set_mixed", "ipeps_es_energy_grad",
     "ipeps_single_dm_Ad", "ipeps_wp_grad", "ipeps_energy_4x4", "ipeps_ctm_run_4x4", "ipeps_energy_grad_4x4", "ipeps_es_energy_grad_4x4", "ipeps_gemm_f64", "ipeps_gemm_tf32x3", "ipeps_orth", "ipeps_gemm_bf16", "ipeps_mlp_create", "ipeps_mlp_destroy", "ipeps_mlp_num_params",
     "ipeps_mlp_get_params", "ipeps_mlp_set_params", "ipeps_mlp_forward", "ipeps_mlp_grad", "ipeps_mlp_train_step",
 ]
@@ -123,6 +123,7 @@ def load_library(path: str = LIB_PATH) -> ct.CDLL:
         "ipeps_ctx_stream": [P, ct.POINTER(P)],
         "ipeps_prof_enable": [P, I],
         "ipeps_prof_query": [P, dp, ct.POINTER(ct.c_uint64), dp, dp],
+        "ipeps_prof_phases": [P, dp],
         "ipeps_energy_grad": [P, dp, dp, I, I, dp, dp],
         "ipeps_env_set_mixed": [P, I, D],
         "ipeps_es_energy_grad": [P, dp, dp, I, I, dp, dp],
@@ -204,6 +205,13 @@ class Engine:
 
     def prof_enable(self, on: bool = True):
         self.check(self.lib.ipeps_prof_enable(self.h, int(on)))
+
+    def prof_phases(self) -> Dict[str, float]:
+        """Wall ms of the pullback's phases while profiling (then cleared)."""
+        ms = np.zeros(5)
+        self.check(self.lib.ipeps_prof_phases(self.h, _dp(ms)))
+        return dict(zip(["checkpoint_iterations", "energy_tape", "recompute_on_tapes", "backward",
+                         "projector_adjoints_in_backward"], [float(x) for x in ms]))
 
     def prof_query(self) -> Dict[str, Dict[str, float]]:
         ms = np.zeros(8)
