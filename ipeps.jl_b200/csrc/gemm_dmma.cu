@@ -208,11 +208,11 @@ void launch_cfg(Ctx& c, int64_t m, int64_t n, int64_t k, double alpha, const dou
   IPEPS_CHECK(gy <= 65535, "gemm: n too large for grid");
   const int64_t tiles = gx * gy;
   int S = 1;
-  // split K when the output grid covers well under two waves and K is long:
-  // up to two waves of CTAs in total (a 64 x 64 output with K ~ 1e5, the
-  // gradient of A, would otherwise run on a few dozen SMs), at least 8 K
-  // blocks per split
-  const int64_t target = 2LL * c.sm_count;
+  // split K when the output grid covers well under four CTAs per SM and K is
+  // long: up to four per SM in total (a 64 x 64 output with K ~ 1e5, the
+  // gradient of A, would otherwise run on a few dozen SMs; finer splits also
+  // even out the last wave), at least 8 K blocks per split
+  const int64_t target = 4LL * c.sm_count;
   if (tiles < target && k >= 16 * kBK) {
     const int64_t want = (target + tiles - 1) / tiles;
     const int64_t maxs = k / (8 * kBK);
