@@ -548,8 +548,9 @@ def run_ours(args):
 
 
 def run_gemm_shapes():
-    """ipeps_gemm_f64 (10 products from one input upload, timed as the difference
-    of 11 and 1 products) against torch.matmul (cuBLAS DGEMM, CUDA events)."""
+    """ipeps_gemm_f64 (10 products from one input upload; device time of the
+    GEMM family by the engine's CUDA-event profile, split-K sums included)
+    against torch.matmul (cuBLAS DGEMM, CUDA events)."""
     import numpy as np
     import torch
     pkg = load_pkg()
@@ -562,14 +563,12 @@ def run_gemm_shapes():
     for oa, ob, m, n, k in shapes:
         A = rng.standard_normal((m, k) if oa == "N" else (k, m))
         B = rng.standard_normal((k, n) if ob == "N" else (n, k))
-        for _ in range(2):  # the second round is the timed one
-            ts = []
-            for reps in (1, 11):
-                torch.cuda.synchronize()
-                t0 = time.perf_counter()
-                pkg.host.gemm_f64(oa, ob, A, B, engine=eng, reps=reps)
-                ts.append(time.perf_counter() - t0)
-        dt = (ts[1] - ts[0]) / 10
+        pkg.host.gemm_f64(oa, ob, A, B, engine=eng, reps=2)  # warm-up
+        eng.prof_enable(True)
+        pkg.host.gemm_f64(oa, ob, A, B, engine=eng, reps=10)
+        pr = eng.prof_query()
+        eng.prof_enable(False)
+        dt = (pr["gemm_f64"]["ms"] + pr["reduce"]["ms"]) / 10 / 1e3
         a, b = torch.tensor(A, device="cuda"), torch.tensor(B, device="cuda")
         fa = (lambda x: x) if oa == "N" else (lambda x: x.T)
         fb = (lambda x: x) if ob == "N" else (lambda x: x.T)
