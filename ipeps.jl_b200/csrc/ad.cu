@@ -523,8 +523,23 @@ void projector_backward(Ctx& c, const Tensor& R1t, bool t1, const Tensor& R2t, b
     Tensor Mx = c.alloc(DType::F64, {N1, N2});
     gemm(c, DType::F64, t1 ? 'T' : 'N', t2 ? 'T' : 'N', N1, N2, K1, cplx(1), R1t.data(), R1t.dims[0], R2t.data(),
          R2t.dims[0], cplx(0), Mx.data(), N1);
-    auto Bu_of = [&](const Tensor& T) { return project_out(c, Ur, mm(c, Mx, 'N', mm(c, Mx, 'T', T, 'N'), 'N')); };
-    auto Bv_of = [&](const Tensor& T) { return project_out(c, Vr, mm(c, Mx, 'T', mm(c, Mx, 'N', T, 'N'), 'N')); };
+    // M_P = (1 - U_r U_r^T) M (1 - V_r V_r^T), formed once.  For vectors in the
+    // complement, P M M^T P = M_P M_P^T + (P M V_r)(P M V_r)^T, and P M V_r is
+    // the resolved triplets' residual (<= 1e-10 s_1 each), so B = M_P M_P^T
+    // (resp. M_P^T M_P) up to ~1e-20 s_1^2 and keeps the complement by
+    // construction: the expansion's terms need no projection.
+    Tensor MP = clone(c, Mx);
+    {
+      const int64_t rr = Ur.dims[1];
+      Tensor C1 = mm(c, Ur, 'T', Mx, 'N', true);  // rr x N2
+      gemm(c, DType::F64, 'N', 'N', N1, N2, rr, cplx(-1), Ur.data(), N1, C1.data(), rr, cplx(1), MP.data(), N1,
+           true);
+      Tensor C2 = mm(c, MP, 'N', Vr, 'N', true);  // N1 x rr
+      gemm(c, DType::F64, 'N', 'T', N1, N2, rr, cplx(-1), C2.data(), N1, Vr.data(), N2, cplx(1), MP.data(), N1,
+           true);
+    }
+    auto Bu_of = [&](const Tensor& T) { return mm(c, MP, 'N', mm(c, MP, 'T', T, 'N', true), 'N', true); };
+    auto Bv_of = [&](const Tensor& T) { return mm(c, MP, 'T', mm(c, MP, 'N', T, 'N', true), 'N', true); };
     bool series_done = (ny0 == 0.0);
     if (!series_done) {
       // b: above the sketch's s_next^2 and a power-iteration estimate of the
@@ -557,7 +572,8 @@ void projector_backward(Ctx& c, const Tensor& R1t, bool t1, const Tensor& R2t, b
       // 2n columns: W1 = M^T [T_u | M T_v] = [M^T T_u | M^T M T_v], then, with the
       // next v-side vector T_v' formed from the second half,
       // W2 = M [M^T T_u | T_v'] = [M M^T T_u | M T_v'], whose second half feeds the
-      // next term.  B~ T = (2/b) P (...) - T, T_{m+1} = 2 B~ T_m - T_{m-1}.
+      // next term (with M_P in place of M).  B~ T = (2/b) B T - T,
+      // T_{m+1} = 2 B~ T_m - T_{m-1}.
       Tensor W1 = c.alloc(DType::F64, {N2, 2 * int64_t(n)}), W2 = c.alloc(DType::F64, {N1, 2 * int64_t(n)});
       auto next_T = [&](Tensor& B, const Tensor& T, const Tensor& Tprev, int m) {
         axpby_kernel<<<gridn(c, B.numel()), 256, 0, c.stream>>>(-1.0, T.f64(), 2.0 / b, B.f64(), B.numel());
@@ -567,15 +583,15 @@ void projector_backward(Ctx& c, const Tensor& R1t, bool t1, const Tensor& R2t, b
       auto apply_B = [&](const Tensor& Tu, const Tensor& Tv, const Tensor& Pu, const Tensor& Pv, int m, Tensor* Bu,
                          Tensor* Bv) {
         IPEPS_CUDA(cudaMemcpyAsync(W2.data(), Tu.data(), size_t(N1) * n * 8, cudaMemcpyDeviceToDevice, c.stream));
-        gemm(c, DType::F64, 'T', 'N', N2, 2 * n, N1, cplx(1), Mx.data(), N1, W2.data(), N1, cplx(0), W1.data(), N2,
+        gemm(c, DType::F64, 'T', 'N', N2, 2 * n, N1, cplx(1), MP.data(), N1, W2.data(), N1, cplx(0), W1.data(), N2,
              true);
-        *Bv = project_out(c, Vr, cols(W1, n, n));
-        next_T(*Bv, Tv, Pv, m);
-        IPEPS_CUDA(cudaMemcpyAsync(cols(W1, n, n).data(), Bv->data(), size_t(N2) * n * 8, cudaMemcpyDeviceToDevice,
-                                   c.stream));
-        gemm(c, DType::F64, 'N', 'N', N1, 2 * n, N2, cplx(1), Mx.data(), N1, W1.data(), N2, cplx(0), W2.data(), N1,
+        // the next v-side vector in place (it feeds the second product), and a copy to keep
+        Tensor zv = cols(W1, n, n);
+        next_T(zv, Tv, Pv, m);
+        *Bv = clone(c, zv);
+        gemm(c, DType::F64, 'N', 'N', N1, 2 * n, N2, cplx(1), MP.data(), N1, W1.data(), N2, cplx(0), W2.data(), N1,
              true);
-        *Bu = project_out(c, Ur, cols(W2, 0, n));
+        *Bu = clone(c, cols(W2, 0, n));
         next_T(*Bu, Tu, Pu, m);
       };
       // relative residual of ((s_i^2 - B)^2 + eta) X_i = (s_i^2 - B) Y_i over all columns of one side
@@ -595,8 +611,8 @@ void projector_backward(Ctx& c, const Tensor& R1t, bool t1, const Tensor& R2t, b
         Tensor Pu = Yu0, Pv = Yv0;  // T_{m-1}
         Tensor Tu = Yu0, Tv = Yv0;  // T_m
         bool blew_up = false, converged = false;
-        // M T_v of the first term, in the second half of W2
-        gemm(c, DType::F64, 'N', 'N', N1, n, N2, cplx(1), Mx.data(), N1, Tv.data(), N2, cplx(0),
+        // M_P T_v of the first term, in the second half of W2
+        gemm(c, DType::F64, 'N', 'N', N1, n, N2, cplx(1), MP.data(), N1, Tv.data(), N2, cplx(0),
              cols(W2, n, n).data(), N1, true);
         for (int m = 0; m < kMaxTerms; ++m) {
           cheb_acc_kernel<<<gridn(c, N1 * n), 256, 0, c.stream>>>(Xu.f64(), Tu.f64(), N1, n, s.f64(), kSvdEta, b, m);
