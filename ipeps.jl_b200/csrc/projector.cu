@@ -203,10 +203,6 @@ struct RealOps {
   // else at most 160 (the widest sketch whose Jacobi fits in shared memory)
   int width(int want, int kw, const SvdParams& sp) const {
     if (kw > 128 && want + std::max(sp.min_oversample, want / 2) <= 128) return 128;
-    // the mixed form's 3xTF32 iterations (residual tolerance ~1e-6 s_1, seeded
-    // sketches) oversample by a quarter: k = 128 at chi = 100 instead of 160,
-    // about half the Jacobi SVD's work and a fifth less of the Cholesky's
-    if (c.precision == kPrecMixed && kw > 128 && want + std::max(sp.min_oversample, want / 4) <= 128) return 128;
     if (kw > 160 && want + sp.min_oversample <= 160) return 160;
     return kw;
   }
