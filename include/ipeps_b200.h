@@ -60,7 +60,7 @@ typedef struct {
   uint64_t jacobi_sweeps;   /* one-sided Jacobi sweeps summed over those projectors */
   uint64_t extra_passes;    /* extra power iterations triggered by the residual check */
   uint64_t series_cap_hits; /* projector adjoints whose Chebyshev expansion of the broadened
-                               resolvent hit its 160-term cap before its 1e-13 tolerance
+                               resolvent hit its 160-term cap before its 1e-11 tolerance
                                (gradient possibly inexact) */
   uint64_t series_terms;    /* Chebyshev terms summed over all projector adjoints */
   uint64_t series_retries;  /* expansions redone over a wider interval because the resolvent

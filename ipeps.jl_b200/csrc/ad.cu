@@ -513,7 +513,7 @@ void projector_backward(Ctx& c, const Tensor& R1t, bool t1, const Tensor& R2t, b
     const Tensor Yu0 = project_out(c, Ur, dUt), Yv0 = project_out(c, Vr, dVt);
     double* d_cmax = reinterpret_cast<double*>(c.scal->p) + 40;
     constexpr int kMaxTerms = 160;
-    constexpr double kTol = 1e-13;
+    constexpr double kTol = 1e-11;
     constexpr double kCheckTol = 1e-10;
     constexpr int kCheckEvery = 4;
     const double ny0 = std::sqrt(dot_host(c, Yu0, Yu0) + dot_host(c, Yv0, Yv0));
@@ -575,6 +575,7 @@ void projector_backward(Ctx& c, const Tensor& R1t, bool t1, const Tensor& R2t, b
       // next term (with M_P in place of M).  B~ T = (2/b) B T - T,
       // T_{m+1} = 2 B~ T_m - T_{m-1}.
       Tensor W1 = c.alloc(DType::F64, {N2, 2 * int64_t(n)}), W2 = c.alloc(DType::F64, {N1, 2 * int64_t(n)});
+      Tensor BYu, BYv;
       auto next_T = [&](Tensor& B, const Tensor& T, const Tensor& Tprev, int m) {
         axpby_kernel<<<gridn(c, B.numel()), 256, 0, c.stream>>>(-1.0, T.f64(), 2.0 / b, B.f64(), B.numel());
         if (m > 0) axpby_kernel<<<gridn(c, B.numel()), 256, 0, c.stream>>>(-1.0, Tprev.f64(), 2.0, B.f64(), B.numel());
@@ -587,17 +588,19 @@ void projector_backward(Ctx& c, const Tensor& R1t, bool t1, const Tensor& R2t, b
              true);
         // the next v-side vector in place (it feeds the second product), and a copy to keep
         Tensor zv = cols(W1, n, n);
+        if (m == 0) BYv = clone(c, zv);  // B Y_0 on the v side, for the resolvent check
         next_T(zv, Tv, Pv, m);
         *Bv = clone(c, zv);
         gemm(c, DType::F64, 'N', 'N', N1, 2 * n, N2, cplx(1), MP.data(), N1, W1.data(), N2, cplx(0), W2.data(), N1,
              true);
         *Bu = clone(c, cols(W2, 0, n));
+        if (m == 0) BYu = clone(c, *Bu);  // B Y_0 on the u side
         next_T(*Bu, Tu, Pu, m);
       };
       // relative residual of ((s_i^2 - B)^2 + eta) X_i = (s_i^2 - B) Y_i over all columns of one side
-      auto check = [&](const Tensor& X, const Tensor& Y, bool u_side) {
+      auto check = [&](const Tensor& X, const Tensor& Y, const Tensor& BY, bool u_side) {
         auto B = [&](const Tensor& T) { return u_side ? Bu_of(T) : Bv_of(T); };
-        const Tensor BX = B(X), BBX = B(BX), BY = B(Y);
+        const Tensor BX = B(X), BBX = B(BX);
         Tensor res = c.alloc(DType::F64, X.shape()), rhs = c.alloc(DType::F64, X.shape());
         resolvent_check_kernel<<<gridn(c, X.numel()), 256, 0, c.stream>>>(
             X.f64(), BX.f64(), BBX.f64(), Y.f64(), BY.f64(), s.f64(), kSvdEta, X.dims[0], n, res.f64(), rhs.f64());
@@ -648,7 +651,7 @@ void projector_backward(Ctx& c, const Tensor& R1t, bool t1, const Tensor& R2t, b
           Tu = Bu;
           Tv = Bv;
         }
-        if (converged && std::max(check(Xu, Yu0, true), check(Xv, Yv0, false)) <= kCheckTol) {
+        if (converged && std::max(check(Xu, Yu0, BYu, true), check(Xv, Yv0, BYv, false)) <= kCheckTol) {
           series_done = true;
           break;
         }
