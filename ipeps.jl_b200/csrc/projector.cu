@@ -352,9 +352,22 @@ ProjResult projector_impl(Ctx& c, Ops& o, int chi, const SvdParams& sp, ProjCach
   // on top of its power iteration; doing the iterations up front is cheaper).
   // Only with sCholQR3 intermediates: a single shifted pass drops directions
   // below ~sqrt(shift) s_1 at every iteration, so more iterations would lose them.
+  // residual tolerance of this call (the mixed form's 3xTF32 iterations settle
+  // for the FP32-level floor of their products)
+  const double rtol = (c.precision == kPrecMixed && dt == DType::F64) ? std::max(sp.resid_tol, sp.resid_tol_mixed)
+                                                                       : sp.resid_tol;
+  // seeds resolved to a looser tolerance than this call's (the first FP64
+  // iterations after the mixed form's 3xTF32 ones, the adjoint's checkpoint
+  // iterations at 1e-12): one power iteration per factor ~7 of the residual,
+  // done up front with sCholQR3 intermediates, instead of as extra passes
+  if (warm && q > 0 && cache->seed_tol(sp.seed_older) > 10.0 * rtol) {
+    inter = std::max(inter, 3);
+    q += std::min(6, int(std::ceil(std::log(cache->seed_tol(sp.seed_older) / rtol) / std::log(7.0))));
+  }
   const bool adapt = q > 0 && cache && inter >= 3;
   if (adapt) q += cache->qbonus;
   int extra = 0;
+  double res_final = 1.0;
 
   ProjResult r;
   r.k = k;
@@ -401,7 +414,10 @@ ProjResult projector_impl(Ctx& c, Ops& o, int chi, const SvdParams& sp, ProjCach
     gather_cols(c, sk.J.f64(), w * k, w * k, d_perm, k, nullptr, 0, Js.f64(), w * k);
     Vk = c.alloc(dt, {N2, k});
     gemm(c, dt, 'N', 'N', N2, k, k, cplx(1), sk.Q2.data(), N2, Js.data(), k, cplx(0), Vk.data(), N2, true);
-    if (q == 0 && k == Nmin) break;  // the sketch spans a whole side of M: exact
+    if (q == 0 && k == Nmin) {  // the sketch spans a whole side of M: exact
+      res_final = 0.0;
+      break;
+    }
     // residual of the kept triplets and the next one: ||M v_i - s_i u_i|| <= resid_tol * s_1.
     // For the adjoint (keep_factors) also the tail down to 0.8 s_n: the adjoint
     // sums those triplets exactly, and the interval of its expansion of the
@@ -425,8 +441,7 @@ ProjResult projector_impl(Ctx& c, Ops& o, int chi, const SvdParams& sp, ProjCach
     c.sync();
     // done when below tolerance, or when it stopped decreasing (the FP64 floor of
     // R1 (R2 v), ~eps ||R1|| ||R2||, can sit above resid_tol * s_1)
-    const double rtol = (c.precision == kPrecMixed && dt == DType::F64) ? std::max(sp.resid_tol, sp.resid_tol_mixed)
-                                                                         : sp.resid_tol;
+    res_final = smax > 0 ? res / smax : 1.0;
     if (res <= rtol * smax) break;
     if (res > 0.5 * prev_res || attempt >= sp.max_extra_passes) {
       c.resid_misses++;
@@ -459,6 +474,8 @@ ProjResult projector_impl(Ctx& c, Ops& o, int chi, const SvdParams& sp, ProjCach
     copy_cols(c, Vc, Vk, N2, rr, w);
     cache->Vold = cache->V;
     cache->V = Vc;
+    cache->tol_old = cache->tol;
+    cache->tol = std::max(res_final, 1e-15);  // the residual these vectors reached
     cache->cutoff_limited = n_above_last < new_chi;
     if (adapt)
       cache->qbonus = extra > 0 ? std::min(cache->qbonus + extra, sp.max_extra_passes) : std::max(cache->qbonus - 1, 0);

@@ -54,7 +54,10 @@ struct ProjCache {
   // power iterations added to the next call's sketch: raised by the extra
   // passes a call needed, lowered by one after a call that needed none
   int qbonus = 0;
+  // residual (relative to s_1) the call that produced V (Vold) reached
+  double tol = 1.0, tol_old = 1.0;
   const Tensor& seed(bool older) const { return (older && !Vold.empty()) ? Vold : V; }
+  double seed_tol(bool older) const { return (older && !Vold.empty()) ? tol_old : tol; }
 };
 
 struct ProjResult {
