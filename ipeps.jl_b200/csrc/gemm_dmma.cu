@@ -184,13 +184,35 @@ __global__ void __launch_bounds__(WGM * WGN * 32)
   }
 }
 
+// Sum of the S split-K partial products (in split order, so the result does
+// not depend on the launch).  Contiguous C (ldc == M) takes two elements per
+// thread with 16-byte loads; the general case one element per thread.
 __global__ void dmma_splitk_reduce(int64_t M, int64_t N, int S, const double* __restrict__ partial, double alpha,
                                    double beta, double* __restrict__ C, int64_t ldc) {
+  const int64_t tot = M * N;
+  if (ldc == M && (tot & 1) == 0 && (reinterpret_cast<uintptr_t>(C) & 15) == 0) {
+    const int64_t i2 = int64_t(blockIdx.x) * blockDim.x + threadIdx.x, idx = 2 * i2;
+    if (idx >= tot) return;
+    double2 acc = *reinterpret_cast<const double2*>(partial + idx);
+    for (int z = 1; z < S; ++z) {
+      const double2 p = *reinterpret_cast<const double2*>(partial + int64_t(z) * tot + idx);
+      acc.x += p.x;
+      acc.y += p.y;
+    }
+    double2 v = make_double2(alpha * acc.x, alpha * acc.y);
+    if (beta != 0.0) {
+      const double2 c = *reinterpret_cast<const double2*>(C + idx);
+      v.x = fma(beta, c.x, v.x);
+      v.y = fma(beta, c.y, v.y);
+    }
+    *reinterpret_cast<double2*>(C + idx) = v;
+    return;
+  }
   const int64_t idx = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (idx >= M * N) return;
-  const int64_t gm = idx % M, gn = idx / M;
+  if (idx >= tot) return;
+  const int64_t gn = idx / M, gm = idx - gn * M;
   double s = partial[idx];
-  for (int z = 1; z < S; ++z) s += partial[int64_t(z) * M * N + idx];
+  for (int z = 1; z < S; ++z) s += partial[int64_t(z) * tot + idx];
   double v = alpha * s;
   if (beta != 0.0) v = fma(beta, C[gm + gn * ldc], v);
   C[gm + gn * ldc] = v;
@@ -229,7 +251,9 @@ void launch_cfg(Ctx& c, int64_t m, int64_t n, int64_t k, double alpha, const dou
   IPEPS_LAUNCH_CHECK();
   if (S > 1) {
     const int64_t tot = m * n;
-    dmma_splitk_reduce<<<unsigned((tot + 255) / 256), 256, 0, c.stream>>>(m, n, S, partial, alpha, beta, C, ldc);
+    const bool pairs = ldc == m && (tot & 1) == 0 && (reinterpret_cast<uintptr_t>(C) & 15) == 0;
+    const int64_t threads = pairs ? tot / 2 : tot;
+    dmma_splitk_reduce<<<unsigned((threads + 255) / 256), 256, 0, c.stream>>>(m, n, S, partial, alpha, beta, C, ldc);
     IPEPS_LAUNCH_CHECK();
     c.count(KFam::Reduce, 0, double(S + 2) * tot * sizeof(double));
   }

@@ -170,7 +170,16 @@ __global__ void permute_rows(RowArgs a, int64_t rows, int64_t nchunk, const T* _
     const T* src = in + off;
     T* dst = out + r * a.n0;
     const int64_t c1 = min(a.n0, c0 + kPermChunk);
-    for (int64_t i = c0 + lane; i < c1; i += 32) dst[i] = src[i];
+    if (sizeof(T) == 8 && ((off | a.n0 | c0) & 1) == 0 &&
+        ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & 15) == 0) {
+      // both runs 16-byte aligned: two doubles per load and store
+      const double2* s2 = reinterpret_cast<const double2*>(src);
+      double2* d2 = reinterpret_cast<double2*>(dst);
+      for (int64_t i = (c0 >> 1) + lane; i < (c1 >> 1); i += 32) d2[i] = s2[i];
+      if ((c1 & 1) && lane == 0) dst[c1 - 1] = src[c1 - 1];
+    } else {
+      for (int64_t i = c0 + lane; i < c1; i += 32) dst[i] = src[i];
+    }
   }
 }
 
