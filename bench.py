@@ -795,6 +795,32 @@ def run_projector_shapes():
     return 0
 
 
+def run_orth_shapes():
+    """The projector's CholeskyQR alone (ipeps_orth, three passes, host buffers)
+    on Gaussian 2500 x k sketches, k = 160, 128, 101: device time per pass of
+    the Cholesky and the triangular solve (the engine's small_linalg family;
+    the Gram product is the gemm_f64 family), the aid behind the Cholesky's
+    ncu summary."""
+    pkg = load_pkg()
+    eng = pkg.Engine(0, precision="fp64")
+    rng = np.random.default_rng(1)
+    for k in (160, 128, 101):
+        Y = rng.standard_normal((2500, k))
+        pkg.orth(Y, 3, engine=eng)  # warm-up (kernel loads, pool)
+        eng.prof_enable(True)
+        reps = 20
+        for _ in range(reps):
+            Q, _ = pkg.orth(Y, 3, engine=eng)
+        prof = eng.prof_query()
+        eng.prof_enable(False)
+        print(json.dumps({"orth": f"N=2500 k={k}", "passes": 3,
+                          "small_linalg_us_per_pass": round(1e3 * prof["small_linalg"]["ms"] / (3 * reps), 2),
+                          "gram_us_per_pass": round(1e3 * prof["gemm_f64"]["ms"] / (3 * reps), 2),
+                          "orthogonality": float(np.abs(Q.T @ Q - np.eye(k)).max())}), flush=True)
+    eng.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -814,6 +840,8 @@ def main():
                     help="kernel aid: 3xTF32 tcgen05 GEMM throughput (splits included) on the engine's shapes")
     ap.add_argument("--projector-shapes", action="store_true",
                     help="kernel aid: the projector alone on synthetic enlarged corners of the workload's size")
+    ap.add_argument("--orth-shapes", action="store_true",
+                    help="kernel aid: the projector's CholeskyQR alone on 2500 x k sketches (k = 160, 128, 101)")
     ap.add_argument("--optim-gs", type=int, default=0, metavar="STEPS",
                     help="workload aid: optim_gs (L-BFGS) for STEPS steps in each form, evals/s and final energies")
     ap.add_argument("--es-momentum", action="store_true",
@@ -828,6 +856,8 @@ def main():
     if args.projector_shapes:
         WORKLOAD = WORKLOADS[args.workload]
         return run_projector_shapes()
+    if args.orth_shapes:
+        return run_orth_shapes()
     if args.optim_gs > 0:
         WORKLOAD = WORKLOADS[args.workload]
         WORKLOAD_NAME = workload_name(WORKLOAD)

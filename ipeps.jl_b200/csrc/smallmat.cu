@@ -222,6 +222,71 @@ size_t chol_ldl_smem_doubles(int k) {
   return npk + 4 * 160 + 2 * 160 + 8;
 }
 
+// Publishes row j (16 JB <= j < 16 JB + 16, held in slot a = JB of the calling
+// warp): a[j][c] (c >= j) into rw, a[j][c] / a[j][j] (c > j) into sc, the
+// pivot into dd[j] (0 for a failed pivot).
+template <int NBB, int JB>
+__device__ __forceinline__ void ldl_publish(const double (&v)[2 * NBB][NBB], int j, int k, int lane, double* rw,
+                                            double* sc, double* dd, double tiny) {
+  constexpr int B0 = JB / 2;
+  // the pivot a[j][j] sits in column block JB / 2 of lane j mod 32
+  const double d = __shfl_sync(kFull, v[JB][B0], j & 31);
+  const bool ok = d > tiny;
+  const double inv = ok ? __drcp_rn(d) : 0.0;
+#pragma unroll
+  for (int b = B0; b < NBB; ++b) {
+    const int c = lane + 32 * b;
+    if (c >= j && c < k) {
+      rw[c] = v[JB][b];
+      if (c > j) sc[c] = v[JB][b] * inv;
+    }
+  }
+  if (lane == 0) dd[j] = ok ? d : 0.0;
+}
+
+// Elimination steps j = 16 JB .. 16 JB + 15 of chol_ldl_kernel, then the next
+// block of 16 (JB is a compile-time constant, so the slots of rows that are
+// finished, a < JB, and of column blocks left of every pivot of the block,
+// 32 b + 31 <= 16 JB, drop out of the code instead of being tested per step).
+// Step j: the warp holding row j (warp j mod 16, slot a = JB) publishes it in
+// shared memory, double-buffered by the parity of j, and after the barrier
+// every slot of a row r > j takes a[r][c] -= a[j][r] (a[j][c] / a[j][j]).
+// Slots left of the diagonal take stale buffer entries and are never read.
+// (Publishing row j + 1 during step j, as soon as its warp has updated it,
+// measured no faster: the steps are bound by the barrier and the shared-memory
+// broadcasts, not by the pivot's reciprocal.)
+template <int NBB, int JB>
+__device__ __forceinline__ void ldl_steps(double (&v)[2 * NBB][NBB], int k, int warp, int lane, double* raw,
+                                          double* scl, double* dd, double tiny) {
+  constexpr int NBA = 2 * NBB, KP = 32 * NBB, B0 = JB / 2;
+  const int tmax = min(16, k - 16 * JB);
+  for (int t = 0; t < tmax; ++t) {
+    const int j = 16 * JB + t;
+    double* rw = raw + (t & 1) * KP;
+    double* sc = scl + (t & 1) * KP;
+    if (warp == t) ldl_publish<NBB, JB>(v, j, k, lane, rw, sc, dd, tiny);
+    __syncthreads();
+    double s[NBB];
+#pragma unroll
+    for (int b = B0; b < NBB; ++b) s[b] = sc[lane + 32 * b];
+    if (warp > t) {  // slot a = JB holds row 16 JB + warp > j
+      const double ra = rw[16 * JB + warp];
+#pragma unroll
+      for (int b = B0; b < NBB; ++b) v[JB][b] = fma(-ra, s[b], v[JB][b]);
+    }
+#pragma unroll
+    for (int a = JB + 1; a < NBA; ++a) {
+      const double ra = rw[warp + 16 * a];
+#pragma unroll
+      for (int b = B0; b < NBB; ++b) {
+        if (a > 2 * b + 1) continue;
+        v[a][b] = fma(-ra, s[b], v[a][b]);
+      }
+    }
+  }
+  if constexpr (JB + 1 < NBA) ldl_steps<NBB, JB + 1>(v, k, warp, lane, raw, scl, dd, tiny);
+}
+
 template <int NBB>
 __global__ void __launch_bounds__(kLdlThreads, 1) chol_ldl_kernel(double* G, int k, int64_t ldg, double shift_factor,
                                                                 double* Rrow) {
@@ -238,16 +303,17 @@ __global__ void __launch_bounds__(kLdlThreads, 1) chol_ldl_kernel(double* G, int
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
   {
+    constexpr int kU = 4;
     const int kk2 = k * k;
-    for (int t0 = tid; t0 < kk2; t0 += 4 * kLdlThreads) {
-      double v[4];
+    for (int t0 = tid; t0 < kk2; t0 += kU * kLdlThreads) {
+      double v[kU];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
+      for (int u = 0; u < kU; ++u) {
         const int t = t0 + u * kLdlThreads, i = t % k, j = t / k;
         v[u] = (t < kk2 && i <= j) ? G[i + int64_t(j) * ldg] : 0.0;
       }
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
+      for (int u = 0; u < kU; ++u) {
         const int t = t0 + u * kLdlThreads, i = t % k, j = t / k;
         if (t < kk2 && i <= j) P[pku(i, j)] = v[u];
       }
@@ -281,52 +347,7 @@ __global__ void __launch_bounds__(kLdlThreads, 1) chol_ldl_kernel(double* G, int
       v[a][b] = x;
     }
 
-  for (int j = 0; j < k; ++j) {
-    const int p = j & 1;
-    double* rw = raw + p * KP;
-    double* sc = scl + p * KP;
-    if (warp == (j & 15)) {
-      // this warp holds row j: publish a[j][c] (c >= j), then a[j][c] / a[j][j]
-      const int aj = j >> 4;
-#pragma unroll
-      for (int a = 0; a < NBA; ++a) {
-        if (a != aj) continue;
-#pragma unroll
-        for (int b = 0; b < NBB; ++b) {
-          if (a > 2 * b + 1) continue;
-          const int c = lane + 32 * b;
-          if (c >= j && c < k) rw[c] = v[a][b];
-        }
-      }
-      __syncwarp();
-      const double d = rw[j];
-      const bool ok = d > tiny;
-      const double inv = ok ? __drcp_rn(d) : 0.0;
-#pragma unroll
-      for (int b = 0; b < NBB; ++b) {
-        const int c = lane + 32 * b;
-        if (c > j && c < k) sc[c] = rw[c] * inv;
-      }
-      if (lane == 0) dd[j] = ok ? d : 0.0;
-    }
-    __syncthreads();
-    // a[r][c] -= a[j][r] * (a[j][c] / a[j][j]) for r > j; slots left of the
-    // diagonal take garbage that is never read
-    double s[NBB];
-#pragma unroll
-    for (int b = 0; b < NBB; ++b) s[b] = (32 * b + 31 > j) ? sc[lane + 32 * b] : 0.0;
-#pragma unroll
-    for (int a = 0; a < NBA; ++a) {
-      const int r = warp + 16 * a;
-      if (r <= j) continue;
-      const double ra = rw[r];
-#pragma unroll
-      for (int b = 0; b < NBB; ++b) {
-        if (a > 2 * b + 1) continue;
-        v[a][b] = fma(-ra, s[b], v[a][b]);
-      }
-    }
-  }
+  ldl_steps<NBB, 0>(v, k, warp, lane, raw, scl, dd, tiny);
   for (int i = tid; i < k; i += kLdlThreads) rs[i] = dd[i] > 0.0 ? rsqrt(dd[i]) : 0.0;
   __syncthreads();
   // R = D^1/2 U into P; a failed pivot gives R[j][j] = 1 and row j zero

@@ -21,6 +21,8 @@ CASES = [
     (130, 70, 33, 1),
     (2500, 160, 2500, 0),   # projector range finder: few output tiles, long K (split-K)
     (160, 160, 2500, 0),    # Gram matrix shape
+    (161, 157, 3001, 1),    # split-K with edge tiles and beta (23 splits)
+    (97, 33, 20000, 1),     # two output tiles, 156 splits
     (1000, 1200, 100, 0),   # many output tiles (128x128 kernel)
     (1001, 1203, 101, 1),   # the same with odd sizes (odd leading dimensions)
     (40000, 50, 25, 0),     # tall and narrow (128x64 tiles): the contractions with A
@@ -47,3 +49,17 @@ def test_gemm_f64_matches_numpy(engine, pkg, opA, opB, case):
     out = pkg.host.gemm_f64(opA, opB, A, B, alpha=alpha, beta=beta, C=C, engine=engine)
     bound = 2 * k * EPS * abs(alpha) * (np.abs(opa(A)) @ np.abs(opb(B))) + 2 * EPS * np.abs(beta * C) + 1e-300
     assert np.all(np.abs(out - ref) <= bound), float(np.max(np.abs(out - ref) / bound))
+
+
+def test_gemm_f64_split_k_is_deterministic(engine, pkg):
+    """The split-K partial products are summed in split order, whatever order
+    the CTAs ran in: repeated products are bitwise equal."""
+    rng = np.random.default_rng(5)
+    A = np.asfortranarray(rng.standard_normal((2500, 160)))
+    B = np.asfortranarray(rng.standard_normal((2500, 160)))
+    outs = [pkg.host.gemm_f64("T", "N", A, B, engine=engine) for _ in range(4)]
+    for o in outs[1:]:
+        assert np.array_equal(o, outs[0])
+    ref = A.T @ B
+    bound = 2 * 2500 * EPS * (np.abs(A.T) @ np.abs(B))
+    assert np.all(np.abs(outs[0] - ref) <= bound)
