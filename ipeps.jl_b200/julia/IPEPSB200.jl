@@ -267,4 +267,113 @@ function ChainRulesCore.rrule(::typeof(ctm_energy), A::AbstractArray{Float64,5},
     return E, ctm_energy_pullback
 end
 
+# ---- plaquette (2x2-cluster) observables of the h4 drivers and optim_wp
+
+"""`ipeps_ctensor_t`: one complex column-major tensor of the plaquette MPO."""
+struct CTensor
+    data::Ptr{Float64}
+    nd::Cint
+    dims::NTuple{4,Int64}
+end
+
+"""The MPO [s1, s2, s3, s4] of `get_local_h` (src/model/local_h.jl:1-31) as C
+tensors; keep the returned arrays alive (GC.@preserve) during the call."""
+function mpo_tensors(H4)
+    length(H4) == 4 || error("the plaquette Hamiltonian is the MPO [s1, s2, s3, s4]")
+    arrs = [Array{ComplexF64}(h) for h in H4]
+    cts = [CTensor(Ptr{Float64}(pointer(a)), Cint(ndims(a)),
+                   ntuple(i -> i <= ndims(a) ? Int64(size(a, i)) : Int64(0), 4)) for a in arrs]
+    return arrs, cts
+end
+
+"""`get_gs_energy_4x4(ts, H4)` (evaluation.jl:339-356); with `es=true`
+`get_es_energy_4x4` (evaluation.jl:358-398, B set)."""
+function get_energy_4x4(ts::CTMTensorsB200, H4; es::Bool=false)
+    arrs, cts = mpo_tensors(H4)
+    E = zeros(2)
+    GC.@preserve arrs cts E begin
+        check(ts.eng.h, ccall((:ipeps_energy_4x4, lib), Cint, (Ptr{Cvoid}, Ptr{CTensor}, Cint, Ptr{Float64}),
+                              ts.h, cts, es ? 1 : 0, E))
+    end
+    return complex(E[1], E[2])
+end
+
+"""`run_ctm(ts; conv_fun = ts -> get_gs_energy_4x4(ts, H4))` (optim_gs_h4.jl);
+`es=true`: the nested criterion of optim_es_h4.jl:139.  Returns (ts, last diff)."""
+function run_ctm_4x4(ts::CTMTensorsB200, H4; es::Bool=false)
+    push_params!(ts)
+    arrs, cts = mpo_tensors(H4)
+    iters, diff, conv = Ref{Cint}(0), Ref{Float64}(0), Ref{Cint}(0)
+    GC.@preserve arrs cts begin
+        check(ts.eng.h, ccall((:ipeps_ctm_run_4x4, lib), Cint,
+                              (Ptr{Cvoid}, Ptr{CTensor}, Cint, Ref{Cint}, Ref{Float64}, Ref{Cint}),
+                              ts.h, cts, es ? 1 : 0, iters, diff, conv))
+    end
+    conv[] == 0 && println("--------- Not Converged ----------")
+    return ts, diff[]
+end
+
+"""The pullback of `run_gs_h4` (optim_gs_h4.jl:113-123) w.r.t. A (real A)."""
+function energy_grad_4x4!(ts::CTMTensorsB200{Float64}, H4)
+    arrs, cts = mpo_tensors(H4)
+    E = zeros(1)
+    g = similar(ts.A)
+    GC.@preserve arrs cts E g begin
+        check(ts.eng.h, ccall((:ipeps_energy_grad_4x4, lib), Cint,
+                              (Ptr{Cvoid}, Ptr{CTensor}, Cint, Ptr{Float64}, Ptr{Float64}),
+                              ts.h, cts, get(ts.Params, "ad_max_iter", 4), E, g))
+    end
+    return E[1], g
+end
+
+"""The pullback of `run_es_h4` w.r.t. B in `get_es_grad_h4` (optim_es_h4.jl:150-188)."""
+function es_energy_grad_4x4!(ts::CTMTensorsB200, H4)
+    arrs, cts = mpo_tensors(H4)
+    E = zeros(1)
+    g = Array{ComplexF64}(undef, size(ts.A))
+    GC.@preserve arrs cts E g begin
+        check(ts.eng.h, ccall((:ipeps_es_energy_grad_4x4, lib), Cint,
+                              (Ptr{Cvoid}, Ptr{CTensor}, Cint, Ptr{Float64}, Ptr{ComplexF64}),
+                              ts.h, cts, get(ts.Params, "ad_max_iter", 4), E, g))
+    end
+    return E[1], g
+end
+
+"""`get_wp_grad` (optim_wp.jl:195-238) in the environment held by ts (no
+CTMRG): the plaquette operator wp4 (an MPO as for the energy) and the norm of
+the cluster whose site `site` (Params["wp"], 1..4) holds B, the others A.
+Returns (operator value, norm, gH, gN)."""
+function get_wp_grad(ts::CTMTensorsB200, wp4, site::Integer, B::AbstractArray)
+    arrs, cts = mpo_tensors(wp4)
+    Bc = Array{ComplexF64}(reshape(B, size(ts.A)))
+    vn = zeros(4)
+    gH = Array{ComplexF64}(undef, size(ts.A))
+    gN = Array{ComplexF64}(undef, size(ts.A))
+    GC.@preserve arrs cts Bc vn gH gN begin
+        check(ts.eng.h, ccall((:ipeps_wp_grad, lib), Cint,
+                              (Ptr{Cvoid}, Ptr{CTensor}, Cint, Ptr{ComplexF64}, Ptr{Float64}, Ptr{ComplexF64},
+                               Ptr{ComplexF64}),
+                              ts.h, cts, site, Bc, vn, gH, gN))
+    end
+    return complex(vn[1], vn[2]), complex(vn[3], vn[4]), gH, gN
+end
+
+"""`run_gs_h4` of optim_gs_h4.jl:113-123 as one differentiable function
+(converge with the plaquette energy, ad_max_iter iterations, the energy);
+its rrule returns the hand-written adjoint for fg! (optim_gs_h4.jl:74)."""
+function ctm_energy_h4(A::AbstractArray{Float64,5}, H4, cfg::Dict)
+    ts = CTMTensorsB200(A, cfg)
+    run_ctm_4x4(ts, H4)
+    E, _ = energy_grad_4x4!(ts, H4)
+    return E
+end
+
+function ChainRulesCore.rrule(::typeof(ctm_energy_h4), A::AbstractArray{Float64,5}, H4, cfg::Dict)
+    ts = CTMTensorsB200(A, cfg)
+    run_ctm_4x4(ts, H4)
+    E, g = energy_grad_4x4!(ts, H4)
+    ctm_energy_h4_pullback(dE) = (NoTangent(), unthunk(dE) .* g, NoTangent(), NoTangent())
+    return E, ctm_energy_h4_pullback
+end
+
 end # module
