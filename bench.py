@@ -723,7 +723,7 @@ def run_es_momentum(args):
     dt = time.perf_counter() - t0
     for w in workers:
         w.close()
-    es = pkg.drivers.evaluate_es(effH, effN, 1e-3)
+    es = pkg.drivers.band_energies(effH, effN, 1e-3)
     print(json.dumps({"es_momentum": "heisenberg D=3 d=2 chi=48, (px, py) = (pi, 0)", "basis_vectors": int(basis.shape[1]),
                       "gs_lbfgs_steps": args.es_gs_steps, "E_gs": r["energies"][-1],
                       "contexts": max(args.es_workers, 1),

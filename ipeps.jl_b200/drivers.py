@@ -6,7 +6,7 @@ small matrices); only their calls into CTMRG go to the device.
     optim_gs(H, A0, cfg)        src/optimize/optim_gs.jl:14-118 (L-BFGS on the sphere)
     prepare_basis(H, A, cfg)    src/optimize/optim_es.jl:34-73
     optim_es(px, py, prep, cfg) src/optimize/optim_es.jl:91-165
-    evaluate_es(effH, effN)     src/graph/expectation.jl:152-183
+    evaluate_es(effH, effN)     src/graph/expectation.jl:152-183 (band_energies: its real parts)
     prepare_basis_h4 / optim_es_h4 (the plaquette Hamiltonian)
                                 src/optimize/optim_es_h4.jl
 
@@ -230,9 +230,17 @@ def compute_es(effH: np.ndarray, effN: np.ndarray, nrmB_cut=1e-3):
 
 
 def evaluate_es(effH: np.ndarray, effN: np.ndarray, nrmB_cut=1e-3):
-    """evaluate_es (expectation.jl:152-183): the sorted real parts of the
-    generalised eigenvalues of compute_es."""
-    es, _, _ = compute_es(effH, effN, nrmB_cut)
+    """evaluate_es (expectation.jl:152-183): (es, vecs), the generalised
+    eigenvalues (complex) and eigenvectors of H x = E N x on the selected
+    subspace, sorted by real part."""
+    es, vecs, _ = compute_es(effH, effN, nrmB_cut)
+    return es, vecs
+
+
+def band_energies(effH: np.ndarray, effN: np.ndarray, nrmB_cut=1e-3) -> np.ndarray:
+    """The real parts of evaluate_es's eigenvalues, ascending: the band
+    energies of one momentum."""
+    es, _ = evaluate_es(effH, effN, nrmB_cut)
     return np.sort(es.real)
 
 

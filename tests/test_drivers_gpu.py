@@ -57,7 +57,7 @@ def test_optim_es_band_energies_match_oracle(engine, pkg):
     E0, _ = pkg.get_gs_energy(ts, H)
     assert abs(E0.real - g["E0"]) <= 1e-10
     effH, effN = pkg.drivers.optim_es(g["px"], g["py"], ts, H2, basis)
-    es = pkg.drivers.evaluate_es(effH, effN, g["nrmB_cut"])
+    es = pkg.drivers.band_energies(effH, effN, g["nrmB_cut"])
     eo = np.asarray(g["es"])
     assert len(es) == len(eo)
     assert np.allclose(es[:4], eo[:4], rtol=0, atol=1e-6), (es[:4], eo[:4])
@@ -82,7 +82,7 @@ def test_optim_es_concurrent_contexts_match_oracle(engine, pkg):
         for e in extra:
             e.close()
     assert np.all(np.abs(effN).sum(axis=0) > 0)  # every column computed
-    es = pkg.drivers.evaluate_es(effH, effN, g["nrmB_cut"])
+    es = pkg.drivers.band_energies(effH, effN, g["nrmB_cut"])
     eo = np.asarray(g["es"])
     assert len(es) == len(eo)
     assert np.allclose(es, eo, rtol=1e-6, atol=1e-6), (es[:4], eo[:4])

@@ -52,3 +52,37 @@ def test_get_wp_basis_splits_the_basis_by_eigenvalue_sign(pkg):
     cp, cm = basis.conj().T @ bp, basis.conj().T @ bm
     assert np.abs(cm.conj().T @ N @ cp).max() <= 1e-9 * np.abs(N).max() * max(np.abs(cp).max(), 1) * max(
         np.abs(cm).max(), 1)
+
+
+def test_evaluate_es_generalised_eigenproblem_and_cuts(pkg):
+    """compute_es / evaluate_es (expectation.jl:13-56, 152-183) on a synthetic
+    pair with known answers: N = X X^H, H = X diag(E) X^H has the generalised
+    eigenvalues E; directions of N below nrmB_cut (a ratio to its largest
+    eigenvalue) drop out, and an integer cut keeps the eigenvalues above the
+    (cut+1)-th (Julia's 1-based ev_N[nrmB_cut+1])."""
+    drv = pkg.drivers
+    rng = np.random.default_rng(11)
+    nb = 12
+    X = rng.standard_normal((nb, nb)) + 1j * rng.standard_normal((nb, nb))
+    E = np.sort(rng.uniform(-1.0, 2.0, nb))
+    N = X @ X.conj().T
+    H = X @ np.diag(E) @ X.conj().T
+    es, vecs = drv.evaluate_es(H, N, 1e-12)
+    assert np.allclose(es.real, E, atol=1e-9) and np.abs(es.imag).max() < 1e-9
+    assert np.all(np.diff(es.real) >= 0)
+    # each eigenvector solves H2 x = e N2 x on the selected subspace
+    Hp, Np, P = drv._es_subspace(H, N, 1e-12)
+    assert np.allclose(Hp @ vecs, (Np @ vecs) * es[None, :], atol=1e-8 * np.abs(Hp).max())
+    assert np.allclose(drv.band_energies(H, N, 1e-12), E, atol=1e-9)
+    # a nearly null direction of N (1e-8 of its largest eigenvalue) is cut at 1e-3
+    w, Q = np.linalg.eigh(N)
+    w2 = w.copy()
+    w2[0] = 1e-8 * w.max()
+    N2 = (Q * w2) @ Q.conj().T
+    _, _, P2 = drv._es_subspace(H, N2, 1e-3)
+    assert P2.shape[1] == nb - 1
+    # integer cut: the 4 largest eigenvalues of N
+    _, _, P4 = drv._es_subspace(H, N, 4)
+    assert P4.shape[1] == 4
+    top = np.sort(np.linalg.eigvalsh(N))[::-1][:4]
+    assert np.allclose(np.sort(np.linalg.eigvalsh(P4.conj().T @ N @ P4))[::-1], top)

@@ -66,7 +66,7 @@ def test_sharded_es_matches_serial(tmp_path, nb):
         seen += list(d["calls"])
     assert sorted(seen) == list(range(nb))
     # the eigenproblem of the gathered matrices is the serial one
-    w_serial = drivers.evaluate_es(H @ H.conj().T, N @ N.conj().T + np.eye(nb))
+    w_serial = drivers.band_energies(H @ H.conj().T, N @ N.conj().T + np.eye(nb))
     d = np.load(tmp_path / "r1.npz")
-    w_shard = drivers.evaluate_es(d["effH"] @ d["effH"].conj().T, d["effN"] @ d["effN"].conj().T + np.eye(nb))
+    w_shard = drivers.band_energies(d["effH"] @ d["effH"].conj().T, d["effN"] @ d["effN"].conj().T + np.eye(nb))
     assert np.allclose(w_serial, w_shard)
