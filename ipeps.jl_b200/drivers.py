@@ -333,6 +333,17 @@ def correlation_TM(ts: host.CTMTensors, direction: str = "h", N: int = 10, full:
     return es1[es1 > 0], es, TM
 
 
+def correlation_TM_A(A, cfg: Dict[str, Any], direction: str = "h", engine: Optional[host.Engine] = None):
+    """correlation_TM_A (expectation.jl:185-191): CTMTensors(A, cfg), run_ctm
+    with the spectrum criterion, then correlation_TM of the converged edges."""
+    ts = host.CTMTensors(A, cfg, engine=engine)
+    try:
+        ts, _ = host.run_ctm(ts)
+        return correlation_TM(ts, direction=direction)
+    finally:
+        ts.close()
+
+
 # ---------------------------------------------------------------- plaquette (h4) drivers
 def _wrap_svd(M: np.ndarray):
     """wrap_svd (wrapper.jl:25-55) without a rank cap: SVD sorted descending,
