@@ -108,3 +108,19 @@ def test_correlation_TM_matches_oracle(engine, pkg, direction):
     ts.close()
     eo = eo.numpy()
     assert np.allclose(es1[:4], eo[:4], rtol=1e-9), (es1[:4], eo[:4])
+
+
+def test_correlation_TM_A_matches_oracle(engine, pkg):
+    """correlation_TM_A (expectation.jl:185-191): CTMTensors(A, cfg), run_ctm
+    with the spectrum criterion, correlation_TM; against the oracle's run_ctm
+    (spectrum criterion) + correlation_TM, 1e-8 relative."""
+    A = O.random_A(2, 2, seed=12)
+    cfg = O.default_config()
+    cfg.update(chi=10, min_iter=4, max_iter=60, rg_tol=1e-12)
+    ts_o = O.make_ctm_tensors(A, cfg)
+    with torch.no_grad():
+        ts_o, _ = O.run_ctm(ts_o)
+        eo, _ = O.correlation_TM(ts_o, "h", N=4)
+    es1, es, TM = pkg.drivers.correlation_TM_A(A.numpy(), cfg, direction="h", engine=engine)
+    eo = eo.numpy()
+    assert np.allclose(es1[:4], eo[:4], rtol=1e-8), (es1[:4], eo[:4])
