@@ -495,6 +495,20 @@ def run_ours(args):
             out["families_ms"] = {k: round(v["ms"], 3) for k, v in pr.items()}
             if n == "mixed" and gname != "gemm_tf32x3" and pr["gemm_tf32x3"]["ms"] > 0:
                 out["tf32x3"] = gemm_roofline(pr, "gemm_tf32x3", total_ms)
+            pm = pr["permute"]
+            if pm["ms"] > 0:
+                # the HBM-bound family: the tcon planner's permutes (one read and one
+                # write of every element) and the 3xTF32 operand splits (FP64 in,
+                # hi/lo TF32 planes out), over their event-timed device time (the
+                # events bracket each launch, so short launches read a little low)
+                gbs = pm["bytes"] / (pm["ms"] / 1e3) / 1e9
+                out["permute"] = {"bound": "hbm", "kernel": "permute_rows / permute_tiled / split_kc / split_tr",
+                                  "achieved": gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                                  "frac": gbs / peaks["hbm_gbs"], "traffic": None,
+                                  "peak_source": f"{peak_kind} hbm_gbs",
+                                  "bytes_per_launch": pm["bytes"] / max(1, pm["launches"]),
+                                  "kernel_share_of_device_time": pm["ms"] / total_ms if total_ms else None,
+                                  "launches_in_profiled_step": pm["launches"]}
             return out
 
         acc = {}
