@@ -154,18 +154,37 @@ struct RowArgs {
 // short rows take one warp each.
 constexpr int64_t kPermChunk = 2048;
 
-template <typename T>
+// SMALL: the unit count and every output dim fit in 32 bits, so the row
+// index is decomposed with 32-bit divisions (a 64-bit division is several
+// times the instructions, and the decomposition is most of the work of a
+// short row).
+template <typename T, bool SMALL>
 __global__ void permute_rows(RowArgs a, int64_t rows, int64_t nchunk, const T* __restrict__ in, T* __restrict__ out) {
   const int lane = threadIdx.x & 31;
   const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
   const int64_t units = rows * nchunk;
   for (int64_t u = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; u < units; u += nwarps) {
-    const int64_t r = u / nchunk, c0 = (u - r * nchunk) * kPermChunk;
-    int64_t q = r, off = 0;
-    for (int i = 0; i < a.nd; ++i) {
-      const int64_t t = q / a.odims[i];
-      off += (q - t * a.odims[i]) * a.istride[i];
-      q = t;
+    int64_t r, c0, off = 0;
+    if constexpr (SMALL) {
+      const uint32_t uu = uint32_t(u), nc = uint32_t(nchunk);
+      uint32_t q = uu / nc;
+      r = q;
+      c0 = int64_t(uu - q * nc) * kPermChunk;
+      for (int i = 0; i < a.nd; ++i) {
+        const uint32_t od = uint32_t(a.odims[i]);
+        const uint32_t t = q / od;
+        off += int64_t(q - t * od) * a.istride[i];
+        q = t;
+      }
+    } else {
+      r = u / nchunk;
+      c0 = (u - r * nchunk) * kPermChunk;
+      int64_t q = r;
+      for (int i = 0; i < a.nd; ++i) {
+        const int64_t t = q / a.odims[i];
+        off += (q - t * a.odims[i]) * a.istride[i];
+        q = t;
+      }
     }
     const T* src = in + off;
     T* dst = out + r * a.n0;
@@ -175,9 +194,11 @@ __global__ void permute_rows(RowArgs a, int64_t rows, int64_t nchunk, const T* _
       // both runs 16-byte aligned: two doubles per load and store
       const double2* s2 = reinterpret_cast<const double2*>(src);
       double2* d2 = reinterpret_cast<double2*>(dst);
+#pragma unroll 4
       for (int64_t i = (c0 >> 1) + lane; i < (c1 >> 1); i += 32) d2[i] = s2[i];
       if ((c1 & 1) && lane == 0) dst[c1 - 1] = src[c1 - 1];
     } else {
+#pragma unroll 4
       for (int64_t i = c0 + lane; i < c1; i += 32) dst[i] = src[i];
     }
   }
@@ -245,7 +266,12 @@ void permute_impl(Ctx& c, const Tensor& in, const std::vector<int>& perm, Tensor
     const int64_t rows = total / a.n0;
     const int64_t nchunk = (a.n0 + kPermChunk - 1) / kPermChunk;
     const int64_t blocks = std::min<int64_t>((rows * nchunk + 7) / 8, int64_t(c.sm_count) * 16);
-    permute_rows<T><<<unsigned(std::max<int64_t>(blocks, 1)), 256, 0, c.stream>>>(a, rows, nchunk, ip, op);
+    bool small = rows * nchunk <= int64_t(UINT32_MAX);
+    for (int i = 0; i < a.nd; ++i) small = small && a.odims[i] <= int64_t(UINT32_MAX);
+    if (small)
+      permute_rows<T, true><<<unsigned(std::max<int64_t>(blocks, 1)), 256, 0, c.stream>>>(a, rows, nchunk, ip, op);
+    else
+      permute_rows<T, false><<<unsigned(std::max<int64_t>(blocks, 1)), 256, 0, c.stream>>>(a, rows, nchunk, ip, op);
   } else if (perm[0] == 0 || in.dims[0] == 1 || out.dims[0] == 1) {
     PermArgs a{};
     a.nd = nd;
